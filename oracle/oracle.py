@@ -1,0 +1,691 @@
+"""CPU oracle for the quantum-jax kick-drift-kick Schroedinger-Poisson step.
+
+TEST INFRASTRUCTURE ONLY.  This module is the float64 NumPy/SciPy restatement
+of the reference's step functions, op for op, used as the correctness checker.
+Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg
+may import it; the product path (``qj``) never does and has no CPU fallback.
+
+Parity pin: ``tests/golden/make_golden.py`` executes the reference scripts'
+own functions (quantum-stars.py, quantum-gas-bh.py, quantum-tidal.py,
+quantum-cosmo.py, quantum-fluid-accretion-test.py) on a float64 NumPy stand-in
+for ``jax.numpy`` (JAX itself is not installable here) and stores their outputs
+under ``tests/golden``.  ``tests/test_oracle_golden.py`` checks this module
+against those fixtures.  The pin covers the algorithm (k-grid, k=0 handling,
+Nyquist sign, CIC weights and order, limiter, fluxes, accretion formulas), not
+XLA's float32 rounding, which cannot be run here.
+
+Every function cites the reference lines it restates.  Arrays are C-order
+``[nx][ny][nz]`` (z fastest), as built by ``meshgrid(..., indexing="ij")``.
+"""
+
+from __future__ import annotations
+
+import dataclasses
+import math
+import os
+
+import numpy as np
+
+try:  # scipy's pocketfft is threaded; numpy's is the fallback
+    import scipy.fft as _sfft
+
+    def _fftn(a, workers):
+        return _sfft.fftn(a, workers=workers)
+
+    def _ifftn(a, workers):
+        return _sfft.ifftn(a, workers=workers)
+
+except ImportError:  # pragma: no cover
+    def _fftn(a, workers):
+        return np.fft.fftn(a)
+
+    def _ifftn(a, workers):
+        return np.fft.ifftn(a)
+
+
+WORKERS = int(os.environ.get("QJ_ORACLE_WORKERS", "1"))
+
+
+# ---------------------------------------------------------------------------
+# Configuration (the reference keeps these as module globals,
+# quantum-stars.py:61-157, quantum-gas-bh.py:46-133)
+# ---------------------------------------------------------------------------
+
+
+@dataclasses.dataclass
+class Grid:
+    nx: int
+    ny: int
+    nz: int
+    Lx: float
+    Ly: float
+    Lz: float
+
+    @property
+    def shape(self):
+        return (self.nx, self.ny, self.nz)
+
+    @property
+    def dx(self):
+        return self.Lx / self.nx
+
+    @property
+    def dy(self):
+        return self.Ly / self.ny
+
+    @property
+    def dz(self):
+        return self.Lz / self.nz
+
+    @property
+    def vol(self):
+        return self.dx * self.dy * self.dz
+
+    @property
+    def ncell(self):
+        return self.nx * self.ny * self.nz
+
+
+@dataclasses.dataclass
+class Phys:
+    m_per_hbar: float = 1.0
+    G: float = 1.0 / (4.0 * math.pi)
+    rho_bar: float = 1.0
+    b_coeff: float = 0.0  # self-interaction, quantum-stars.py:117-125
+    m_s: float = 0.0  # star particle mass, quantum-stars.py:115
+    cs: float = 1.0  # gas sound speed, quantum-gas-bh.py:74
+    c_light: float = 299792.458  # quantum-gas-bh.py:86
+
+
+# ---------------------------------------------------------------------------
+# R1: Fourier grid, quantum-stars.py:142-149
+# ---------------------------------------------------------------------------
+
+
+def k_lin(n: int, L: float) -> np.ndarray:
+    """ifftshift(2 pi / L * arange(-n/2, n/2)): index n/2 holds -pi n / L."""
+    return np.fft.ifftshift(2.0 * np.pi / L * np.arange(-n / 2, n / 2))
+
+
+def kgrid(g: Grid):
+    kx, ky, kz = np.meshgrid(
+        k_lin(g.nx, g.Lx), k_lin(g.ny, g.Ly), k_lin(g.nz, g.Lz), indexing="ij"
+    )
+    k_sq = kx**2 + ky**2 + kz**2
+    return kx, ky, kz, k_sq
+
+
+def cell_centres(g: Grid):
+    """quantum-stars.py:136-139."""
+    x = np.linspace(0.5 * g.dx, g.Lx - 0.5 * g.dx, g.nx)
+    y = np.linspace(0.5 * g.dy, g.Ly - 0.5 * g.dy, g.ny)
+    z = np.linspace(0.5 * g.dz, g.Lz - 0.5 * g.dz, g.nz)
+    return np.meshgrid(x, y, z, indexing="ij")
+
+
+# ---------------------------------------------------------------------------
+# R2: Poisson, quantum-stars.py:189-193
+# ---------------------------------------------------------------------------
+
+
+def get_potential(rho, g: Grid, p: Phys, k=None, self_interaction=False):
+    """V = Re ifftn(-fftn(4 pi G (rho - rho_bar)) / (k^2 + [k^2 == 0]))."""
+    k_sq = (k if k is not None else kgrid(g))[3]
+    V_hat = -_fftn(4.0 * np.pi * p.G * (rho - p.rho_bar), WORKERS) / (
+        k_sq + (k_sq == 0)
+    )
+    V = np.real(_ifftn(V_hat, WORKERS))
+    return V + p.b_coeff * rho if self_interaction else V
+
+
+# ---------------------------------------------------------------------------
+# R3/R4: cloud-in-cell, quantum-stars.py:200-247
+# ---------------------------------------------------------------------------
+
+# The 8 corner visits in the fixed order of quantum-stars.py:220-243 and
+# :264-287: 0 selects i, 1 selects ip1, per axis.
+CORNERS = (
+    (0, 0, 0),
+    (1, 0, 0),
+    (0, 1, 0),
+    (0, 0, 1),
+    (1, 1, 0),
+    (1, 0, 1),
+    (0, 1, 1),
+    (1, 1, 1),
+)
+
+
+def get_cic_indices_and_weights(pos, g: Grid):
+    """quantum-stars.py:200-209 (float64)."""
+    dxs = np.array([g.dx, g.dy, g.dz])
+    i = np.floor((pos - 0.5 * dxs) / dxs)
+    ip1 = i + 1.0
+    weight_i = ((ip1 + 0.5) * dxs - pos) / dxs
+    weight_ip1 = (pos - (i + 0.5) * dxs) / dxs
+    n = np.array([g.nx, g.ny, g.nz])
+    i = np.mod(i, n).astype(np.int64)
+    ip1 = np.mod(ip1, n).astype(np.int64)
+    return i, ip1, weight_i, weight_ip1
+
+
+def bin_stars(pos, g: Grid, masses):
+    """quantum-stars.py:212-247 / quantum-gas-bh.py:414-449.
+
+    ``masses`` is the per-particle mass (m_s for every star, m_bh[s] for black
+    holes).  Deposits in star order, corners in the fixed order."""
+    rho = np.zeros(g.shape)
+    i, ip1, w_i, w_ip1 = get_cic_indices_and_weights(pos, g)
+    vol = g.dx * g.dy * g.dz
+    idx = (i, ip1)
+    w = (w_i, w_ip1)
+    for s in range(pos.shape[0]):
+        fac = masses[s] / vol
+        for c in CORNERS:
+            rho[idx[c[0]][s, 0], idx[c[1]][s, 1], idx[c[2]][s, 2]] += (
+                w[c[0]][s, 0] * w[c[1]][s, 1] * w[c[2]][s, 2] * fac
+            )
+    return rho
+
+
+def grid_accelerations(rho, g: Grid, p: Phys, k=None):
+    """Grid part of quantum-stars.py:254-260: a_d = -Re ifftn(i k_d V_hat)."""
+    kx, ky, kz, k_sq = k if k is not None else kgrid(g)
+    V_hat = -_fftn(4.0 * np.pi * p.G * (rho - p.rho_bar), WORKERS) / (
+        k_sq + (k_sq == 0)
+    )
+    ax = -np.real(_ifftn(1.0j * kx * V_hat, WORKERS))
+    ay = -np.real(_ifftn(1.0j * ky * V_hat, WORKERS))
+    az = -np.real(_ifftn(1.0j * kz * V_hat, WORKERS))
+    return ax, ay, az
+
+
+def interpolate_cic(a_grid, pos, g: Grid):
+    """quantum-stars.py:262-287: 8-point gather in fixed corner order."""
+    i, ip1, w_i, w_ip1 = get_cic_indices_and_weights(pos, g)
+    idx = (i, ip1)
+    w = (w_i, w_ip1)
+    acc = np.zeros((pos.shape[0], a_grid.shape[-1]))
+    for c in CORNERS:
+        acc += (w[c[0]][:, 0] * w[c[1]][:, 1] * w[c[2]][:, 2])[:, None] * a_grid[
+            idx[c[0]][:, 0], idx[c[1]][:, 1], idx[c[2]][:, 2]
+        ]
+    return acc
+
+
+def get_acceleration(pos, rho, g: Grid, p: Phys, k=None):
+    """quantum-stars.py:250-288 -> (acc [n,3], a_max)."""
+    ax, ay, az = grid_accelerations(rho, g, p, k)
+    a_grid = np.stack((ax, ay, az), axis=-1)
+    a_max = np.max(np.abs(a_grid))
+    return interpolate_cic(a_grid, pos, g), a_max
+
+
+def ref_mod(x, y):
+    """jnp.mod / np.mod: result carries the sign of the divisor."""
+    return np.mod(x, y)
+
+
+# ---------------------------------------------------------------------------
+# R6-R9: the stars KDK step, quantum-stars.py:295-330
+# ---------------------------------------------------------------------------
+
+
+def kick(psi, V, p: Phys, dt):
+    """quantum-stars.py:301 / :318."""
+    return np.exp(-1.0j * p.m_per_hbar * dt / 2.0 * V) * psi
+
+
+def drift(psi, g: Grid, p: Phys, dt, k=None, kin_fac=1.0):
+    """quantum-stars.py:307-309 (kin_fac: quantum-cosmo.py:185)."""
+    k_sq = (k if k is not None else kgrid(g))[3]
+    psi_hat = _fftn(psi, WORKERS)
+    psi_hat = np.exp(dt * kin_fac * (-1.0j * k_sq / p.m_per_hbar / 2.0)) * psi_hat
+    return _ifftn(psi_hat, WORKERS)
+
+
+def stars_compute_step(
+    psi, pos, vel, t, a_max, dt_s, g: Grid, p: Phys, dt, k=None,
+    self_interaction=False,
+):
+    """quantum-stars.py:295-330, float64."""
+    if k is None:
+        k = kgrid(g)
+    L = np.array([g.Lx, g.Ly, g.Lz])
+    masses = np.full(pos.shape[0], p.m_s)
+    # (1/2) kick
+    rho_s = bin_stars(pos, g, masses)
+    rho_tot = np.abs(psi) ** 2 + rho_s
+    V = get_potential(rho_tot, g, p, k, self_interaction)
+    psi = kick(psi, V, p, dt)
+    acc, a_max1 = get_acceleration(pos, rho_tot, g, p, k)
+    vel = vel + acc * dt / 2.0
+    # drift
+    psi = drift(psi, g, p, dt, k)
+    pos = pos + vel * dt
+    pos = ref_mod(pos, L)
+    # (1/2) kick
+    rho_s = bin_stars(pos, g, masses)
+    rho_tot = np.abs(psi) ** 2 + rho_s
+    V = get_potential(rho_tot, g, p, k, self_interaction)
+    psi = kick(psi, V, p, dt)
+    acc, a_max2 = get_acceleration(pos, rho_tot, g, p, k)
+    vel = vel + acc * dt / 2.0
+    t = t + dt
+    a_max = max(a_max, a_max1, a_max2)
+    with np.errstate(divide="ignore"):
+        dt_s = np.min(np.abs(g.dx / vel)) if vel.size else np.inf
+    return psi, pos, vel, t, a_max, dt_s
+
+
+def stars_run(psi, pos, vel, nsteps, g, p, dt, t=0.0, a_max=0.0, dt_s=None,
+              self_interaction=False):
+    k = kgrid(g)
+    if dt_s is None:
+        dt_s = dt
+    for _ in range(nsteps):
+        psi, pos, vel, t, a_max, dt_s = stars_compute_step(
+            psi, pos, vel, t, a_max, dt_s, g, p, dt, k, self_interaction
+        )
+    return psi, pos, vel, t, a_max, dt_s
+
+
+def timestep_constants(g: Grid, p: Phys, t_end, dt_fac=1.0):
+    """quantum-stars.py:151-157: dt_kin, nt (multiple of 100), nt_sub, dt."""
+    dt_kin = dt_fac * p.m_per_hbar / 6.0 * (g.dx * g.dy * g.dz) ** (2.0 / 3.0)
+    nt = int(math.ceil(math.ceil(t_end / dt_kin) / 100.0) * 100)
+    nt_sub = int(round(nt / 100.0))
+    return dt_kin, nt, nt_sub, t_end / nt
+
+
+# ---------------------------------------------------------------------------
+# R11: tidal and cosmological variants
+# ---------------------------------------------------------------------------
+
+
+def external_potential(g: Grid, G, M_halo):
+    """quantum-tidal.py:175-179 (point mass at the box centre, softened)."""
+    X, Y, Z = cell_centres(g)
+    r = np.sqrt((X - 0.5 * g.Lx) ** 2 + (Y - 0.5 * g.Ly) ** 2 + (Z - 0.5 * g.Lz) ** 2)
+    return -G * M_halo / (r + 0.5 * g.dx)
+
+
+def tidal_compute_step(psi, t, g: Grid, p: Phys, dt, V_ext, k=None):
+    """quantum-tidal.py:186-207."""
+    if k is None:
+        k = kgrid(g)
+    V = get_potential(np.abs(psi) ** 2, g, p, k) + V_ext
+    psi = kick(psi, V, p, dt)
+    psi = drift(psi, g, p, dt, k)
+    V = get_potential(np.abs(psi) ** 2, g, p, k) + V_ext
+    psi = kick(psi, V, p, dt)
+    return psi, t + dt
+
+
+def cosmo_compute_dt(a, da, H0, omega_matter, omega_lambda):
+    """quantum-cosmo.py:149-162 (1000-point midpoint quadrature)."""
+    n_quad = 1000
+    h = 1.0 / n_quad
+    lin = np.linspace(0.5 * h, 1.0 - 0.5 * h, n_quad)
+    a_tmp = a * lin
+    adot = H0 * np.sqrt((omega_matter / a_tmp) + (omega_lambda * a_tmp**2))
+    t = np.mean(1.0 / adot) * (a - 0.0)
+    a_tmp = (a + da) * lin
+    adot = H0 * np.sqrt((omega_matter / a_tmp) + (omega_lambda * a_tmp**2))
+    return np.mean(1.0 / adot) * ((a + da) - 0.0) - t
+
+
+def cosmo_factors(a, da, H0, omega_matter, omega_lambda):
+    """quantum-cosmo.py:173-176 -> (dt, kin_fac, pot_fac)."""
+    kin_fac = 0.5 * (a**-2 + (a + da) ** -2)
+    pot_fac = 0.5 * (a**-1 + (a + da) ** -1)
+    return cosmo_compute_dt(a, da, H0, omega_matter, omega_lambda), kin_fac, pot_fac
+
+
+def cosmo_compute_step(psi, a, da, g: Grid, p: Phys, H0, om, ol, k=None):
+    """quantum-cosmo.py:169-196."""
+    if k is None:
+        k = kgrid(g)
+    dt, kin_fac, pot_fac = cosmo_factors(a, da, H0, om, ol)
+    V = get_potential(np.abs(psi) ** 2, g, p, k)
+    psi = np.exp(-1.0j * p.m_per_hbar * dt * pot_fac / 2.0 * V) * psi
+    psi = drift(psi, g, p, dt, k, kin_fac)
+    V = get_potential(np.abs(psi) ** 2, g, p, k)
+    psi = np.exp(-1.0j * p.m_per_hbar * dt * pot_fac / 2.0 * V) * psi
+    return psi, a + da
+
+
+# ---------------------------------------------------------------------------
+# R12/R13: isothermal MUSCL hydro, quantum-gas-bh.py:170-395
+# (cubic grid with spacing dx, as in the reference)
+# ---------------------------------------------------------------------------
+
+
+def get_conserved(rho, vx, vy, vz, vol):
+    """quantum-gas-bh.py:170-176."""
+    return rho * vol, rho * vx * vol, rho * vy * vol, rho * vz * vol
+
+
+def get_primitive(Mass, Momx, Momy, Momz, vol):
+    """quantum-gas-bh.py:179-185."""
+    return Mass / vol, Momx / Mass, Momy / Mass, Momz / Mass
+
+
+def get_gradient(f, dx):
+    """quantum-gas-bh.py:188-193 (central differences)."""
+    return (
+        (np.roll(f, -1, axis=0) - np.roll(f, 1, axis=0)) / (2.0 * dx),
+        (np.roll(f, -1, axis=1) - np.roll(f, 1, axis=1)) / (2.0 * dx),
+        (np.roll(f, -1, axis=2) - np.roll(f, 1, axis=2)) / (2.0 * dx),
+    )
+
+
+def extrap_to_face(f, f_dx, f_dy, f_dz, dx):
+    """quantum-gas-bh.py:196-209."""
+    f_XL = f + 0.5 * f_dx * dx
+    f_XR = np.roll(f - 0.5 * f_dx * dx, -1, axis=0)
+    f_YL = f + 0.5 * f_dy * dx
+    f_YR = np.roll(f - 0.5 * f_dy * dx, -1, axis=1)
+    f_ZL = f + 0.5 * f_dz * dx
+    f_ZR = np.roll(f - 0.5 * f_dz * dx, -1, axis=2)
+    return f_XL, f_XR, f_YL, f_YR, f_ZL, f_ZR
+
+
+def apply_fluxes(F, fX, fY, fZ, dx, dt):
+    """quantum-gas-bh.py:212-223."""
+    fac = dt * dx * dx
+    F = F + -fac * fX
+    F = F + fac * np.roll(fX, 1, axis=0)
+    F = F + -fac * fY
+    F = F + fac * np.roll(fY, 1, axis=1)
+    F = F + -fac * fZ
+    F = F + fac * np.roll(fZ, 1, axis=2)
+    return F
+
+
+def get_flux(rho_L, vx_L, vy_L, vz_L, rho_R, vx_R, vy_R, vz_R, cs):
+    """quantum-gas-bh.py:226-252: Rusanov flux evaluated on the averaged state."""
+    rho_star = 0.5 * (rho_L + rho_R)
+    momx_star = 0.5 * (rho_L * vx_L + rho_R * vx_R)
+    momy_star = 0.5 * (rho_L * vy_L + rho_R * vy_R)
+    momz_star = 0.5 * (rho_L * vz_L + rho_R * vz_R)
+    P_star = rho_star * cs * cs
+    flux_Mass = momx_star
+    flux_Momx = momx_star**2 / rho_star + P_star
+    flux_Momy = momx_star * momy_star / rho_star
+    flux_Momz = momx_star * momz_star / rho_star
+    C = np.maximum(cs + np.abs(vx_L), cs + np.abs(vx_R))
+    flux_Mass = flux_Mass - C * 0.5 * (rho_R - rho_L)
+    flux_Momx = flux_Momx - C * 0.5 * (rho_R * vx_R - rho_L * vx_L)
+    flux_Momy = flux_Momy - C * 0.5 * (rho_R * vy_R - rho_L * vy_L)
+    flux_Momz = flux_Momz - C * 0.5 * (rho_R * vz_R - rho_L * vz_L)
+    return flux_Mass, flux_Momx, flux_Momy, flux_Momz
+
+
+def _adjust_denominator(denom, eps=1.0e-12):
+    """quantum-gas-bh.py:353-357."""
+    return np.where(denom > 0, denom + eps, np.where(denom < 0, denom - eps, eps))
+
+
+def slope_limiter(f, dx, f_dx, f_dy, f_dz):
+    """quantum-gas-bh.py:340-395: two clamp01 ratios applied multiplicatively."""
+    out = []
+    for axis, fd in enumerate((f_dx, f_dy, f_dz)):
+        denom = _adjust_denominator(fd)
+        num = (f - np.roll(f, 1, axis=axis)) / dx
+        fd = np.maximum(0.0, np.minimum(1.0, num / denom)) * fd
+        num = -(f - np.roll(f, -1, axis=axis)) / dx
+        fd = np.maximum(0.0, np.minimum(1.0, num / denom)) * fd
+        out.append(fd)
+    return tuple(out)
+
+
+def solve_hydro(rho, vx, vy, vz, dt, dx, cs):
+    """quantum-gas-bh.py:269-337."""
+    vol = dx * dx * dx
+    rho_dx, rho_dy, rho_dz = get_gradient(rho, dx)
+    vx_dx, vx_dy, vx_dz = get_gradient(vx, dx)
+    vy_dx, vy_dy, vy_dz = get_gradient(vy, dx)
+    vz_dx, vz_dy, vz_dz = get_gradient(vz, dx)
+    rho_dx, rho_dy, rho_dz = slope_limiter(rho, dx, rho_dx, rho_dy, rho_dz)
+    vx_dx, vx_dy, vx_dz = slope_limiter(vx, dx, vx_dx, vx_dy, vx_dz)
+    vy_dx, vy_dy, vy_dz = slope_limiter(vy, dx, vy_dx, vy_dy, vy_dz)
+    vz_dx, vz_dy, vz_dz = slope_limiter(vz, dx, vz_dx, vz_dy, vz_dz)
+    rho_prime = rho - 0.5 * dt * (
+        vx * rho_dx + rho * vx_dx + vy * rho_dy + rho * vy_dy + vz * rho_dz
+        + rho * vz_dz
+    )
+    vx_prime = vx - 0.5 * dt * (
+        vx * vx_dx + vy * vx_dy + vz * vx_dz + (1.0 / rho) * rho_dx * cs * cs
+    )
+    vy_prime = vy - 0.5 * dt * (
+        vx * vy_dx + vy * vy_dy + vz * vy_dz + (1.0 / rho) * rho_dy * cs * cs
+    )
+    vz_prime = vz - 0.5 * dt * (
+        vx * vz_dx + vy * vz_dy + vz * vz_dz + (1.0 / rho) * rho_dz * cs * cs
+    )
+    r_XL, r_XR, r_YL, r_YR, r_ZL, r_ZR = extrap_to_face(rho_prime, rho_dx, rho_dy, rho_dz, dx)
+    x_XL, x_XR, x_YL, x_YR, x_ZL, x_ZR = extrap_to_face(vx_prime, vx_dx, vx_dy, vx_dz, dx)
+    y_XL, y_XR, y_YL, y_YR, y_ZL, y_ZR = extrap_to_face(vy_prime, vy_dx, vy_dy, vy_dz, dx)
+    z_XL, z_XR, z_YL, z_YR, z_ZL, z_ZR = extrap_to_face(vz_prime, vz_dx, vz_dy, vz_dz, dx)
+    fM_X, fPx_X, fPy_X, fPz_X = get_flux(r_XL, x_XL, y_XL, z_XL, r_XR, x_XR, y_XR, z_XR, cs)
+    fM_Y, fPy_Y, fPz_Y, fPx_Y = get_flux(r_YL, y_YL, z_YL, x_YL, r_YR, y_YR, z_YR, x_YR, cs)
+    fM_Z, fPz_Z, fPx_Z, fPy_Z = get_flux(r_ZL, z_ZL, x_ZL, y_ZL, r_ZR, z_ZR, x_ZR, y_ZR, cs)
+    Mass, Momx, Momy, Momz = get_conserved(rho, vx, vy, vz, vol)
+    Mass = apply_fluxes(Mass, fM_X, fM_Y, fM_Z, dx, dt)
+    Momx = apply_fluxes(Momx, fPx_X, fPx_Y, fPx_Z, dx, dt)
+    Momy = apply_fluxes(Momy, fPy_X, fPy_Y, fPy_Z, dx, dt)
+    Momz = apply_fluxes(Momz, fPz_X, fPz_Y, fPz_Z, dx, dt)
+    return get_primitive(Mass, Momx, Momy, Momz, vol)
+
+
+def apply_grav_accel(rho, vx, vy, vz, dt, g: Grid, p: Phys, k=None):
+    """quantum-gas-bh.py:255-266."""
+    ax, ay, az = grid_accelerations(rho, g, p, k)
+    return vx + ax * dt, vy + ay * dt, vz + az * dt
+
+
+# ---------------------------------------------------------------------------
+# R14: black-hole dark-matter accretion, quantum-gas-bh.py:497-530
+# ---------------------------------------------------------------------------
+
+
+def do_accretion(psi, pos, vel, m_bh, g: Grid, p: Phys, dt, sigma_v):
+    """quantum-gas-bh.py:497-530 (sigma_v = cs there, sigma in quantum-bh.py:319)."""
+    dxs = np.array([g.dx, g.dy, g.dz])
+    i = np.floor((pos - 0.5 * dxs) / dxs)
+    i = np.mod(i, np.array(g.shape)).astype(np.int64)
+    s = 0
+    psi = psi.copy()
+    psi_at_bh = psi[i[s, 0], i[s, 1], i[s, 2]]
+    psi_amp = np.abs(psi_at_bh)
+    psi_theta = np.angle(psi_at_bh)
+    v = np.sqrt(sigma_v**2 + vel[0, 0] ** 2 + vel[0, 1] ** 2 + vel[0, 2] ** 2)
+    xi = 2.0 * np.pi * p.G * m_bh[0] * p.m_per_hbar / v
+    dM_dt = (
+        32.0 * np.pi**2 * (p.G * m_bh[0]) ** 3 * p.m_per_hbar * psi_amp**2
+        / (p.c_light**3 * v * (1.0 - np.exp(-xi)))
+    )
+    new_psi_amp = np.abs(psi_amp) - np.sqrt(dM_dt * dt / g.vol)
+    psi[i[s, 0], i[s, 1], i[s, 2]] = new_psi_amp * np.exp(1.0j * psi_theta)
+    m_bh = m_bh + dM_dt * dt
+    return psi, m_bh
+
+
+# ---------------------------------------------------------------------------
+# R15: isothermal Bondi gas sink, quantum-fluid-accretion-test.py:404-494
+# ---------------------------------------------------------------------------
+
+LAMBDA_ISO = math.exp(1.5) / 4.0
+
+
+def bondi_sink(rho, M_bh, x_bh, dx, Lx, cs, G, dt, r_acc_mult=4.0,
+               lam=LAMBDA_ISO, fmax=0.25):
+    """quantum-fluid-accretion-test.py:454-494 (v_rel = 0)."""
+    nx = rho.shape[0]
+    r_B = G * M_bh / (cs * cs)
+    r_acc = r_acc_mult * dx
+    rK = np.clip(r_B, 0.25 * dx, 0.5 * r_acc)
+    xs = (np.arange(nx) + 0.5) * dx
+
+    def pdelta(x0):
+        d = np.abs(xs - x0)
+        return np.minimum(d, Lx - d)
+
+    dX, dY, dZ = np.meshgrid(pdelta(x_bh[0]), pdelta(x_bh[1]), pdelta(x_bh[2]), indexing="ij")
+    R2 = dX * dX + dY * dY + dZ * dZ
+    mask = R2 <= r_acc * r_acc
+    W = np.exp(-0.5 * R2 / (rK * rK)) * mask
+    sumW = np.sum(W) + 1e-30
+    rho_inf = np.sum(W * rho) / sumW
+    dMdt = 4.0 * np.pi * lam * (G * M_bh) ** 2 * rho_inf / (cs**3)
+    dM = dMdt * dt
+    WRho = W * rho
+    sumWRho = np.sum(WRho) + 1e-30
+    phi = WRho / sumWRho
+    M_avail = np.sum(rho * mask) * (dx**3)
+    dM_cap = min(dM, fmax * M_avail)
+    rho_new = np.maximum(0.0, rho - (dM_cap / (dx**3)) * phi)
+    return rho_new, M_bh + dM_cap, dMdt, rho_inf, r_B, dM_cap
+
+
+# ---------------------------------------------------------------------------
+# R16: the gas + black-hole step, quantum-gas-bh.py:537-578
+# ---------------------------------------------------------------------------
+
+
+def gasbh_compute_step(psi, rho, vx, vy, vz, m_bh, pos, vel, t, g: Grid, p: Phys,
+                       dt, k=None, bondi_r_acc_mult=None, dm_accretion=True):
+    """quantum-gas-bh.py:537-578.
+
+    With ``bondi_r_acc_mult`` set, the isothermal Bondi gas sink of
+    quantum-fluid-accretion-test.py:534-536 is applied after the hydro and
+    black-hole drift, before the second half kick."""
+    if k is None:
+        k = kgrid(g)
+    L = np.array([g.Lx, g.Ly, g.Lz])
+    # (1/2) kick
+    rho_bh = bin_stars(pos, g, m_bh)
+    rho_tot = np.abs(psi) ** 2 + rho_bh + rho
+    V = get_potential(rho_tot, g, p, k)
+    psi = kick(psi, V, p, dt)
+    vx, vy, vz = apply_grav_accel(rho_tot, vx, vy, vz, dt / 2.0, g, p, k)
+    acc, _ = get_acceleration(pos, rho_tot, g, p, k)
+    vel = vel + acc * dt / 2.0
+    # drift
+    psi = drift(psi, g, p, dt, k)
+    rho, vx, vy, vz = solve_hydro(rho, vx, vy, vz, dt, g.dx, p.cs)
+    pos = pos + vel * dt
+    pos = ref_mod(pos, L)
+    if bondi_r_acc_mult is not None:
+        rho, M_new, *_ = bondi_sink(rho, m_bh[0], pos[0], g.dx, g.Lx, p.cs, p.G, dt,
+                                    r_acc_mult=bondi_r_acc_mult)
+        m_bh = np.array([M_new] + list(m_bh[1:]))
+    # (1/2) kick
+    rho_bh = bin_stars(pos, g, m_bh)
+    rho_tot = np.abs(psi) ** 2 + rho_bh + rho
+    V = get_potential(rho_tot, g, p, k)
+    psi = kick(psi, V, p, dt)
+    vx, vy, vz = apply_grav_accel(rho_tot, vx, vy, vz, dt / 2.0, g, p, k)
+    acc, _ = get_acceleration(pos, rho_tot, g, p, k)
+    vel = vel + acc * dt / 2.0
+    # accretion
+    if dm_accretion:
+        psi, m_bh = do_accretion(psi, pos, vel, m_bh, g, p, dt, p.cs)
+    return psi, rho, vx, vy, vz, m_bh, pos, vel, t + dt
+
+
+# ---------------------------------------------------------------------------
+# float32 star deposit in the reference's exact operation order
+# ---------------------------------------------------------------------------
+
+
+def cic_weights_f32(pos32, g: Grid):
+    """quantum-stars.py:200-209 evaluated in float32 like the x64-off reference.
+
+    dxs is float32(dx); every operation rounds to float32 in the written order
+    (no fused multiply-add)."""
+    f = np.float32
+    pos32 = np.asarray(pos32, dtype=np.float32)
+    dxs = np.array([g.dx, g.dy, g.dz], dtype=np.float32)
+    half = f(0.5)
+    i = np.floor((pos32 - half * dxs) / dxs)
+    ip1 = i + f(1.0)
+    w_i = ((ip1 + half) * dxs - pos32) / dxs
+    w_ip1 = (pos32 - (i + half) * dxs) / dxs
+    n = np.array(g.shape, dtype=np.float32)
+    ii = np.mod(i, n).astype(np.int64)
+    ip = np.mod(ip1, n).astype(np.int64)
+    return ii, ip, w_i.astype(np.float32), w_ip1.astype(np.float32)
+
+
+def bin_stars_f32(pos32, g: Grid, m_s):
+    """Sequential float32 deposit, stars in order, corners in the order of
+    quantum-stars.py:220-243; each cell accumulates from 0 in that order.
+    fac = float32(m_s / (dx dy dz)) as the weak-typed Python scalar becomes."""
+    ii, ip, w_i, w_ip1 = cic_weights_f32(pos32, g)
+    fac = np.float32(m_s / (g.dx * g.dy * g.dz))
+    rho = np.zeros(g.shape, dtype=np.float32)
+    idx = (ii, ip)
+    w = (w_i, w_ip1)
+    for s in range(ii.shape[0]):
+        for c in CORNERS:
+            v = np.float32(np.float32(np.float32(w[c[0]][s, 0] * w[c[1]][s, 1])
+                                      * w[c[2]][s, 2]) * fac)
+            cell = (idx[c[0]][s, 0], idx[c[1]][s, 1], idx[c[2]][s, 2])
+            rho[cell] = np.float32(rho[cell] + v)
+    return rho
+
+
+# ---------------------------------------------------------------------------
+# Seeded initial conditions (the benchmark IC family)
+# ---------------------------------------------------------------------------
+
+
+def delta_field(n, seed, shape=None):
+    """Unit-variance Gaussian random field with P(k) ~ k^-3 for
+    0 < |k| <= k_Nyq/2 (zero elsewhere, k=0 included), float64."""
+    shape = shape or (n, n, n)
+    rng = np.random.default_rng(seed)
+    w = rng.standard_normal(shape)
+    kk = np.meshgrid(*[np.fft.fftfreq(m) * m for m in shape], indexing="ij")
+    kmag = np.sqrt(sum(k**2 for k in kk))
+    knyq = min(shape) / 2.0
+    amp = np.zeros(shape)
+    sel = (kmag > 0) & (kmag <= knyq / 2.0)
+    amp[sel] = kmag[sel] ** -1.5
+    d = np.real(np.fft.ifftn(np.fft.fftn(w) * amp))
+    d -= d.mean()
+    d /= d.std()
+    return d
+
+
+def stars_ic(n, n_s, seed=0, shape=None, L=(1.0, 1.0, 1.0), star_frac=0.1):
+    """psi = sqrt(1 + 0.1 delta), theta = 0; n_s uniform stars at rest with
+    total mass star_frac of the dark-matter box mass.  Returns
+    (psi complex128, pos, vel, Grid, Phys)."""
+    shape = shape or (n, n, n)
+    g = Grid(*shape, *L)
+    rho_dm = 1.0 + 0.1 * delta_field(n, seed, shape)
+    psi = np.sqrt(rho_dm).astype(np.complex128)
+    rng = np.random.default_rng(seed + 1)
+    pos = rng.uniform(0.0, 1.0, (n_s, 3)) * np.array(L)
+    vel = np.zeros((n_s, 3))
+    M_dm = rho_dm.sum() * g.vol
+    M_s = star_frac * M_dm
+    Lvol = L[0] * L[1] * L[2]
+    p = Phys(m_per_hbar=1.0, G=1.0 / (4.0 * np.pi),
+             rho_bar=rho_dm.mean() + M_s / Lvol,
+             m_s=(M_s / n_s) if n_s else 0.0)
+    return psi, pos, vel, g, p
+
+
+def default_dt(g: Grid, p: Phys):
+    """dt = dx^2/6 for m/hbar = 1 (quantum-stars.py:153 with a cubic cell)."""
+    return p.m_per_hbar / 6.0 * (g.dx * g.dy * g.dz) ** (2.0 / 3.0)
+
+
+def rel_l2(a, b):
+    a = np.asarray(a)
+    b = np.asarray(b)
+    return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))
