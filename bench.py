@@ -1,0 +1,401 @@
+#!/usr/bin/env python
+"""Benchmark: kick-drift-kick cell-steps/s of the quantum-jax stars step.
+
+Workload (one B200): periodic box L=1, 256^3 complex64 psi = sqrt(1 + 0.1 delta)
+(delta: seeded Gaussian field, P(k) ~ k^-3 cut at k_Nyq/2, unit variance),
+4096 equal-mass stars (10 % of the dark-matter mass) uniform at rest,
+hbar/m = 1, 4 pi G = 1, dt = dx^2/6.  Synthetic seeded data (no dataset).
+
+A step is one KDK step (quantum-stars.py:295-330); K steps run as one
+qj_kdk_step call (the fori_loop of quantum-stars.py:454).  psi is 128 MiB,
+larger than L2 (126 MB), so no explicit flush is needed between steps.
+
+Printed (one JSON line on rank 0): value = fused float32 cell-steps/s over all
+ranks (device time, CUDA events, max over ranks); the plain float64 GPU path's
+rate; psi / rho rel-L2 of the fused path against the float64 path after the
+same steps; e2e through the public API with host buffers; the roofline of the
+dominant pass; the CPU baseline (the float64 NumPy oracle on the host cores);
+SM clocks sampled during the timed region.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl qj|reference]
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for _p in (ROOT, os.path.join(ROOT, "quantum-jax_b200")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "KDK cell-steps/s at 256^3 (fused FP32; plain FP64 and psi rel-L2 reported)"
+UNIT = "cell-steps/s"
+# Algorithmic HBM bytes per cell of each fused pass (complex64 fields: each
+# input read once, each output written once).
+PASS_NAMES = ["density", "fft_y", "poisson", "ifft2_y", "kick_drift", "drift_y",
+              "drift_density", "deposit_sort", "particles"]
+PASS_BYTES = {0: 16, 1: 16, 2: 24, 3: 32, 4: 32, 5: 16, 6: 24}
+STEP_BYTES = 144  # per cell per steady-state step: passes 1..6 once each
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="qj", choices=["qj", "reference"])
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--stars", type=int, default=4096)
+    ap.add_argument("--err-steps", type=int, default=None,
+                    help="steps of the fused-vs-float64 error check (default: --steps)")
+    ap.add_argument("--plain-steps", type=int, default=10)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--e2e-sub", type=int, default=10,
+                    help="steps per public-API call in the e2e leg (the reference's nt_sub)")
+    return ap.parse_args()
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """dram bytes per launch of each pass from the committed ncu summary."""
+    out = {}
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("traffic_bytes_per_launch["):
+                    k, v = line.split("=", 1)
+                    out[k[len("traffic_bytes_per_launch["):-1]] = float(v)
+    except OSError:
+        pass
+    return out
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_ic(n, n_s):
+    from oracle import oracle as O
+
+    psi, pos, vel, g, p = O.stars_ic(n, n_s, seed=0)
+    return psi, pos, vel, g, p, O.default_dt(g, p)
+
+
+def cpu_baseline(n, n_s, steps=2):
+    """The float64 NumPy oracle on the host cores (scipy.fft workers = all)."""
+    import numpy as np
+
+    from oracle import oracle as O
+
+    O.WORKERS = os.cpu_count() or 1
+    psi, pos, vel, g, p, dt = make_ic(n, n_s)
+    k = O.kgrid(g)
+    state = (psi, pos, vel, 0.0, 0.0, dt)
+    state = O.stars_compute_step(*state, g, p, dt, k)  # warm-up
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        state = O.stars_compute_step(*state, g, p, dt, k)
+    el = time.perf_counter() - t0
+    assert np.isfinite(state[0]).all()
+    return {"value": g.ncell * steps / el, "unit": UNIT, "cores": O.WORKERS, "kind": "port",
+            "sample": f"{steps} timed steps (after 1 warm-up) of the {n}^3, {n_s}-star "
+                      f"workload; float64 NumPy/SciPy restatement of quantum-stars.py:295-330 "
+                      f"(reference JAX is not installable)",
+            "s_per_step": el / steps}
+
+
+def run_reference(a, rank):
+    if rank != 0:
+        return
+    steps = max(1, min(a.steps, 3))
+    cb = cpu_baseline(a.n, a.stars, steps)
+    line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT,
+            "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": cb["s_per_step"] * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"stars KDK {a.n}^3 complex, {a.stars} stars",
+                       "grid": [a.n] * 3, "n_stars": a.stars, "l2_flush": "inputs > L2"},
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    a = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if a.impl == "reference":
+        run_reference(a, rank)
+        return
+
+    import numpy as np
+    import torch
+
+    import qj
+    from oracle import oracle as O
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=dev)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    n, n_s = a.n, a.stars
+    psi0, pos0, vel0, g, p, dt = make_ic(n, n_s)
+    C = g.ncell
+    grid = qj.Grid(n, n, n)
+    phys = qj.Phys(m_per_hbar=1.0, G=p.G, rho_bar=p.rho_bar)
+
+    def fresh(precision):
+        ct = torch.complex64 if precision == qj.FUSED_F32 else torch.complex128
+        rt = torch.float32 if precision == qj.FUSED_F32 else torch.float64
+        ps = torch.as_tensor(psi0, dtype=ct, device=dev)
+        po = torch.as_tensor(pos0, dtype=rt, device=dev)
+        ve = torch.as_tensor(vel0, dtype=rt, device=dev)
+        diag = torch.tensor([0.0, 0.0, dt], dtype=torch.float64, device=dev)
+        return ps, po, ve, diag
+
+    lib = qj.lib()
+    stream = torch.cuda.current_stream()
+
+    # ---------------- fused float32: device-timed ----------------
+    fused = qj.Plan(grid, phys, qj.FUSED_F32, n_s)
+    ps, po, ve, diag = fresh(qj.FUSED_F32)
+    fused.kdk_step(ps, po, ve, diag, dt, a.warmup, p.m_s)
+    barrier()
+    clocks = Clocks(local)
+    clocks.start()
+    time.sleep(0.3)
+    lib.qj_profile_enable(1)
+    l0 = lib.qj_launch_count()
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    fused.kdk_step(ps, po, ve, diag, dt, a.steps, p.m_s)
+    e1.record(stream)
+    barrier()
+    launches = int(lib.qj_launch_count() - l0)
+    ms = e0.elapsed_time(e1)
+    clk = clocks.stop()
+    import ctypes
+
+    pms = (ctypes.c_double * 9)()
+    pcnt = (ctypes.c_int64 * 9)()
+    lib.qj_profile_read(pms, pcnt, 9)
+    lib.qj_profile_enable(0)
+    ms_max = max_over_ranks(ms)
+    value = world * C * a.steps / (ms_max * 1e-3)
+
+    # roofline of the dominant pass
+    hbm, hbm_kind = peaks()
+    per_pass = {}
+    for b in range(9):
+        if pcnt[b]:
+            per_pass[PASS_NAMES[b]] = {"launches": int(pcnt[b]), "total_ms": pms[b],
+                                       "avg_us": 1e3 * pms[b] / pcnt[b]}
+    dom = max((b for b in PASS_BYTES if pcnt[b]), key=lambda b: pms[b])
+    avg_s = pms[dom] / pcnt[dom] * 1e-3
+    achieved = PASS_BYTES[dom] * C / avg_s / 1e9
+    tr = ncu_traffic().get(PASS_NAMES[dom])
+    roofline = {"bound": "hbm", "kernel": PASS_NAMES[dom], "achieved": achieved, "peak": hbm,
+                "peak_kind": hbm_kind, "unit": "GB/s", "frac": achieved / hbm,
+                "traffic": tr, "alg_bytes_per_launch": PASS_BYTES[dom] * C}
+    step_bw = STEP_BYTES * C * a.steps / (ms * 1e-3) / 1e9
+    step_roof = {"alg_bytes_per_cell_step": STEP_BYTES, "achieved_gbs": step_bw,
+                 "frac": step_bw / hbm}
+
+    # ---------------- plain float64 rate ----------------
+    plain = qj.Plan(grid, phys, qj.PLAIN_F64, n_s)
+    qs, qo, qv, qd = fresh(qj.PLAIN_F64)
+    plain.kdk_step(qs, qo, qv, qd, dt, 1, p.m_s)
+    barrier()
+    e0.record(stream)
+    plain.kdk_step(qs, qo, qv, qd, dt, a.plain_steps, p.m_s)
+    e1.record(stream)
+    barrier()
+    pl_ms = max_over_ranks(e0.elapsed_time(e1))
+    plain_value = world * C * a.plain_steps / (pl_ms * 1e-3)
+
+    # ---------------- accuracy: fused vs float64 after the same steps --------
+    err_steps = a.err_steps if a.err_steps is not None else a.steps
+    ps, po, ve, diag = fresh(qj.FUSED_F32)
+    qs, qo, qv, qd = fresh(qj.PLAIN_F64)
+    mass0 = float((qs.abs() ** 2).sum())
+    fused.kdk_step(ps, po, ve, diag, dt, err_steps, p.m_s)
+    plain.kdk_step(qs, qo, qv, qd, dt, err_steps, p.m_s)
+    torch.cuda.synchronize()
+    psi_err = float(torch.linalg.vector_norm(ps.to(torch.complex128) - qs) /
+                    torch.linalg.vector_norm(qs))
+    rf, rp = ps.abs().double() ** 2, qs.abs() ** 2
+    rho_err = float(torch.linalg.vector_norm(rf - rp) / torch.linalg.vector_norm(rp))
+    mass_drift = float(rf.sum()) / mass0 - 1.0
+    pos_err = float(torch.linalg.vector_norm(po.double() - qo) / torch.linalg.vector_norm(qo))
+    del qs, qo, qv, qd
+    plain.close()
+
+    # ---------------- e2e through the public API with host buffers ----------
+    e2e = None
+    if not a.no_e2e:
+        sub = a.e2e_sub
+        h_psi = torch.as_tensor(psi0, dtype=torch.complex64).pin_memory()
+        h_pos = torch.as_tensor(pos0, dtype=torch.float32).pin_memory()
+        h_vel = torch.as_tensor(vel0, dtype=torch.float32).pin_memory()
+        o_psi = torch.empty_like(h_psi).pin_memory()
+        o_pos = torch.empty_like(h_pos).pin_memory()
+        o_vel = torch.empty_like(h_vel).pin_memory()
+        o_diag = torch.empty(3, dtype=torch.float64).pin_memory()
+        step = qj.StarsStep(grid, phys, p.m_s, dt, n_s)
+        d_psi = torch.empty(h_psi.shape, dtype=torch.complex64, device=dev)
+        d_pos = torch.empty(h_pos.shape, dtype=torch.float32, device=dev)
+        d_vel = torch.empty(h_vel.shape, dtype=torch.float32, device=dev)
+        d_diag = torch.tensor([0.0, 0.0, dt], dtype=torch.float64, device=dev)
+
+        def e2e_call():
+            d_psi.copy_(h_psi, non_blocking=True)
+            d_pos.copy_(h_pos, non_blocking=True)
+            d_vel.copy_(h_vel, non_blocking=True)
+            step.plan.kdk_step(d_psi, d_pos, d_vel, d_diag, dt, sub, p.m_s)
+            o_psi.copy_(d_psi, non_blocking=True)
+            o_pos.copy_(d_pos, non_blocking=True)
+            o_vel.copy_(d_vel, non_blocking=True)
+            o_diag.copy_(d_diag, non_blocking=True)
+
+        e2e_call()
+        barrier()
+        calls = max(1, a.steps // sub)
+        e0.record(stream)
+        for _ in range(calls):
+            e2e_call()
+        e1.record(stream)
+        barrier()
+        e_ms = max_over_ranks(e0.elapsed_time(e1))
+        h2d = h_psi.numel() * 8 + h_pos.numel() * 4 + h_vel.numel() * 4
+        d2h = h2d + 24
+        e2e = {"value": world * C * sub * calls / (e_ms * 1e-3), "unit": UNIT,
+               "h2d_bytes_per_step": h2d / sub, "d2h_bytes_per_step": d2h / sub,
+               "unit_of_call": f"one public-API call = host->device psi/pos/vel, {sub} KDK "
+                               f"steps, device->host psi/pos/vel/diag (the reference's "
+                               f"host-sync interval nt_sub)"}
+        step.plan.close()
+
+    cb = None
+    if rank == 0 and world == 1 and not a.no_cpu:
+        cb = cpu_baseline(n, n_s, 2)
+        cb = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+                "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_max / a.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "c64/f32 (phases, k=0 mode, mean density in f64)",
+                "data": "synthetic (seeded Gaussian random field, uniform stars)",
+                "config": {"workload": f"stars KDK {n}^3 complex64, {n_s} stars, one box per "
+                                       f"GPU (replicas)", "grid": [n, n, n], "n_stars": n_s,
+                           "dt": dt, "l2_flush": "inputs larger than L2 (psi 128 MiB)",
+                           "parallelism": f"replicas x{world}"},
+                "plain_f64": {"value": plain_value, "ms_per_step": pl_ms / a.plain_steps,
+                              "steps": a.plain_steps},
+                "fused_over_plain": value / plain_value,
+                "accuracy": {"steps": err_steps, "psi_rel_l2_vs_f64": psi_err,
+                             "rho_rel_l2_vs_f64": rho_err, "mass_drift": mass_drift,
+                             "pos_rel_l2_vs_f64": pos_err,
+                             "f64_path": "plain float64 GPU path (matches the oracle to 1e-11)"},
+                "roofline": roofline, "step_roofline": step_roof, "passes": per_pass,
+                "gpu_launches": launches, "clocks": clk, "e2e": e2e, "cpu_baseline": cb}
+        print(json.dumps(line), flush=True)
+    fused.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,140 @@
+/*
+ * qj.h -- C ABI of libqj, the B200 (sm_100a) implementation of quantum-jax's
+ * kick-drift-kick Schroedinger-Poisson step.
+ *
+ * The reference (pmocz/quantum-jax) has no native interface: its boundary is
+ * the Python signature of the per-script functions that a jitted fori_loop
+ * calls, with every physical constant captured from module globals.  Each
+ * entry point below replaces one of those functions; the constants travel in
+ * a plan.  Paths are the reference's files.
+ *
+ * Conventions
+ *  - Arrays are C-order [nx][ny][nz] (z fastest), as built by the reference's
+ *    meshgrid(..., indexing="ij") (quantum-stars.py:139,145).
+ *  - Precision QJ_PLAIN_F64: psi complex128, real fields / particles float64.
+ *    Precision QJ_FUSED_F32: psi complex64, real fields / particles float32
+ *    (phase arguments, the k=0 mode, mean density and reductions in FP64).
+ *  - Particle arrays are [n][3] (x, y, z), like the reference's pos / vel.
+ *  - All pointers are device pointers unless stated otherwise.  Every call is
+ *    asynchronous on `stream` (a cudaStream_t; NULL = legacy default stream).
+ *  - Status: 0 on success, a QJ_ERR_* code otherwise; qj_last_error() gives a
+ *    thread-local message.  No call aborts, exits or traps on the device.
+ *  - A plan is not safe for concurrent use from several streams; make one
+ *    plan per stream.  The plan owns its device workspace and tables.
+ */
+#ifndef QJ_H
+#define QJ_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define QJ_OK 0
+#define QJ_ERR_ARG 1       /* invalid argument / unsupported size */
+#define QJ_ERR_CUDA 2      /* a CUDA runtime call failed */
+#define QJ_ERR_NONFINITE 3 /* non-finite value detected in the state */
+#define QJ_ERR_TIMEOUT 4   /* a bounded device wait gave up */
+#define QJ_ERR_ALLOC 5     /* device allocation failed */
+
+#define QJ_PLAIN_F64 0 /* unfused float64 kernels, op for op with the reference */
+#define QJ_FUSED_F32 1 /* fused pencil-pass kernels, complex64 bulk */
+
+typedef struct qj_plan qj_plan;
+
+/* Grid: quantum-stars.py:73-80 (nx, ny, nz, Lx, Ly, Lz). */
+typedef struct qj_grid {
+  int32_t nx, ny, nz;
+  double Lx, Ly, Lz;
+} qj_grid;
+
+/* Physical constants the reference reads from module globals:
+ * m_per_hbar (quantum-stars.py:109), G (:103), rho_bar (:83 or set in main,
+ * quantum-gas-bh.py:680-681), b_coeff (:117-125; 0 disables the
+ * self-interaction term), cs (quantum-gas-bh.py:74), c_light (:86). */
+typedef struct qj_phys {
+  double m_per_hbar;
+  double G;
+  double rho_bar;
+  double b_coeff;
+  double cs;
+  double c_light;
+} qj_phys;
+
+/* The scalar part of the stars state dict (quantum-stars.py:434-440):
+ * t, a_max, dt_s.  Lives in DEVICE memory; qj_kdk_step updates it in place. */
+typedef struct qj_diag {
+  double t;
+  double a_max;
+  double dt_s;
+} qj_diag;
+
+/* Create / destroy a plan.  Replaces the module-level set-up of
+ * quantum-stars.py:61-157 (grid, k-grid, constants).  Supported lengths per
+ * axis: 16, 32, 64, 128, 256, 512; nz must be a multiple of 16.
+ * max_particles bounds n_s of later calls (workspace is sized for it). */
+int qj_plan_create(qj_plan **plan, const qj_grid *grid, const qj_phys *phys,
+                   int precision, int max_particles);
+int qj_plan_destroy(qj_plan *plan);
+/* Update rho_bar / b_coeff / G / m_per_hbar / cs of an existing plan. */
+int qj_plan_set_phys(qj_plan *plan, const qj_phys *phys);
+
+/* Thread-local message of the last failing call on this thread. */
+const char *qj_last_error(void);
+
+/* get_potential(rho) -> V.  quantum-stars.py:189-193 (also gas-bh :159-163,
+ * tidal :168-172, cosmo :142-146).  rho, V: real [nx][ny][nz] of the plan's
+ * real type.  self_interaction != 0 adds b_coeff * rho (:193). */
+int qj_get_potential(qj_plan *plan, const void *rho, void *V,
+                     int self_interaction, void *stream);
+
+/* bin_stars(pos) -> rho_s.  quantum-stars.py:212-247 / bin_particles
+ * quantum-gas-bh.py:414-449.  masses: per-particle mass array [n] (device,
+ * real type) or NULL to use m_s for every particle.  Deterministic: each
+ * cell sums its contributions in (particle, corner) order, like the
+ * reference's sequential fori_loop. */
+int qj_bin_stars(qj_plan *plan, const void *pos, int n, double m_s,
+                 const void *masses, void *rho_s, void *stream);
+
+/* get_acceleration(pos, rho) -> (acc [n][3], a_max).  quantum-stars.py:250-288.
+ * a_max: device pointer to one double. */
+int qj_get_acceleration(qj_plan *plan, const void *pos, int n, const void *rho,
+                        void *acc, double *a_max, void *stream);
+
+/* nsteps x compute_step(psi, pos, vel, t, a_max, dt_s), quantum-stars.py:295-330
+ * (the body of `update`, :333-351, iterated like fori_loop at :454).
+ * psi, pos, vel and diag are updated in place.  n_s may be 0 (no stars).
+ * self_interaction as in qj_get_potential.  v_ext: optional static external
+ * potential [nx][ny][nz] (real type) added to V at each kick
+ * (quantum-tidal.py:191,201); NULL for none. */
+int qj_kdk_step(qj_plan *plan, void *psi, void *pos, void *vel, int n_s,
+                double m_s, double dt, int nsteps, int self_interaction,
+                const void *v_ext, qj_diag *diag, void *stream);
+
+/* 3-D FFT of a complex [nx][ny][nz] array with the plan's pencil kernels
+ * (direction -1 forward, unnormalised; +1 inverse, scaled by 1/(nx ny nz)),
+ * i.e. jnp.fft.fftn / ifftn as called at quantum-stars.py:191-192,307-309.
+ * in == out is allowed. */
+int qj_fft3d(qj_plan *plan, const void *in, void *out, int direction,
+             void *stream);
+
+/* Bytes of device workspace the plan holds. */
+int64_t qj_plan_workspace_bytes(const qj_plan *plan);
+
+/* Instrumentation (no reference counterpart; used by the benchmark).
+ * qj_launch_count: kernels libqj has launched in this process.
+ * qj_profile_enable(1) clears and starts per-pass CUDA-event timing;
+ * qj_profile_read fills ms[b] / count[b] for buckets b < nbuckets
+ * (0 density, 1 forward FFT, 2 Poisson, 3 inverse FFT, 4 kick, 5 drift,
+ * 6 drift + density, 7 deposit sort, 8 particle gather / update); it waits
+ * for the recorded events. */
+int64_t qj_launch_count(void);
+int qj_profile_enable(int on);
+int qj_profile_read(double *ms, int64_t *count, int nbuckets);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QJ_H */

@@ -1,0 +1,705 @@
+// libqj C ABI: plans, the kick-drift-kick step (fused float32 and plain
+// float64 forms) and the standalone operators.  See include/qj.h.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/qj.h"
+#include "qj_internal.h"
+
+namespace qj {
+
+static thread_local std::string g_err;
+
+void set_error(const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+}
+
+std::atomic<long long> g_launches{0};
+
+// ----- per-pass event timing -----
+namespace {
+struct Prof {
+  std::mutex mu;
+  bool on = false;
+  std::vector<cudaEvent_t> pool;
+  struct Mark {
+    int bucket;
+    cudaEvent_t a, b;
+  };
+  std::vector<Mark> marks;
+  cudaEvent_t pending = nullptr;
+  cudaEvent_t get() {
+    if (!pool.empty()) {
+      cudaEvent_t e = pool.back();
+      pool.pop_back();
+      return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+  }
+};
+Prof &prof() {
+  static Prof p;
+  return p;
+}
+}  // namespace
+
+bool prof_on() { return prof().on; }
+void prof_mark_begin(cudaStream_t st) {
+  Prof &p = prof();
+  std::lock_guard<std::mutex> g(p.mu);
+  p.pending = p.get();
+  cudaEventRecord(p.pending, st);
+}
+void prof_mark_end(int bucket, cudaStream_t st) {
+  Prof &p = prof();
+  std::lock_guard<std::mutex> g(p.mu);
+  cudaEvent_t b = p.get();
+  cudaEventRecord(b, st);
+  p.marks.push_back({bucket, p.pending, b});
+  p.pending = nullptr;
+}
+
+int cuda_fail(cudaError_t e, const char *what, const char *file, int line) {
+  set_error("CUDA error %d (%s) in %s at %s:%d", (int)e, cudaGetErrorString(e), what, file, line);
+  return e == cudaErrorMemoryAllocation ? QJ_ERR_ALLOC : QJ_ERR_CUDA;
+}
+
+// Drift propagator of each axis, float64 phase, rounded once:
+// prop_a[i] = exp(-1j * dt_kin * k_a[i]^2 / (2 m_per_hbar)) / n_a
+// (the separable factor of quantum-stars.py:308, with the 1/n_a of ifftn).
+__global__ void k_prop_tables(float2 *p0, float2 *p1, float2 *p2, const double *k0,
+                              const double *k1, const double *k2, int n0, int n1, int n2,
+                              double dtk, double mph) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  float2 *P[3] = {p0, p1, p2};
+  const double *K[3] = {k0, k1, k2};
+  const int N[3] = {n0, n1, n2};
+  for (int a = 0; a < 3; ++a) {
+    if (i < N[a]) {
+      const double th = -dtk * K[a][i] * K[a][i] / (2.0 * mph);
+      double s, c;
+      sincos(th, &s, &c);
+      P[a][i] = float2{(float)(c / N[a]), (float)(s / N[a])};
+    }
+  }
+}
+
+}  // namespace qj
+
+using namespace qj;
+
+struct qj_plan {
+  qj_grid g;
+  qj_phys ph;
+  int prec;
+  bool dbl;
+  int max_particles;
+  int n[3];
+  long long ncell;
+  size_t rsz, csz;  // bytes of one real / complex element
+  std::vector<void *> allocs;
+  int64_t ws_bytes = 0;
+  // tables
+  void *tw[3] = {nullptr, nullptr, nullptr};  // float2 / double2
+  double *kd[3] = {nullptr, nullptr, nullptr};
+  float *kf[3] = {nullptr, nullptr, nullptr};
+  float *ktf[3] = {nullptr, nullptr, nullptr};
+  void *kr[3] = {nullptr, nullptr, nullptr};  // k tables of the real type
+  float2 *prop[3] = {nullptr, nullptr, nullptr};
+  double prop_dtk = NAN;
+  // fused workspace
+  float2 *R = nullptr, *S1 = nullptr, *S2 = nullptr;
+  double *part = nullptr;
+  // plain / standalone workspace (lazy for fused plans)
+  void *c0 = nullptr, *c1 = nullptr;
+  void *rho_tot = nullptr, *V = nullptr, *ax = nullptr, *ay = nullptr, *az = nullptr,
+       *rho_s = nullptr;
+  // particles
+  unsigned *keys = nullptr, *kA = nullptr, *iA = nullptr, *kB = nullptr, *iB = nullptr,
+           *ukey = nullptr, *cell_u = nullptr;
+  void *vals = nullptr, *uval = nullptr, *A = nullptr, *acc = nullptr;
+  int *pstart = nullptr;
+  int *n_unique = nullptr;
+  void *amax = nullptr, *dts = nullptr;  // real type scalars
+  void *tmp_scalar = nullptr;
+};
+
+namespace {
+
+int dev_alloc(qj_plan *P, void **p, size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    return cuda_fail(e, "cudaMalloc", __FILE__, __LINE__);
+  }
+  P->allocs.push_back(*p);
+  P->ws_bytes += (int64_t)bytes;
+  return 0;
+}
+
+template <typename T> int dev_alloc_t(qj_plan *P, T **p, size_t count) {
+  return dev_alloc(P, (void **)p, count * sizeof(T));
+}
+
+#define QJ_TRY(x)             \
+  do {                        \
+    int rc_ = (x);            \
+    if (rc_) return rc_;      \
+  } while (0)
+
+CicGeomD geom(const qj_plan *P) {
+  CicGeomD g;
+  g.n[0] = P->g.nx;
+  g.n[1] = P->g.ny;
+  g.n[2] = P->g.nz;
+  g.d[0] = P->g.Lx / P->g.nx;
+  g.d[1] = P->g.Ly / P->g.ny;
+  g.d[2] = P->g.Lz / P->g.nz;
+  g.L[0] = P->g.Lx;
+  g.L[1] = P->g.Ly;
+  g.L[2] = P->g.Lz;
+  g.vol = g.d[0] * g.d[1] * g.d[2];
+  return g;
+}
+
+KTabs ktabs(const qj_plan *P) {
+  KTabs k;
+  for (int a = 0; a < 3; ++a) {
+    k.k[a] = P->kr[a];
+    k.n[a] = P->n[a];
+  }
+  return k;
+}
+
+int ensure_plain_ws(qj_plan *P) {
+  if (P->c0) return 0;
+  QJ_TRY(dev_alloc(P, &P->c0, P->ncell * P->csz));
+  QJ_TRY(dev_alloc(P, &P->c1, P->ncell * P->csz));
+  for (void **f : {&P->rho_tot, &P->V, &P->ax, &P->ay, &P->az, &P->rho_s})
+    QJ_TRY(dev_alloc(P, f, P->ncell * P->rsz));
+  return 0;
+}
+
+FftArgs fft_args(const qj_plan *P, int axis, void *data, double scale) {
+  FftArgs a;
+  a.nx = P->n[0];
+  a.ny = P->n[1];
+  a.nz = P->n[2];
+  a.axis = axis;
+  a.stride = axis == 0 ? (long long)P->n[1] * P->n[2] : (axis == 1 ? P->n[2] : 1);
+  a.outer_stride = axis == 0 ? P->n[2] : (long long)P->n[1] * P->n[2];
+  a.ztiles = P->n[2] / 16;
+  a.data = data;
+  a.tw = P->tw[axis];
+  a.scale = scale;
+  return a;
+}
+
+// jnp.fft.fftn (dir -1) / ifftn (dir +1) in place, axes z, y, x.
+int fft3d(qj_plan *P, void *data, int dir, cudaStream_t st) {
+  for (int axis = 2; axis >= 0; --axis) {
+    const double scale = dir > 0 ? 1.0 / P->n[axis] : 1.0;
+    QJ_TRY(launch_fft(P->dbl, P->n[axis], dir, fft_args(P, axis, data, scale), st));
+  }
+  return 0;
+}
+
+FusedArgs fused_args(const qj_plan *P, int axis) {
+  FusedArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.nx = P->n[0];
+  a.ny = P->n[1];
+  a.nz = P->n[2];
+  a.axis = axis;
+  a.stride = axis == 0 ? (long long)P->n[1] * P->n[2] : (axis == 1 ? P->n[2] : 1);
+  a.outer_stride = axis == 0 ? P->n[2] : (long long)P->n[1] * P->n[2];
+  a.ztiles = P->n[2] / 16;
+  a.R = P->R;
+  a.S1 = P->S1;
+  a.S2 = P->S2;
+  a.tw = (const float2 *)P->tw[axis];
+  a.prop = P->prop[axis];
+  for (int d = 0; d < 3; ++d) {
+    a.k[d] = P->kf[d];
+    a.kt[d] = P->ktf[d];
+  }
+  a.part = P->part;
+  a.fourpiG = 4.0 * M_PI * P->ph.G;
+  a.rho_bar = P->ph.rho_bar;
+  a.inv_ncell = 1.0 / (double)P->ncell;
+  a.amax_bits = (unsigned *)P->amax;
+  return a;
+}
+
+int ensure_prop(qj_plan *P, double dtk, cudaStream_t st) {
+  if (P->prop_dtk == dtk) return 0;
+  const int m = std::max(P->n[0], std::max(P->n[1], P->n[2]));
+  k_prop_tables<<<(m + 127) / 128, 128, 0, st>>>(P->prop[0], P->prop[1], P->prop[2], P->kd[0],
+                                                  P->kd[1], P->kd[2], P->n[0], P->n[1], P->n[2], dtk,
+                                                  P->ph.m_per_hbar);
+  QJ_CK_LAUNCH();
+  P->prop_dtk = dtk;
+  return 0;
+}
+
+int n_pencils(const qj_plan *P, int q) { return (int)(P->ncell / P->n[q]); }
+
+// CIC deposit list of `pos` in orientation q: sorted unique cells + starts.
+int deposit_list(qj_plan *P, const void *pos, int n, double m_s, const void *masses, int q,
+                 bool keys_ready, void *dts_reset, cudaStream_t st) {
+  if (!keys_ready)
+    QJ_TRY(launch_cic_prepare(P->dbl, pos, n, masses, m_s, geom(P), q, P->keys, P->vals, st));
+  QJ_TRY(launch_sort_unique(P->dbl, P->keys, P->vals, 8 * n, cell_bits(P->ncell), P->kA, P->iA,
+                            P->kB, P->iB, P->ukey, P->uval, P->cell_u, P->n_unique, dts_reset, st));
+  return launch_pencil_starts(P->ukey, P->n_unique, n_pencils(P, q), (unsigned)P->n[q], P->pstart, st);
+}
+
+// ---------------------------------------------------------------------------
+// Fused single-precision KDK (complex64 psi).  Consecutive half kicks of
+// adjacent steps share their potential (the density |psi|^2 and the star
+// positions do not change between them), so nsteps steps take nsteps + 1
+// Poisson solves; each kick still advances the star velocities by two
+// separate dt/2 half kicks and records dt_s between them, as the reference's
+// step boundary does.
+// ---------------------------------------------------------------------------
+int fused_kdk(qj_plan *P, float2 *psi, float *pos, float *vel, int n_s, double m_s, double dt,
+              int nsteps, int si, const float *vext, double *diag, cudaStream_t st) {
+  const bool parts = n_s > 0;
+  QJ_TRY(ensure_prop(P, dt, st));
+  QJ_TRY(launch_diag_load(false, diag, P->amax, st));
+  const double half_coef = P->ph.m_per_hbar * dt / 2.0;
+  int q = 2;
+  if (parts) {
+    if (prof_on()) prof_mark_begin(st);
+    QJ_TRY(deposit_list(P, pos, n_s, m_s, nullptr, q, false, P->dts, st));
+    if (prof_on()) prof_mark_end(7, st);
+  }
+  {
+    FusedArgs a = fused_args(P, q);
+    a.psi = psi;
+    if (parts) {
+      a.pstart = P->pstart;
+      a.ukey = P->ukey;
+      a.uval = (const float *)P->uval;
+    }
+    QJ_TRY(launch_fused(M_DENSITY, P->n[q], a, st));
+  }
+  for (int k = 0; k <= nsteps; ++k) {
+    const int r = 2 - q;
+    const bool last = (k == nsteps);
+    {
+      FusedArgs a = fused_args(P, 1);
+      QJ_TRY(launch_fused(M_FFT_FWD, P->n[1], a, st));
+    }
+    {
+      FusedArgs a = fused_args(P, r);
+      a.part_in = P->part;
+      a.n_part = pass_blocks(P->n[q], q, P->n[0], P->n[1], P->n[2]);
+      QJ_TRY(launch_fused(M_POISSON, P->n[r], a, st));
+    }
+    {
+      FusedArgs a = fused_args(P, 1);
+      QJ_TRY(launch_fused(M_IFFT2, P->n[1], a, st));
+    }
+    {
+      FusedArgs a = fused_args(P, q);
+      a.psi = psi;
+      a.kick_coef = half_coef * ((k == 0 || last) ? 1.0 : 2.0);
+      a.b_coeff = si ? (float)P->ph.b_coeff : 0.0f;
+      a.v_ext = vext;
+      a.do_drift = last ? 0 : 1;
+      if (parts) {
+        a.pstart = P->pstart;
+        a.ukey = P->ukey;
+        a.uval = (const float *)P->uval;
+        a.A = (float *)P->A;
+      }
+      QJ_TRY(launch_fused(M_KICK, P->n[q], a, st));
+    }
+    if (parts) {
+      if (prof_on()) prof_mark_begin(st);
+      QJ_TRY(launch_gather_unique(false, pos, n_s, geom(P), P->A, P->cell_u, P->acc, st));
+      UpdateArgs u;
+      std::memset(&u, 0, sizeof(u));
+      u.n = n_s;
+      u.dt = dt;
+      u.k2 = k > 0;
+      u.k1 = !last;
+      u.drift = !last;
+      u.dts_bits = P->dts;
+      u.q_next = r;
+      u.keys = last ? nullptr : P->keys;
+      u.vals = P->vals;
+      u.m_s = m_s;
+      QJ_TRY(launch_particles_update(false, pos, vel, P->acc, geom(P), u, st));
+      if (prof_on()) prof_mark_end(8, st);
+      if (!last) {
+        if (prof_on()) prof_mark_begin(st);
+        QJ_TRY(deposit_list(P, pos, n_s, m_s, nullptr, r, true, P->dts, st));
+        if (prof_on()) prof_mark_end(7, st);
+      }
+    }
+    if (!last) {
+      {
+        FusedArgs a = fused_args(P, 1);
+        a.psi = psi;
+        QJ_TRY(launch_fused(M_DRIFT, P->n[1], a, st));
+      }
+      {
+        FusedArgs a = fused_args(P, r);
+        a.psi = psi;
+        if (parts) {
+          a.pstart = P->pstart;
+          a.ukey = P->ukey;
+          a.uval = (const float *)P->uval;
+        }
+        QJ_TRY(launch_fused(M_DRIFT_DENSITY, P->n[r], a, st));
+      }
+    }
+    q = r;
+  }
+  return launch_diag_store(false, diag, P->amax, P->dts, parts ? 1 : 0, nsteps * dt, st);
+}
+
+// ---------------------------------------------------------------------------
+// Plain path: the reference's compute_step call for call (quantum-stars.py:295-330).
+// ---------------------------------------------------------------------------
+
+// get_potential(rho) -> V (rho given as rho_in, or |psi|^2 + rho_s).
+int plain_potential(qj_plan *P, const void *psi, const void *rho_s, const void *rho_in, void *V,
+                    int si, const void *vext, cudaStream_t st) {
+  QJ_TRY(launch_build_rho(P->dbl, psi, rho_s, nullptr, rho_in, 4.0 * M_PI * P->ph.G, P->ph.rho_bar,
+                          P->rho_tot, P->c0, P->ncell, st));
+  QJ_TRY(fft3d(P, P->c0, -1, st));
+  QJ_TRY(launch_poisson_div(P->dbl, P->c0, ktabs(P), P->ncell, st));
+  QJ_TRY(fft3d(P, P->c0, +1, st));
+  return launch_real_part(P->dbl, P->c0, 1.0, si ? P->rho_tot : nullptr, P->ph.b_coeff, vext, V,
+                          P->ncell, st);
+}
+
+// Grid accelerations of get_acceleration (:254-260) from P->rho_tot (or rho_in).
+int plain_accel(qj_plan *P, const void *rho_in, void *amax_bits, cudaStream_t st) {
+  QJ_TRY(launch_build_rho(P->dbl, nullptr, nullptr, nullptr, rho_in ? rho_in : P->rho_tot,
+                          4.0 * M_PI * P->ph.G, P->ph.rho_bar, nullptr, P->c0, P->ncell, st));
+  QJ_TRY(fft3d(P, P->c0, -1, st));
+  QJ_TRY(launch_poisson_div(P->dbl, P->c0, ktabs(P), P->ncell, st));
+  void *ag[3] = {P->ax, P->ay, P->az};
+  for (int d = 0; d < 3; ++d) {
+    QJ_TRY(launch_mul_ik(P->dbl, P->c0, d, ktabs(P), P->c1, P->ncell, st));
+    QJ_TRY(fft3d(P, P->c1, +1, st));
+    QJ_TRY(launch_real_part(P->dbl, P->c1, -1.0, nullptr, 0.0, nullptr, ag[d], P->ncell, st));
+  }
+  return launch_amax3(P->dbl, P->ax, P->ay, P->az, P->ncell, amax_bits, st);
+}
+
+int plain_bin(qj_plan *P, const void *pos, int n, double m_s, const void *masses, void *rho_s,
+              cudaStream_t st) {
+  QJ_CK(cudaMemsetAsync(rho_s, 0, P->ncell * P->rsz, st));
+  if (n <= 0) return 0;
+  QJ_TRY(deposit_list(P, pos, n, m_s, masses, 2, false, nullptr, st));
+  return launch_scatter_unique(P->dbl, P->ukey, P->uval, P->n_unique, 8 * n, rho_s, st);
+}
+
+int plain_kdk(qj_plan *P, void *psi, void *pos, void *vel, int n_s, double m_s, double dt,
+              int nsteps, int si, const void *vext, double *diag, cudaStream_t st) {
+  QJ_TRY(ensure_plain_ws(P));
+  QJ_TRY(launch_diag_load(P->dbl, diag, P->amax, st));
+  const double coef = P->ph.m_per_hbar * dt / 2.0;
+  for (int step = 0; step < nsteps; ++step) {
+    for (int half = 0; half < 2; ++half) {
+      // (1/2) kick
+      QJ_TRY(plain_bin(P, pos, n_s, m_s, nullptr, P->rho_s, st));
+      QJ_TRY(plain_potential(P, psi, P->rho_s, nullptr, P->V, si, vext, st));
+      QJ_TRY(launch_kick_plain(P->dbl, psi, P->V, coef, P->ncell, st));
+      QJ_TRY(plain_accel(P, nullptr, P->amax, st));
+      if (n_s > 0) {
+        QJ_TRY(launch_gather_dense(P->dbl, pos, n_s, geom(P), P->ax, P->ay, P->az, P->acc, st));
+        if (half == 1) QJ_TRY(launch_set_scalar(P->dbl, P->dts, INFINITY, st));
+        UpdateArgs u;
+        std::memset(&u, 0, sizeof(u));
+        u.n = n_s;
+        u.dt = dt;
+        u.k1 = half == 0;
+        u.k2 = half == 1;
+        u.drift = half == 0;
+        u.dts_bits = P->dts;
+        QJ_TRY(launch_particles_update(P->dbl, pos, vel, P->acc, geom(P), u, st));
+      }
+      if (half == 0) {
+        // drift (:307-309); the particle drift ran in the update above
+        QJ_TRY(fft3d(P, psi, -1, st));
+        QJ_TRY(launch_drift_mul(P->dbl, psi, ktabs(P), dt, P->ph.m_per_hbar, P->ncell, st));
+        QJ_TRY(fft3d(P, psi, +1, st));
+      }
+    }
+  }
+  return launch_diag_store(P->dbl, diag, P->amax, P->dts, n_s > 0 ? 1 : 0, nsteps * dt, st);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+const char *qj_last_error(void) { return g_err.c_str(); }
+
+int qj_plan_create(qj_plan **plan, const qj_grid *grid, const qj_phys *phys, int precision,
+                   int max_particles) {
+  if (!plan || !grid || !phys) {
+    set_error("qj_plan_create: null argument");
+    return QJ_ERR_ARG;
+  }
+  *plan = nullptr;
+  if (precision != QJ_PLAIN_F64 && precision != QJ_FUSED_F32) {
+    set_error("qj_plan_create: precision must be QJ_PLAIN_F64 or QJ_FUSED_F32");
+    return QJ_ERR_ARG;
+  }
+  const int n[3] = {grid->nx, grid->ny, grid->nz};
+  for (int a = 0; a < 3; ++a) {
+    if (!fft_length_supported(n[a])) {
+      set_error("qj_plan_create: axis %d length %d unsupported (16, 32, 64, 128, 256, 512)", a, n[a]);
+      return QJ_ERR_ARG;
+    }
+  }
+  if (n[2] % 16) {
+    set_error("qj_plan_create: nz must be a multiple of 16");
+    return QJ_ERR_ARG;
+  }
+  if (!(grid->Lx > 0 && grid->Ly > 0 && grid->Lz > 0)) {
+    set_error("qj_plan_create: box lengths must be positive");
+    return QJ_ERR_ARG;
+  }
+  if (max_particles < 0 || max_particles > (1 << 24) / 8) {
+    set_error("qj_plan_create: max_particles must be in [0, %d]", (1 << 24) / 8);
+    return QJ_ERR_ARG;
+  }
+  qj_plan *P = new qj_plan();
+  P->g = *grid;
+  P->ph = *phys;
+  P->prec = precision;
+  P->dbl = precision == QJ_PLAIN_F64;
+  P->max_particles = max_particles;
+  for (int a = 0; a < 3; ++a) P->n[a] = n[a];
+  P->ncell = (long long)n[0] * n[1] * n[2];
+  P->rsz = P->dbl ? 8 : 4;
+  P->csz = 2 * P->rsz;
+  const double L[3] = {grid->Lx, grid->Ly, grid->Lz};
+  int rc = 0;
+  auto fail = [&](int code) {
+    qj_plan_destroy(P);
+    return code;
+  };
+  for (int a = 0; a < 3 && !rc; ++a) {
+    const int N = n[a];
+    std::vector<double> k(N), kt(N);
+    std::vector<float> kf(N), ktf(N);
+    for (int i = 0; i < N; ++i) {
+      // ifftshift(2 pi / L * arange(-N/2, N/2)): index N/2 holds -pi N / L
+      const int m = i < N / 2 ? i : i - N;
+      k[i] = 2.0 * M_PI / L[a] * m;
+      kt[i] = (i == N / 2) ? 0.0 : k[i];
+      kf[i] = (float)k[i];
+      ktf[i] = (float)kt[i];
+    }
+    if ((rc = dev_alloc_t(P, &P->kd[a], N))) break;
+    if ((rc = dev_alloc_t(P, &P->kf[a], N))) break;
+    if ((rc = dev_alloc_t(P, &P->ktf[a], N))) break;
+    if ((rc = dev_alloc_t(P, &P->prop[a], N))) break;
+    cudaError_t e = cudaMemcpy(P->kd[a], k.data(), N * 8, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(P->kf[a], kf.data(), N * 4, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(P->ktf[a], ktf.data(), N * 4, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      rc = cuda_fail(e, "cudaMemcpy(tables)", __FILE__, __LINE__);
+      break;
+    }
+    P->kr[a] = P->dbl ? (void *)P->kd[a] : (void *)P->kf[a];
+    // twiddles w[m] = exp(-2 pi i m / N), long double, rounded once
+    if (P->dbl) {
+      std::vector<double2> w(N);
+      for (int m = 0; m < N; ++m) {
+        const long double th = -2.0L * 3.14159265358979323846264338327950288L * m / N;
+        w[m] = double2{(double)cosl(th), (double)sinl(th)};
+      }
+      if ((rc = dev_alloc(P, &P->tw[a], N * sizeof(double2)))) break;
+      e = cudaMemcpy(P->tw[a], w.data(), N * sizeof(double2), cudaMemcpyHostToDevice);
+    } else {
+      std::vector<float2> w(N);
+      for (int m = 0; m < N; ++m) {
+        const long double th = -2.0L * 3.14159265358979323846264338327950288L * m / N;
+        w[m] = float2{(float)cosl(th), (float)sinl(th)};
+      }
+      if ((rc = dev_alloc(P, &P->tw[a], N * sizeof(float2)))) break;
+      e = cudaMemcpy(P->tw[a], w.data(), N * sizeof(float2), cudaMemcpyHostToDevice);
+    }
+    if (e != cudaSuccess) rc = cuda_fail(e, "cudaMemcpy(twiddles)", __FILE__, __LINE__);
+  }
+  if (rc) return fail(rc);
+  if (!P->dbl) {
+    if ((rc = dev_alloc_t(P, &P->R, P->ncell))) return fail(rc);
+    if ((rc = dev_alloc_t(P, &P->S1, P->ncell))) return fail(rc);
+    if ((rc = dev_alloc_t(P, &P->S2, P->ncell))) return fail(rc);
+    int nb = 0;
+    for (int a = 0; a < 3; ++a) nb = std::max(nb, pass_blocks(n[a], a, n[0], n[1], n[2]));
+    if ((rc = dev_alloc_t(P, &P->part, nb))) return fail(rc);
+  } else {
+    if ((rc = ensure_plain_ws(P))) return fail(rc);
+  }
+  const size_t np8 = (size_t)8 * std::max(1, max_particles);
+  for (unsigned **b : {&P->keys, &P->kA, &P->iA, &P->kB, &P->iB, &P->ukey, &P->cell_u})
+    if ((rc = dev_alloc_t(P, b, np8))) return fail(rc);
+  if ((rc = dev_alloc(P, &P->vals, np8 * P->rsz))) return fail(rc);
+  if ((rc = dev_alloc(P, &P->uval, np8 * P->rsz))) return fail(rc);
+  if ((rc = dev_alloc(P, &P->A, 3 * np8 * P->rsz))) return fail(rc);
+  if ((rc = dev_alloc(P, &P->acc, 3 * (np8 / 8) * P->rsz))) return fail(rc);
+  long long npen = 0;
+  for (int a = 0; a < 3; ++a) npen = std::max(npen, P->ncell / n[a]);
+  if ((rc = dev_alloc_t(P, &P->pstart, npen + 1))) return fail(rc);
+  if ((rc = dev_alloc_t(P, &P->n_unique, 1))) return fail(rc);
+  if ((rc = dev_alloc(P, &P->amax, 8))) return fail(rc);
+  if ((rc = dev_alloc(P, &P->dts, 8))) return fail(rc);
+  if ((rc = dev_alloc(P, &P->tmp_scalar, 8))) return fail(rc);
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) return fail(cuda_fail(e, "plan init", __FILE__, __LINE__));
+  *plan = P;
+  return QJ_OK;
+}
+
+int qj_plan_destroy(qj_plan *P) {
+  if (!P) return QJ_OK;
+  for (void *p : P->allocs) cudaFree(p);
+  delete P;
+  return QJ_OK;
+}
+
+int qj_plan_set_phys(qj_plan *P, const qj_phys *phys) {
+  if (!P || !phys) {
+    set_error("qj_plan_set_phys: null argument");
+    return QJ_ERR_ARG;
+  }
+  if (phys->m_per_hbar != P->ph.m_per_hbar) P->prop_dtk = NAN;
+  P->ph = *phys;
+  return QJ_OK;
+}
+
+int64_t qj_plan_workspace_bytes(const qj_plan *P) { return P ? P->ws_bytes : 0; }
+
+int64_t qj_launch_count(void) { return (int64_t)g_launches.load(); }
+
+int qj_profile_enable(int on) {
+  Prof &p = prof();
+  std::lock_guard<std::mutex> g(p.mu);
+  for (auto &m : p.marks) {
+    p.pool.push_back(m.a);
+    p.pool.push_back(m.b);
+  }
+  p.marks.clear();
+  p.on = on != 0;
+  return QJ_OK;
+}
+
+int qj_profile_read(double *ms, int64_t *count, int nbuckets) {
+  Prof &p = prof();
+  std::lock_guard<std::mutex> g(p.mu);
+  for (int i = 0; i < nbuckets; ++i) {
+    ms[i] = 0.0;
+    count[i] = 0;
+  }
+  for (auto &m : p.marks) {
+    cudaError_t e = cudaEventSynchronize(m.b);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaEventSynchronize", __FILE__, __LINE__);
+    float t = 0.f;
+    e = cudaEventElapsedTime(&t, m.a, m.b);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaEventElapsedTime", __FILE__, __LINE__);
+    if (m.bucket >= 0 && m.bucket < nbuckets) {
+      ms[m.bucket] += t;
+      count[m.bucket] += 1;
+    }
+  }
+  return QJ_OK;
+}
+
+int qj_fft3d(qj_plan *P, const void *in, void *out, int direction, void *stream) {
+  if (!P || !in || !out || (direction != -1 && direction != 1)) {
+    set_error("qj_fft3d: bad argument");
+    return QJ_ERR_ARG;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  if (in != out) QJ_CK(cudaMemcpyAsync(out, in, P->ncell * P->csz, cudaMemcpyDeviceToDevice, st));
+  return fft3d(P, out, direction, st);
+}
+
+int qj_get_potential(qj_plan *P, const void *rho, void *V, int self_interaction, void *stream) {
+  if (!P || !rho || !V) {
+    set_error("qj_get_potential: null argument");
+    return QJ_ERR_ARG;
+  }
+  QJ_TRY(ensure_plain_ws(P));
+  return plain_potential(P, nullptr, nullptr, rho, V, self_interaction, nullptr,
+                         (cudaStream_t)stream);
+}
+
+int qj_bin_stars(qj_plan *P, const void *pos, int n, double m_s, const void *masses, void *rho_s,
+                 void *stream) {
+  if (!P || !rho_s || (n > 0 && !pos) || n < 0 || n > P->max_particles) {
+    set_error("qj_bin_stars: bad argument (n=%d, max_particles=%d)", n, P ? P->max_particles : 0);
+    return QJ_ERR_ARG;
+  }
+  return plain_bin(P, pos, n, m_s, masses, rho_s, (cudaStream_t)stream);
+}
+
+int qj_get_acceleration(qj_plan *P, const void *pos, int n, const void *rho, void *acc,
+                        double *a_max, void *stream) {
+  if (!P || !rho || (n > 0 && (!pos || !acc)) || n < 0 || n > P->max_particles) {
+    set_error("qj_get_acceleration: bad argument (n=%d, max_particles=%d)", n,
+              P ? P->max_particles : 0);
+    return QJ_ERR_ARG;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  QJ_TRY(ensure_plain_ws(P));
+  QJ_CK(cudaMemsetAsync(P->tmp_scalar, 0, 8, st));
+  QJ_TRY(plain_accel(P, rho, P->tmp_scalar, st));
+  if (n > 0) QJ_TRY(launch_gather_dense(P->dbl, pos, n, geom(P), P->ax, P->ay, P->az, acc, st));
+  if (a_max) QJ_TRY(launch_bits_to_double(P->dbl, P->tmp_scalar, a_max, st));
+  return QJ_OK;
+}
+
+int qj_kdk_step(qj_plan *P, void *psi, void *pos, void *vel, int n_s, double m_s, double dt,
+                int nsteps, int self_interaction, const void *v_ext, qj_diag *diag,
+                void *stream) {
+  if (!P || !psi || !diag || nsteps < 0 || n_s < 0 || (n_s > 0 && (!pos || !vel))) {
+    set_error("qj_kdk_step: bad argument");
+    return QJ_ERR_ARG;
+  }
+  if (n_s > P->max_particles) {
+    set_error("qj_kdk_step: n_s=%d exceeds the plan's max_particles=%d", n_s, P->max_particles);
+    return QJ_ERR_ARG;
+  }
+  if (!(dt > 0) || !std::isfinite(dt)) {
+    set_error("qj_kdk_step: dt must be positive and finite");
+    return QJ_ERR_ARG;
+  }
+  if (nsteps == 0) return QJ_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (P->dbl)
+    return plain_kdk(P, psi, pos, vel, n_s, m_s, dt, nsteps, self_interaction, v_ext,
+                     (double *)diag, st);
+  return fused_kdk(P, (float2 *)psi, (float *)pos, (float *)vel, n_s, m_s, dt, nsteps,
+                   self_interaction, (const float *)v_ext, (double *)diag, st);
+}
+
+}  // extern "C"

@@ -1,0 +1,124 @@
+// Host-side declarations shared by the libqj translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <atomic>
+
+#include "qj_pass.cuh"
+
+namespace qj {
+
+// ----- error state (qj_api.cu) -----
+void set_error(const char *fmt, ...);
+int cuda_fail(cudaError_t e, const char *what, const char *file, int line);
+
+#define QJ_CK(call)                                                      \
+  do {                                                                   \
+    cudaError_t e_ = (call);                                             \
+    if (e_ != cudaSuccess) return ::qj::cuda_fail(e_, #call, __FILE__, __LINE__); \
+  } while (0)
+// Every kernel launch in libqj is followed by QJ_CK_LAUNCH(), which also
+// counts it (qj_launch_count).
+extern std::atomic<long long> g_launches;
+#define QJ_CK_LAUNCH()                      \
+  do {                                      \
+    ::qj::g_launches.fetch_add(1, std::memory_order_relaxed); \
+    QJ_CK(cudaGetLastError());              \
+  } while (0)
+
+// Optional per-pass timing with CUDA events on the launching stream
+// (qj_profile_enable / qj_profile_read).  Bucket = pass mode (0..6), 7 = the
+// deposit sort, 8 = other particle kernels.
+constexpr int kProfBuckets = 9;
+bool prof_on();
+void prof_mark_begin(cudaStream_t st);
+void prof_mark_end(int bucket, cudaStream_t st);
+
+bool fft_length_supported(int n);
+
+// ----- pencil passes (qj_fused.cu, qj_fftpass.cu) -----
+// Launch one fused single-precision pass of `mode` along `a.axis` (length n).
+int launch_fused(int mode, int n, const FusedArgs &a, cudaStream_t st);
+// Number of CTAs a pass along `axis` launches (= partial sums written).
+int pass_blocks(int n_axis, int axis, int nx, int ny, int nz);
+// Generic in-place FFT pass over a complex field (float2 if dbl == 0, else
+// double2) along a.axis.
+int launch_fft(bool dbl, int n, int dir, const FftArgs &a, cudaStream_t st);
+
+// ----- particles (qj_particles.cu) -----
+struct CicGeomD {
+  int n[3];
+  double d[3];
+  double L[3];
+  double vol;
+};
+unsigned cell_bits(long long ncell);
+// keys / vals of the 8 CIC corner deposits of n particles, in orientation q.
+int launch_cic_prepare(bool dbl, const void *pos, int n, const void *masses, double m_s,
+                       const CicGeomD &g, int q, unsigned *keys, void *vals, cudaStream_t st);
+// Stable sort of (key, index) + per-cell ordered sums.  Outputs ukey[u],
+// uval[u], cell_u[original index] = u, *n_unique.  dts_reset (optional) is
+// set to +inf bits.
+int launch_sort_unique(bool dbl, const unsigned *keys, const void *vals, int n, unsigned nbits,
+                       unsigned *kA, unsigned *iA, unsigned *kB, unsigned *iB, unsigned *ukey,
+                       void *uval, unsigned *cell_u, int *n_unique, void *dts_reset,
+                       cudaStream_t st);
+int launch_pencil_starts(const unsigned *ukey, const int *n_unique, int n_pencils, unsigned nq,
+                         int *start, cudaStream_t st);
+int launch_scatter_unique(bool dbl, const unsigned *ukey, const void *uval, const int *n_unique,
+                          int max_unique, void *grid, cudaStream_t st);
+// acc[s] = sum_c w_c A[cell_u[8 s + c]] (deposit-cell accelerations).
+int launch_gather_unique(bool dbl, const void *pos, int n, const CicGeomD &g, const void *A,
+                         const unsigned *cell_u, void *acc, cudaStream_t st);
+// acc[s] = sum_c w_c (ax, ay, az)[cell_c] from dense grids.
+int launch_gather_dense(bool dbl, const void *pos, int n, const CicGeomD &g, const void *ax,
+                        const void *ay, const void *az, void *acc, cudaStream_t st);
+// Leapfrog update: optional second half kick (K2, end of a step; updates
+// dt_s), optional first half kick (K1), optional drift + CIC keys of the new
+// positions in orientation q_next.
+struct UpdateArgs {
+  int n;
+  double dt;
+  int k2, k1, drift;
+  void *dts_bits;  // unsigned (float) / unsigned long long (double)
+  int q_next;
+  unsigned *keys;
+  void *vals;
+  const void *masses;
+  double m_s;
+};
+int launch_particles_update(bool dbl, void *pos, void *vel, const void *acc, const CicGeomD &g,
+                            const UpdateArgs &u, cudaStream_t st);
+
+// ----- plain elementwise kernels (qj_plain.cu), R = float or double -----
+struct KTabs {
+  const void *k[3];  // per-axis k tables of the real type
+  int n[3];
+};
+int launch_build_rho(bool dbl, const void *psi, const void *rho_s, const void *rho_gas,
+                     const void *rho_in, double fourpiG, double rho_bar, void *rho_tot,
+                     void *cbuf, long long ncell, cudaStream_t st);
+int launch_poisson_div(bool dbl, void *cbuf, const KTabs &k, long long ncell, cudaStream_t st);
+int launch_mul_ik(bool dbl, const void *vh, int d, const KTabs &k, void *out, long long ncell,
+                  cudaStream_t st);
+int launch_real_part(bool dbl, const void *c, double sign, const void *rho, double b,
+                     const void *vext, void *out, long long ncell, cudaStream_t st);
+int launch_kick_plain(bool dbl, void *psi, const void *V, double coef, long long ncell,
+                      cudaStream_t st);
+int launch_drift_mul(bool dbl, void *cbuf, const KTabs &k, double dt_kin, double m_per_hbar,
+                     long long ncell, cudaStream_t st);
+int launch_amax3(bool dbl, const void *ax, const void *ay, const void *az, long long ncell,
+                 void *bits, cudaStream_t st);
+int launch_gas_kick(bool dbl, void *vx, void *vy, void *vz, const void *ax, const void *ay,
+                    const void *az, double dt, long long ncell, cudaStream_t st);
+
+// ----- small scalar kernels (qj_particles.cu) -----
+int launch_diag_load(bool dbl, const void *diag, void *amax_bits, cudaStream_t st);
+int launch_diag_store(bool dbl, void *diag, const void *amax_bits, const void *dts_bits,
+                      int has_particles, double t_add, cudaStream_t st);
+int launch_set_scalar(bool dbl, void *dst, double v, cudaStream_t st);
+int launch_bits_to_double(bool dbl, const void *bits, double *out, cudaStream_t st);
+
+}  // namespace qj

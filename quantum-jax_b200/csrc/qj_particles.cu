@@ -1,0 +1,487 @@
+// Particle kernels: cloud-in-cell deposit and gather, leapfrog update.
+//
+// The deposit is deterministic without floating-point atomics: every particle
+// emits its 8 corner contributions (key = cell in the pass orientation,
+// value = w_x w_y w_z m / vol), a single-CTA stable LSD radix sort orders them
+// by cell while keeping (particle, corner) order inside a cell, and the head
+// of each run sums the run sequentially from zero.  That is exactly the order
+// of the reference's sequential fori_loop over stars with 8 fixed-order
+// scatter-adds each (quantum-stars.py:212-247), so the float32 result matches
+// a float32 evaluation of the reference bit for bit.
+#include <cstdio>
+
+#include "qj_internal.h"
+
+namespace qj {
+
+// Corner visit order of quantum-stars.py:220-243 and :264-287
+// (bit d set = ip1 along axis d).
+__constant__ int c_corner[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1},
+                                   {1, 1, 0}, {1, 0, 1}, {0, 1, 1}, {1, 1, 1}};
+
+template <typename R> struct CicGeom {
+  int n[3];
+  R d[3];
+  R L[3];
+  R vol;
+};
+
+template <typename R> static CicGeom<R> cast_geom(const CicGeomD &g) {
+  CicGeom<R> o;
+  for (int i = 0; i < 3; ++i) {
+    o.n[i] = g.n[i];
+    o.d[i] = (R)g.d[i];
+    o.L[i] = (R)g.L[i];
+  }
+  o.vol = (R)g.vol;
+  return o;
+}
+
+// quantum-stars.py:200-209 for one axis, every operation rounded in the
+// written order:  i = floor((x - 0.5 dx) / dx);  w_i = ((i + 1 + 0.5) dx - x) / dx;
+// w_ip1 = (x - (i + 0.5) dx) / dx;  indices wrapped with jnp.mod.
+template <typename R>
+__device__ __forceinline__ void cic_axis(R x, R dx, int n, int &i0, int &i1, R &w0, R &w1) {
+  const R half = (R)0.5;
+  const R i = floor(fdiv_rn(fsub_rn(x, fmul_rn(half, dx)), dx));
+  const R ip1 = fadd_rn(i, (R)1);
+  w0 = fdiv_rn(fsub_rn(fmul_rn(fadd_rn(ip1, half), dx), x), dx);
+  w1 = fdiv_rn(fsub_rn(x, fmul_rn(fadd_rn(i, half), dx)), dx);
+  R m0 = ref_mod(i, (R)n), m1 = ref_mod(ip1, (R)n);
+  // non-finite positions map to cell 0 (the state is reported non-finite
+  // by the caller's checks); keeps every index in bounds.
+  i0 = (m0 >= (R)0 && m0 < (R)n) ? (int)m0 : 0;
+  i1 = (m1 >= (R)0 && m1 < (R)n) ? (int)m1 : 0;
+}
+
+__device__ __forceinline__ unsigned cell_key(int cx, int cy, int cz, int q, int nx, int ny,
+                                             int nz) {
+  if (q == 2) return ((unsigned)cx * (unsigned)ny + (unsigned)cy) * (unsigned)nz + (unsigned)cz;
+  if (q == 0) return ((unsigned)cy * (unsigned)nz + (unsigned)cz) * (unsigned)nx + (unsigned)cx;
+  return ((unsigned)cx * (unsigned)nz + (unsigned)cz) * (unsigned)ny + (unsigned)cy;
+}
+
+template <typename R>
+__device__ __forceinline__ void cic_emit(const R *pos, int s, const CicGeom<R> &g, R fac, int q,
+                                         unsigned *keys, R *vals) {
+  int i0[3], i1[3];
+  R w0[3], w1[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) cic_axis<R>(pos[3 * s + d], g.d[d], g.n[d], i0[d], i1[d], w0[d], w1[d]);
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    const int bx = c_corner[c][0], by = c_corner[c][1], bz = c_corner[c][2];
+    const R v = fmul_rn(fmul_rn(fmul_rn(bx ? w1[0] : w0[0], by ? w1[1] : w0[1]), bz ? w1[2] : w0[2]), fac);
+    keys[8 * s + c] = cell_key(bx ? i1[0] : i0[0], by ? i1[1] : i0[1], bz ? i1[2] : i0[2], q, g.n[0],
+                               g.n[1], g.n[2]);
+    vals[8 * s + c] = v;
+  }
+}
+
+// fac: m_s / (dx dy dz) evaluated in float64 and rounded (bin_stars,
+// quantum-stars.py:219), or masses[s] / vol rounded per operation
+// (bin_particles, quantum-gas-bh.py:421).
+template <typename R>
+__device__ __forceinline__ R cic_fac(const R *masses, int s, R fac_all, R vol) {
+  return masses ? fdiv_rn(masses[s], vol) : fac_all;
+}
+
+template <typename R>
+__global__ void k_cic_prepare(const R *pos, int n, const R *masses, R fac_all, CicGeom<R> g, int q,
+                              unsigned *keys, R *vals) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  cic_emit<R>(pos, s, g, cic_fac<R>(masses, s, fac_all, g.vol), q, keys, vals);
+}
+
+unsigned cell_bits(long long ncell) {
+  unsigned b = 0;
+  while ((1ll << b) < ncell) ++b;
+  return b;
+}
+
+int launch_cic_prepare(bool dbl, const void *pos, int n, const void *masses, double m_s,
+                       const CicGeomD &g, int q, unsigned *keys, void *vals, cudaStream_t st) {
+  if (n <= 0) return 0;
+  const int T = 128, B = (n + T - 1) / T;
+  const double fac = m_s / (g.d[0] * g.d[1] * g.d[2]);
+  if (dbl)
+    k_cic_prepare<double><<<B, T, 0, st>>>((const double *)pos, n, (const double *)masses, fac,
+                                           cast_geom<double>(g), q, keys, (double *)vals);
+  else
+    k_cic_prepare<float><<<B, T, 0, st>>>((const float *)pos, n, (const float *)masses, (float)fac,
+                                          cast_geom<float>(g), q, keys, (float *)vals);
+  QJ_CK_LAUNCH();
+  return 0;
+}
+
+// Single-CTA stable LSD radix sort (8-bit digits) of (key, index) pairs,
+// then run-length reduction in sorted order.  32 warps each own a
+// contiguous chunk; within a digit pass a warp scatters its chunk in order
+// with __match_any_sync ranks, so equal keys keep their input order.
+template <typename R>
+__global__ void __launch_bounds__(1024)
+    k_sort_unique(const unsigned *keys_in, const R *vals, int n, unsigned nbits, unsigned *kA,
+                  unsigned *iA, unsigned *kB, unsigned *iB, unsigned *ukey, R *uval,
+                  unsigned *cell_u, int *n_unique, R *dts_reset) {
+  __shared__ unsigned hist[32 * 256];
+  __shared__ unsigned dbase[256];
+  __shared__ unsigned wsum[32];
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  if (tid == 0 && dts_reset) *dts_reset = (R)INFINITY;
+  const int chunk = (n + 31) / 32;
+  const int beg = min(n, w * chunk), end = min(n, beg + chunk);
+  const unsigned *kin = keys_in;
+  const unsigned *iin = nullptr;
+  unsigned *kout = kA, *iout = iA;
+  for (unsigned shift = 0; shift < nbits; shift += 8) {
+    for (int i = tid; i < 32 * 256; i += 1024) hist[i] = 0;
+    __syncthreads();
+    for (int i = beg + lane; i < end; i += 32) atomicAdd(&hist[w * 256 + ((kin[i] >> shift) & 255u)], 1u);
+    __syncthreads();
+    if (tid < 256) {
+      unsigned s = 0;
+      for (int ww = 0; ww < 32; ++ww) {
+        const unsigned c = hist[ww * 256 + tid];
+        hist[ww * 256 + tid] = s;
+        s += c;
+      }
+      dbase[tid] = s;
+    }
+    __syncthreads();
+    if (w == 0) {  // exclusive scan of the 256 digit totals
+      unsigned v[8], loc = 0;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        v[j] = dbase[lane * 8 + j];
+        loc += v[j];
+      }
+      unsigned incl = loc;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+      }
+      unsigned run = incl - loc;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const unsigned c = v[j];
+        dbase[lane * 8 + j] = run;
+        run += c;
+      }
+    }
+    __syncthreads();
+    if (tid < 256)
+      for (int ww = 0; ww < 32; ++ww) hist[ww * 256 + tid] += dbase[tid];
+    __syncthreads();
+    for (int i0 = beg; i0 < end; i0 += 32) {
+      const int i = i0 + lane;
+      const bool ok = i < end;
+      unsigned k = 0, id = 0, d = 256u + (unsigned)lane;
+      if (ok) {
+        k = kin[i];
+        id = iin ? iin[i] : (unsigned)i;
+        d = (k >> shift) & 255u;
+      }
+      const unsigned peers = __match_any_sync(0xffffffffu, d);
+      const unsigned rank = __popc(peers & ((1u << lane) - 1u));
+      if (ok) {
+        const unsigned p = hist[w * 256 + d] + rank;
+        kout[p] = k;
+        iout[p] = id;
+      }
+      __syncwarp();
+      if (ok && rank == 0) hist[w * 256 + d] += __popc(peers);
+      __syncwarp();
+    }
+    __syncthreads();
+    kin = kout;
+    iin = iout;
+    kout = (kout == kA) ? kB : kA;
+    iout = (iout == iA) ? iB : iA;
+  }
+  // run heads and ordered per-cell sums
+  const int c2 = (n + 1023) / 1024;
+  const int b2 = min(n, tid * c2), e2 = min(n, b2 + c2);
+  unsigned cnt = 0;
+  for (int i = b2; i < e2; ++i) cnt += (i == 0 || kin[i] != kin[i - 1]) ? 1u : 0u;
+  unsigned incl = cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) wsum[w] = incl;
+  __syncthreads();
+  if (w == 0) {
+    unsigned x = wsum[lane], xi = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned y = __shfl_up_sync(0xffffffffu, xi, o);
+      if (lane >= o) xi += y;
+    }
+    wsum[lane] = xi - x;  // exclusive
+  }
+  __syncthreads();
+  unsigned u = wsum[w] + incl - cnt;
+  for (int i = b2; i < e2; ++i) {
+    const unsigned k = kin[i];
+    if (i == 0 || k != kin[i - 1]) {
+      R s = (R)0;
+      int j = i;
+      do {
+        s = fadd_rn(s, vals[iin ? iin[j] : (unsigned)j]);
+        ++j;
+      } while (j < n && kin[j] == k);
+      ukey[u] = k;
+      uval[u] = s;
+      ++u;
+    }
+    cell_u[iin ? iin[i] : (unsigned)i] = u - 1;
+  }
+  if (tid == 1023) *n_unique = (int)(wsum[w] + incl);
+}
+
+int launch_sort_unique(bool dbl, const unsigned *keys, const void *vals, int n, unsigned nbits,
+                       unsigned *kA, unsigned *iA, unsigned *kB, unsigned *iB, unsigned *ukey,
+                       void *uval, unsigned *cell_u, int *n_unique, void *dts_reset,
+                       cudaStream_t st) {
+  if (n <= 0) return 0;
+  if (dbl)
+    k_sort_unique<double><<<1, 1024, 0, st>>>(keys, (const double *)vals, n, nbits, kA, iA, kB, iB,
+                                              ukey, (double *)uval, cell_u, n_unique,
+                                              (double *)dts_reset);
+  else
+    k_sort_unique<float><<<1, 1024, 0, st>>>(keys, (const float *)vals, n, nbits, kA, iA, kB, iB,
+                                             ukey, (float *)uval, cell_u, n_unique,
+                                             (float *)dts_reset);
+  QJ_CK_LAUNCH();
+  return 0;
+}
+
+__global__ void k_pencil_starts(const unsigned *ukey, const int *n_unique, int n_pencils,
+                                unsigned nq, int *start) {
+  const int pid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pid > n_pencils) return;
+  const unsigned long long target = (unsigned long long)pid * nq;
+  int lo = 0, hi = *n_unique;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if ((unsigned long long)ukey[mid] < target)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  start[pid] = lo;
+}
+
+int launch_pencil_starts(const unsigned *ukey, const int *n_unique, int n_pencils, unsigned nq,
+                         int *start, cudaStream_t st) {
+  const int T = 256, B = (n_pencils + 1 + T - 1) / T;
+  k_pencil_starts<<<B, T, 0, st>>>(ukey, n_unique, n_pencils, nq, start);
+  QJ_CK_LAUNCH();
+  return 0;
+}
+
+template <typename R>
+__global__ void k_scatter_unique(const unsigned *ukey, const R *uval, const int *n_unique, R *grid) {
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u < *n_unique) grid[ukey[u]] = uval[u];
+}
+
+int launch_scatter_unique(bool dbl, const unsigned *ukey, const void *uval, const int *n_unique,
+                          int max_unique, void *grid, cudaStream_t st) {
+  if (max_unique <= 0) return 0;
+  const int T = 256, B = (max_unique + T - 1) / T;
+  if (dbl)
+    k_scatter_unique<double><<<B, T, 0, st>>>(ukey, (const double *)uval, n_unique, (double *)grid);
+  else
+    k_scatter_unique<float><<<B, T, 0, st>>>(ukey, (const float *)uval, n_unique, (float *)grid);
+  QJ_CK_LAUNCH();
+  return 0;
+}
+
+// quantum-stars.py:262-287: acc = sum over corners, in order, of
+// (w_x w_y w_z) * a(corner), starting from zero.
+template <typename R, bool DENSE>
+__global__ void k_gather(const R *pos, int n, CicGeom<R> g, const R *A, const unsigned *cell_u,
+                         const R *ax, const R *ay, const R *az, R *acc) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  int i0[3], i1[3];
+  R w0[3], w1[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) cic_axis<R>(pos[3 * s + d], g.d[d], g.n[d], i0[d], i1[d], w0[d], w1[d]);
+  R a0 = (R)0, a1 = (R)0, a2 = (R)0;
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    const int bx = c_corner[c][0], by = c_corner[c][1], bz = c_corner[c][2];
+    const R wp = fmul_rn(fmul_rn(bx ? w1[0] : w0[0], by ? w1[1] : w0[1]), bz ? w1[2] : w0[2]);
+    R gx, gy, gz;
+    if (DENSE) {
+      const long long cell = ((long long)(bx ? i1[0] : i0[0]) * g.n[1] + (by ? i1[1] : i0[1])) * g.n[2] +
+                             (bz ? i1[2] : i0[2]);
+      gx = ax[cell];
+      gy = ay[cell];
+      gz = az[cell];
+    } else {
+      const unsigned u = cell_u[8 * s + c];
+      gx = A[3 * u + 0];
+      gy = A[3 * u + 1];
+      gz = A[3 * u + 2];
+    }
+    a0 = fadd_rn(a0, fmul_rn(wp, gx));
+    a1 = fadd_rn(a1, fmul_rn(wp, gy));
+    a2 = fadd_rn(a2, fmul_rn(wp, gz));
+  }
+  acc[3 * s + 0] = a0;
+  acc[3 * s + 1] = a1;
+  acc[3 * s + 2] = a2;
+}
+
+int launch_gather_unique(bool dbl, const void *pos, int n, const CicGeomD &g, const void *A,
+                         const unsigned *cell_u, void *acc, cudaStream_t st) {
+  if (n <= 0) return 0;
+  const int T = 128, B = (n + T - 1) / T;
+  if (dbl)
+    k_gather<double, false><<<B, T, 0, st>>>((const double *)pos, n, cast_geom<double>(g),
+                                             (const double *)A, cell_u, nullptr, nullptr, nullptr,
+                                             (double *)acc);
+  else
+    k_gather<float, false><<<B, T, 0, st>>>((const float *)pos, n, cast_geom<float>(g),
+                                            (const float *)A, cell_u, nullptr, nullptr, nullptr,
+                                            (float *)acc);
+  QJ_CK_LAUNCH();
+  return 0;
+}
+
+int launch_gather_dense(bool dbl, const void *pos, int n, const CicGeomD &g, const void *ax,
+                        const void *ay, const void *az, void *acc, cudaStream_t st) {
+  if (n <= 0) return 0;
+  const int T = 128, B = (n + T - 1) / T;
+  if (dbl)
+    k_gather<double, true><<<B, T, 0, st>>>((const double *)pos, n, cast_geom<double>(g), nullptr,
+                                            nullptr, (const double *)ax, (const double *)ay,
+                                            (const double *)az, (double *)acc);
+  else
+    k_gather<float, true><<<B, T, 0, st>>>((const float *)pos, n, cast_geom<float>(g), nullptr,
+                                           nullptr, (const float *)ax, (const float *)ay,
+                                           (const float *)az, (float *)acc);
+  QJ_CK_LAUNCH();
+  return 0;
+}
+
+// vel = vel + acc * dt / 2.0 (quantum-stars.py:304,321); dt_s = min |dx / vel|
+// (:328, dx for every component); pos = mod(pos + vel * dt, L) (:311-312).
+template <typename R>
+__global__ void k_particles_update(R *pos, R *vel, const R *acc, int n, CicGeom<R> g, R dt, int k2,
+                                   int k1, int drift, R *dts, int q_next, unsigned *keys, R *vals,
+                                   const R *masses, R fac_all) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  R v[3], x[3];
+  float dmin = INFINITY;
+  double dmind = INFINITY;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    v[d] = vel[3 * s + d];
+    const R h = fdiv_rn(fmul_rn(acc[3 * s + d], dt), (R)2);
+    if (k2) {
+      v[d] = fadd_rn(v[d], h);
+      const R r = fabs(fdiv_rn(g.d[0], v[d]));
+      if constexpr (sizeof(R) == 4)
+        dmin = fminf(dmin, (float)r);
+      else
+        dmind = fmin(dmind, (double)r);
+    }
+    if (k1) v[d] = fadd_rn(v[d], h);
+    vel[3 * s + d] = v[d];
+  }
+  if (k2) {
+    if constexpr (sizeof(R) == 4)
+      atomic_min_nonneg((unsigned int *)dts, dmin);
+    else
+      atomic_min_nonneg((unsigned long long *)dts, dmind);
+  }
+  if (drift) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      x[d] = ref_mod(fadd_rn(pos[3 * s + d], fmul_rn(v[d], dt)), g.L[d]);
+      pos[3 * s + d] = x[d];
+    }
+    if (keys) cic_emit<R>(pos, s, g, cic_fac<R>(masses, s, fac_all, g.vol), q_next, keys, vals);
+  }
+}
+
+int launch_particles_update(bool dbl, void *pos, void *vel, const void *acc, const CicGeomD &g,
+                            const UpdateArgs &u, cudaStream_t st) {
+  if (u.n <= 0) return 0;
+  const int T = 128, B = (u.n + T - 1) / T;
+  const double fac = u.m_s / (g.d[0] * g.d[1] * g.d[2]);
+  if (dbl)
+    k_particles_update<double><<<B, T, 0, st>>>(
+        (double *)pos, (double *)vel, (const double *)acc, u.n, cast_geom<double>(g), u.dt, u.k2,
+        u.k1, u.drift, (double *)u.dts_bits, u.q_next, u.keys, (double *)u.vals,
+        (const double *)u.masses, fac);
+  else
+    k_particles_update<float><<<B, T, 0, st>>>(
+        (float *)pos, (float *)vel, (const float *)acc, u.n, cast_geom<float>(g), (float)u.dt,
+        u.k2, u.k1, u.drift, (float *)u.dts_bits, u.q_next, u.keys, (float *)u.vals,
+        (const float *)u.masses, (float)fac);
+  QJ_CK_LAUNCH();
+  return 0;
+}
+
+// ----- scalar state kernels -----
+// amax / dt_s are kept as the real type's bit pattern (non-negative values,
+// ordered like unsigned integers) so atomicMax / atomicMin are exact.
+template <typename R> __global__ void k_diag_load(const double *diag, R *amax) {
+  *amax = (R)diag[1];
+}
+template <typename R>
+__global__ void k_diag_store(double *diag, const R *amax, const R *dts, int has_particles,
+                             double t_add) {
+  diag[0] += t_add;
+  diag[1] = (double)*amax;
+  diag[2] = has_particles ? (double)*dts : (double)INFINITY;
+}
+template <typename R> __global__ void k_set_scalar(R *dst, double v) { *dst = (R)v; }
+template <typename R> __global__ void k_to_double(const R *src, double *out) { *out = (double)*src; }
+
+int launch_diag_load(bool dbl, const void *diag, void *amax_bits, cudaStream_t st) {
+  if (dbl)
+    k_diag_load<double><<<1, 1, 0, st>>>((const double *)diag, (double *)amax_bits);
+  else
+    k_diag_load<float><<<1, 1, 0, st>>>((const double *)diag, (float *)amax_bits);
+  QJ_CK_LAUNCH();
+  return 0;
+}
+int launch_diag_store(bool dbl, void *diag, const void *amax_bits, const void *dts_bits,
+                      int has_particles, double t_add, cudaStream_t st) {
+  if (dbl)
+    k_diag_store<double><<<1, 1, 0, st>>>((double *)diag, (const double *)amax_bits,
+                                          (const double *)dts_bits, has_particles, t_add);
+  else
+    k_diag_store<float><<<1, 1, 0, st>>>((double *)diag, (const float *)amax_bits,
+                                         (const float *)dts_bits, has_particles, t_add);
+  QJ_CK_LAUNCH();
+  return 0;
+}
+int launch_set_scalar(bool dbl, void *dst, double v, cudaStream_t st) {
+  if (dbl)
+    k_set_scalar<double><<<1, 1, 0, st>>>((double *)dst, v);
+  else
+    k_set_scalar<float><<<1, 1, 0, st>>>((float *)dst, v);
+  QJ_CK_LAUNCH();
+  return 0;
+}
+int launch_bits_to_double(bool dbl, const void *bits, double *out, cudaStream_t st) {
+  if (dbl)
+    k_to_double<double><<<1, 1, 0, st>>>((const double *)bits, out);
+  else
+    k_to_double<float><<<1, 1, 0, st>>>((const float *)bits, out);
+  QJ_CK_LAUNCH();
+  return 0;
+}
+
+}  // namespace qj

@@ -1,0 +1,254 @@
+// Plain (unfused) elementwise kernels.  Each one is one line of the
+// reference's step functions, in the reference's operation order; the plain
+// float64 step strings them together with full 3-D FFTs exactly as
+// quantum-stars.py:295-330 does.
+#include "qj_internal.h"
+
+namespace qj {
+
+template <typename R> struct KT {
+  const R *k[3];
+  int n[3];
+};
+template <typename R> static KT<R> cast_k(const KTabs &k) {
+  KT<R> o;
+  for (int i = 0; i < 3; ++i) {
+    o.k[i] = (const R *)k.k[i];
+    o.n[i] = k.n[i];
+  }
+  return o;
+}
+template <typename R>
+__device__ __forceinline__ void cell_k(const KT<R> &k, long long idx, R &kx, R &ky, R &kz) {
+  const int iz = (int)(idx % k.n[2]);
+  const long long r = idx / k.n[2];
+  const int iy = (int)(r % k.n[1]);
+  const int ix = (int)(r / k.n[1]);
+  kx = k.k[0][ix];
+  ky = k.k[1][iy];
+  kz = k.k[2][iz];
+}
+
+#define GRID_LOOP(i, n) \
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (n); i += (long long)gridDim.x * blockDim.x)
+
+static int grid_blocks(long long n) {
+  long long b = (n + 255) / 256;
+  return (int)(b > 148 * 32 ? 148 * 32 : (b < 1 ? 1 : b));
+}
+
+// rho_tot = |psi|^2 + rho_s + rho_gas (quantum-stars.py:299, gas-bh :542), or
+// rho_in; cbuf = 4 pi G (rho_tot - rho_bar) as a complex field (the argument
+// of fftn in get_potential, :191).
+template <typename R>
+__global__ void k_build_rho(const cplx<R> *psi, const R *rho_s, const R *rho_gas, const R *rho_in,
+                            R fourpiG, R rho_bar, R *rho_tot, cplx<R> *cbuf, long long n) {
+  GRID_LOOP(i, n) {
+    R r;
+    if (rho_in) {
+      r = rho_in[i];
+    } else {
+      const R a = hypot(psi[i].x, psi[i].y);
+      r = a * a;
+      if (rho_s) r = r + rho_s[i];
+      if (rho_gas) r = r + rho_gas[i];
+    }
+    if (rho_tot) rho_tot[i] = r;
+    cbuf[i] = cplx<R>{fourpiG * (r - rho_bar), (R)0};
+  }
+}
+
+// V^ = -F / (k^2 + [k^2 == 0])  (quantum-stars.py:191)
+template <typename R> __global__ void k_poisson_div(cplx<R> *c, KT<R> k, long long n) {
+  GRID_LOOP(i, n) {
+    R kx, ky, kz;
+    cell_k(k, i, kx, ky, kz);
+    const R k2 = kx * kx + ky * ky + kz * kz;
+    const R den = k2 + (k2 == (R)0 ? (R)1 : (R)0);
+    c[i] = cplx<R>{-c[i].x / den, -c[i].y / den};
+  }
+}
+
+// out = 1j * k_d * V^  (quantum-stars.py:256-258)
+template <typename R>
+__global__ void k_mul_ik(const cplx<R> *vh, int d, KT<R> k, cplx<R> *out, long long n) {
+  GRID_LOOP(i, n) {
+    R kk[3];
+    cell_k(k, i, kk[0], kk[1], kk[2]);
+    const R kd = kk[d];
+    out[i] = cplx<R>{-kd * vh[i].y, kd * vh[i].x};
+  }
+}
+
+// out = sign * Re(c) (+ b * rho) (+ v_ext)
+template <typename R>
+__global__ void k_real_part(const cplx<R> *c, R sign, const R *rho, R b, const R *vext, R *out,
+                            long long n) {
+  GRID_LOOP(i, n) {
+    R v = sign * c[i].x;
+    if (rho) v = v + b * rho[i];
+    if (vext) v = v + vext[i];
+    out[i] = v;
+  }
+}
+
+// psi = exp(-1j * coef * V) * psi, coef = m_per_hbar * dt / 2 (:301)
+template <typename R> __global__ void k_kick_plain(cplx<R> *psi, const R *V, R coef, long long n) {
+  GRID_LOOP(i, n) {
+    R s, c;
+    const R th = -coef * V[i];
+    if constexpr (sizeof(R) == 8)
+      sincos((double)th, (double *)&s, (double *)&c);
+    else
+      sincosf((float)th, (float *)&s, (float *)&c);
+    const cplx<R> z = psi[i];
+    psi[i] = cplx<R>{c * z.x - s * z.y, c * z.y + s * z.x};
+  }
+}
+
+// psi_hat *= exp(dt * (-1j * k_sq / m_per_hbar / 2))  (:308)
+template <typename R>
+__global__ void k_drift_mul(cplx<R> *c, KT<R> k, R dt, R mph, long long n) {
+  GRID_LOOP(i, n) {
+    R kx, ky, kz;
+    cell_k(k, i, kx, ky, kz);
+    const R k2 = kx * kx + ky * ky + kz * kz;
+    const R th = dt * (-(k2 / mph / (R)2));
+    R s, cc;
+    if constexpr (sizeof(R) == 8)
+      sincos((double)th, (double *)&s, (double *)&cc);
+    else
+      sincosf((float)th, (float *)&s, (float *)&cc);
+    const cplx<R> z = c[i];
+    c[i] = cplx<R>{cc * z.x - s * z.y, cc * z.y + s * z.x};
+  }
+}
+
+// a_max = max |a_grid| over the three components (:260)
+template <typename R>
+__global__ void k_amax3(const R *ax, const R *ay, const R *az, long long n, R *out) {
+  R m = (R)0;
+  GRID_LOOP(i, n) {
+    m = fmax(m, fabs(ax[i]));
+    m = fmax(m, fabs(ay[i]));
+    m = fmax(m, fabs(az[i]));
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) {
+    if constexpr (sizeof(R) == 4)
+      atomic_max_nonneg((unsigned int *)out, (float)m);
+    else
+      atomic_max_nonneg((unsigned long long *)out, (double)m);
+  }
+}
+
+// v += a * dt (quantum-gas-bh.py:262-264)
+template <typename R>
+__global__ void k_gas_kick(R *vx, R *vy, R *vz, const R *ax, const R *ay, const R *az, R dt,
+                           long long n) {
+  GRID_LOOP(i, n) {
+    vx[i] = vx[i] + ax[i] * dt;
+    vy[i] = vy[i] + ay[i] * dt;
+    vz[i] = vz[i] + az[i] * dt;
+  }
+}
+
+int launch_build_rho(bool dbl, const void *psi, const void *rho_s, const void *rho_gas,
+                     const void *rho_in, double fourpiG, double rho_bar, void *rho_tot,
+                     void *cbuf, long long ncell, cudaStream_t st) {
+  if (dbl)
+    k_build_rho<double><<<grid_blocks(ncell), 256, 0, st>>>(
+        (const double2 *)psi, (const double *)rho_s, (const double *)rho_gas,
+        (const double *)rho_in, fourpiG, rho_bar, (double *)rho_tot, (double2 *)cbuf, ncell);
+  else
+    k_build_rho<float><<<grid_blocks(ncell), 256, 0, st>>>(
+        (const float2 *)psi, (const float *)rho_s, (const float *)rho_gas, (const float *)rho_in,
+        (float)fourpiG, (float)rho_bar, (float *)rho_tot, (float2 *)cbuf, ncell);
+  QJ_CK_LAUNCH();
+  return 0;
+}
+
+int launch_poisson_div(bool dbl, void *cbuf, const KTabs &k, long long ncell, cudaStream_t st) {
+  if (dbl)
+    k_poisson_div<double><<<grid_blocks(ncell), 256, 0, st>>>((double2 *)cbuf, cast_k<double>(k), ncell);
+  else
+    k_poisson_div<float><<<grid_blocks(ncell), 256, 0, st>>>((float2 *)cbuf, cast_k<float>(k), ncell);
+  QJ_CK_LAUNCH();
+  return 0;
+}
+
+int launch_mul_ik(bool dbl, const void *vh, int d, const KTabs &k, void *out, long long ncell,
+                  cudaStream_t st) {
+  if (dbl)
+    k_mul_ik<double><<<grid_blocks(ncell), 256, 0, st>>>((const double2 *)vh, d, cast_k<double>(k),
+                                                         (double2 *)out, ncell);
+  else
+    k_mul_ik<float><<<grid_blocks(ncell), 256, 0, st>>>((const float2 *)vh, d, cast_k<float>(k),
+                                                        (float2 *)out, ncell);
+  QJ_CK_LAUNCH();
+  return 0;
+}
+
+int launch_real_part(bool dbl, const void *c, double sign, const void *rho, double b,
+                     const void *vext, void *out, long long ncell, cudaStream_t st) {
+  if (dbl)
+    k_real_part<double><<<grid_blocks(ncell), 256, 0, st>>>(
+        (const double2 *)c, sign, (const double *)rho, b, (const double *)vext, (double *)out, ncell);
+  else
+    k_real_part<float><<<grid_blocks(ncell), 256, 0, st>>>(
+        (const float2 *)c, (float)sign, (const float *)rho, (float)b, (const float *)vext,
+        (float *)out, ncell);
+  QJ_CK_LAUNCH();
+  return 0;
+}
+
+int launch_kick_plain(bool dbl, void *psi, const void *V, double coef, long long ncell,
+                      cudaStream_t st) {
+  if (dbl)
+    k_kick_plain<double><<<grid_blocks(ncell), 256, 0, st>>>((double2 *)psi, (const double *)V, coef, ncell);
+  else
+    k_kick_plain<float><<<grid_blocks(ncell), 256, 0, st>>>((float2 *)psi, (const float *)V, (float)coef, ncell);
+  QJ_CK_LAUNCH();
+  return 0;
+}
+
+int launch_drift_mul(bool dbl, void *cbuf, const KTabs &k, double dt_kin, double m_per_hbar,
+                     long long ncell, cudaStream_t st) {
+  if (dbl)
+    k_drift_mul<double><<<grid_blocks(ncell), 256, 0, st>>>((double2 *)cbuf, cast_k<double>(k), dt_kin,
+                                                            m_per_hbar, ncell);
+  else
+    k_drift_mul<float><<<grid_blocks(ncell), 256, 0, st>>>((float2 *)cbuf, cast_k<float>(k),
+                                                           (float)dt_kin, (float)m_per_hbar, ncell);
+  QJ_CK_LAUNCH();
+  return 0;
+}
+
+int launch_amax3(bool dbl, const void *ax, const void *ay, const void *az, long long ncell,
+                 void *bits, cudaStream_t st) {
+  if (dbl)
+    k_amax3<double><<<grid_blocks(ncell), 256, 0, st>>>((const double *)ax, (const double *)ay,
+                                                        (const double *)az, ncell, (double *)bits);
+  else
+    k_amax3<float><<<grid_blocks(ncell), 256, 0, st>>>((const float *)ax, (const float *)ay,
+                                                       (const float *)az, ncell, (float *)bits);
+  QJ_CK_LAUNCH();
+  return 0;
+}
+
+int launch_gas_kick(bool dbl, void *vx, void *vy, void *vz, const void *ax, const void *ay,
+                    const void *az, double dt, long long ncell, cudaStream_t st) {
+  if (dbl)
+    k_gas_kick<double><<<grid_blocks(ncell), 256, 0, st>>>(
+        (double *)vx, (double *)vy, (double *)vz, (const double *)ax, (const double *)ay,
+        (const double *)az, dt, ncell);
+  else
+    k_gas_kick<float><<<grid_blocks(ncell), 256, 0, st>>>(
+        (float *)vx, (float *)vy, (float *)vz, (const float *)ax, (const float *)ay,
+        (const float *)az, (float)dt, ncell);
+  QJ_CK_LAUNCH();
+  return 0;
+}
+
+}  // namespace qj

@@ -1,0 +1,5 @@
+"""qj: B200 (sm_100a) kick-drift-kick Schroedinger-Poisson step of
+quantum-jax, behind the C ABI of libqj.so (include/qj.h)."""
+
+from ._lib import QjError, lib  # noqa: F401
+from .core import FUSED_F32, PLAIN_F64, Grid, Phys, Plan, StarsStep  # noqa: F401

@@ -1,0 +1,89 @@
+"""ctypes binding of libqj.so (the C ABI declared in include/qj.h).
+
+The library is built in-tree (``python quantum-jax_b200/build.py``) and loaded
+from this directory.  There is no fallback: if the library is missing or
+fails to load, every entry point raises.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libqj.so")
+
+QJ_OK = 0
+QJ_ERR_ARG = 1
+QJ_ERR_CUDA = 2
+QJ_ERR_NONFINITE = 3
+QJ_ERR_TIMEOUT = 4
+QJ_ERR_ALLOC = 5
+QJ_PLAIN_F64 = 0
+QJ_FUSED_F32 = 1
+
+# Every symbol include/qj.h declares, with (restype, argtypes).
+c_void_p, c_int, c_double, c_int64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int64
+
+
+class QjGrid(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("nz", ctypes.c_int32),
+                ("Lx", c_double), ("Ly", c_double), ("Lz", c_double)]
+
+
+class QjPhys(ctypes.Structure):
+    _fields_ = [("m_per_hbar", c_double), ("G", c_double), ("rho_bar", c_double),
+                ("b_coeff", c_double), ("cs", c_double), ("c_light", c_double)]
+
+
+SIGNATURES = {
+    "qj_plan_create": (c_int, [ctypes.POINTER(c_void_p), ctypes.POINTER(QjGrid),
+                               ctypes.POINTER(QjPhys), c_int, c_int]),
+    "qj_plan_destroy": (c_int, [c_void_p]),
+    "qj_plan_set_phys": (c_int, [c_void_p, ctypes.POINTER(QjPhys)]),
+    "qj_last_error": (ctypes.c_char_p, []),
+    "qj_get_potential": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
+    "qj_bin_stars": (c_int, [c_void_p, c_void_p, c_int, c_double, c_void_p, c_void_p, c_void_p]),
+    "qj_get_acceleration": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p,
+                                    c_void_p]),
+    "qj_kdk_step": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_double, c_double,
+                            c_int, c_int, c_void_p, c_void_p, c_void_p]),
+    "qj_fft3d": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
+    "qj_plan_workspace_bytes": (c_int64, [c_void_p]),
+    "qj_launch_count": (c_int64, []),
+    "qj_profile_enable": (c_int, [c_int]),
+    "qj_profile_read": (c_int, [ctypes.POINTER(c_double), ctypes.POINTER(c_int64), c_int]),
+}
+
+
+class QjError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"libqj error {code}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def lib():
+    """Load libqj.so once; raise if it is absent (no CPU fallback exists)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `python quantum-jax_b200/build.py`"
+            )
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(rc):
+    if rc != QJ_OK:
+        msg = lib().qj_last_error()
+        raise QjError(rc, msg.decode() if msg else "")
+    return rc

@@ -1,0 +1,233 @@
+"""Torch front end of libqj: plans and the reference's step functions.
+
+The reference scripts keep the grid and physical constants in module globals
+(quantum-stars.py:61-157); here they live in a :class:`Plan`.  Every method
+mirrors one reference function with the same argument meaning and returns
+the same quantities; tensors are CUDA tensors and every call is asynchronous
+on torch's current stream.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+import math
+
+import torch
+
+from . import _lib
+from ._lib import QJ_FUSED_F32, QJ_PLAIN_F64, check, lib
+
+FUSED_F32 = QJ_FUSED_F32
+PLAIN_F64 = QJ_PLAIN_F64
+
+
+@dataclasses.dataclass
+class Grid:
+    """Box [0,Lx]x[0,Ly]x[0,Lz] with nx x ny x nz cells (quantum-stars.py:73-80)."""
+
+    nx: int
+    ny: int
+    nz: int
+    Lx: float = 1.0
+    Ly: float = 1.0
+    Lz: float = 1.0
+
+    @property
+    def shape(self):
+        return (self.nx, self.ny, self.nz)
+
+    @property
+    def dx(self):
+        return self.Lx / self.nx
+
+    @property
+    def dy(self):
+        return self.Ly / self.ny
+
+    @property
+    def dz(self):
+        return self.Lz / self.nz
+
+    @property
+    def ncell(self):
+        return self.nx * self.ny * self.nz
+
+
+@dataclasses.dataclass
+class Phys:
+    """Constants the reference reads as globals (quantum-stars.py:83-125)."""
+
+    m_per_hbar: float = 1.0
+    G: float = 1.0 / (4.0 * math.pi)
+    rho_bar: float = 1.0
+    b_coeff: float = 0.0
+    cs: float = 1.0
+    c_light: float = 299792.458
+
+
+def _stream():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else None
+
+
+class Plan:
+    """A libqj plan: grid, constants, tables and device workspace.
+
+    precision: ``FUSED_F32`` (complex64 psi, float32 fields and particles) or
+    ``PLAIN_F64`` (complex128 / float64, unfused reference-order kernels).
+    """
+
+    def __init__(self, grid: Grid, phys: Phys, precision=FUSED_F32, max_particles=4096):
+        self.grid = grid
+        self.phys = phys
+        self.precision = precision
+        self.max_particles = int(max_particles)
+        self.rdtype = torch.float32 if precision == FUSED_F32 else torch.float64
+        self.cdtype = torch.complex64 if precision == FUSED_F32 else torch.complex128
+        self._h = ctypes.c_void_p()
+        g = _lib.QjGrid(grid.nx, grid.ny, grid.nz, grid.Lx, grid.Ly, grid.Lz)
+        check(lib().qj_plan_create(ctypes.byref(self._h), ctypes.byref(g),
+                                   ctypes.byref(self._phys_struct()), int(precision),
+                                   self.max_particles))
+
+    def _phys_struct(self):
+        p = self.phys
+        return _lib.QjPhys(p.m_per_hbar, p.G, p.rho_bar, p.b_coeff, p.cs, p.c_light)
+
+    def set_phys(self, phys: Phys):
+        self.phys = phys
+        check(lib().qj_plan_set_phys(self._h, ctypes.byref(self._phys_struct())))
+
+    def close(self):
+        if self._h:
+            torch.cuda.synchronize()
+            lib().qj_plan_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def workspace_bytes(self):
+        return int(lib().qj_plan_workspace_bytes(self._h))
+
+    # ----- argument checks -----
+    def _field(self, t, name, complex_=False):
+        dt = self.cdtype if complex_ else self.rdtype
+        if not isinstance(t, torch.Tensor) or not t.is_cuda:
+            raise TypeError(f"{name} must be a CUDA tensor")
+        if t.dtype != dt:
+            raise TypeError(f"{name} must be {dt}, got {t.dtype}")
+        if tuple(t.shape) != self.grid.shape or not t.is_contiguous():
+            raise ValueError(f"{name} must be a contiguous {self.grid.shape} tensor")
+        return t
+
+    def _particles(self, t, name, n=None):
+        if not isinstance(t, torch.Tensor) or not t.is_cuda or t.dtype != self.rdtype:
+            raise TypeError(f"{name} must be a CUDA {self.rdtype} tensor")
+        if t.dim() != 2 or t.shape[1] != 3 or not t.is_contiguous():
+            raise ValueError(f"{name} must be a contiguous [n, 3] tensor")
+        if n is not None and t.shape[0] != n:
+            raise ValueError(f"{name} must have {n} rows")
+        return t
+
+    # ----- reference functions -----
+    def get_potential(self, rho, self_interaction=False):
+        """quantum-stars.py:189-193."""
+        self._field(rho, "rho")
+        V = torch.empty_like(rho)
+        check(lib().qj_get_potential(self._h, _ptr(rho), _ptr(V), int(bool(self_interaction)),
+                                     _stream()))
+        return V
+
+    def bin_stars(self, pos, m_s=None, masses=None):
+        """quantum-stars.py:212-247 (m_s per star) / quantum-gas-bh.py:414-449
+        (``masses`` per particle)."""
+        self._particles(pos, "pos")
+        n = pos.shape[0]
+        if masses is not None:
+            if masses.dtype != self.rdtype or masses.shape != (n,) or not masses.is_cuda:
+                raise ValueError("masses must be a CUDA [n] tensor of the plan's real type")
+        elif m_s is None:
+            raise ValueError("give m_s or masses")
+        rho = torch.empty(self.grid.shape, dtype=self.rdtype, device=pos.device)
+        check(lib().qj_bin_stars(self._h, _ptr(pos), n, float(m_s or 0.0), _ptr(masses),
+                                 _ptr(rho), _stream()))
+        return rho
+
+    def get_acceleration(self, pos, rho):
+        """quantum-stars.py:250-288 -> (acc [n, 3], a_max 0-d float64 tensor)."""
+        self._particles(pos, "pos")
+        self._field(rho, "rho")
+        acc = torch.empty_like(pos)
+        a_max = torch.empty((), dtype=torch.float64, device=pos.device)
+        check(lib().qj_get_acceleration(self._h, _ptr(pos), pos.shape[0], _ptr(rho), _ptr(acc),
+                                        _ptr(a_max), _stream()))
+        return acc, a_max
+
+    def fftn(self, x, inverse=False):
+        """jnp.fft.fftn / ifftn with the plan's pencil kernels."""
+        self._field(x, "x", complex_=True)
+        out = torch.empty_like(x)
+        check(lib().qj_fft3d(self._h, _ptr(x), _ptr(out), 1 if inverse else -1, _stream()))
+        return out
+
+    def kdk_step(self, psi, pos, vel, diag, dt, nsteps=1, m_s=0.0, self_interaction=False,
+                 v_ext=None):
+        """nsteps x compute_step (quantum-stars.py:295-330), in place.
+
+        diag: CUDA float64 tensor [3] = (t, a_max, dt_s), updated in place."""
+        self._field(psi, "psi", complex_=True)
+        n_s = 0
+        if pos is not None:
+            self._particles(pos, "pos")
+            n_s = pos.shape[0]
+            self._particles(vel, "vel", n_s)
+        if diag.dtype != torch.float64 or diag.numel() != 3 or not diag.is_cuda:
+            raise ValueError("diag must be a CUDA float64 tensor of 3 elements")
+        if v_ext is not None:
+            self._field(v_ext, "v_ext")
+        check(lib().qj_kdk_step(self._h, _ptr(psi), _ptr(pos) if n_s else None,
+                                _ptr(vel) if n_s else None, n_s, float(m_s), float(dt),
+                                int(nsteps), int(bool(self_interaction)), _ptr(v_ext),
+                                _ptr(diag), _stream()))
+        return psi, pos, vel, diag
+
+
+class StarsStep:
+    """The quantum-stars.py step as a drop-in: ``compute_step`` and ``update``
+    with the same signatures and state dict keys (quantum-stars.py:295-351).
+
+    The constants the script holds as globals (grid, m_per_hbar, G, rho_bar,
+    m_s, dt, b_coeff with --self_interaction) are given once here."""
+
+    def __init__(self, grid: Grid, phys: Phys, m_s: float, dt: float, n_s: int,
+                 self_interaction=False, precision=FUSED_F32, v_ext=None):
+        self.plan = Plan(grid, phys, precision, max_particles=max(n_s, 1))
+        self.m_s = float(m_s)
+        self.dt = float(dt)
+        self.self_interaction = self_interaction
+        self.v_ext = v_ext
+
+    def compute_step(self, psi, pos, vel, t, a_max, dt_s, nsteps=1):
+        """Returns (psi, pos, vel, t, a_max, dt_s); tensors are updated in place."""
+        dev = psi.device
+        diag = torch.tensor([float(t), float(a_max), float(dt_s)], dtype=torch.float64,
+                            device=dev)
+        self.plan.kdk_step(psi, pos, vel, diag, self.dt, nsteps, self.m_s,
+                           self.self_interaction, self.v_ext)
+        return psi, pos, vel, diag[0], diag[1], diag[2]
+
+    def update(self, _, state):
+        """quantum-stars.py:333-351: one step on the state dict."""
+        (state["psi"], state["pos"], state["vel"], state["t"], state["a_max"],
+         state["dt_s"]) = self.compute_step(state["psi"], state["pos"], state["vel"],
+                                            state["t"], state["a_max"], state["dt_s"])
+        return state
