@@ -119,6 +119,25 @@ int qj_kdk_step(qj_plan *plan, void *psi, void *pos, void *vel, int n_s,
 int qj_fft3d(qj_plan *plan, const void *in, void *out, int direction,
              void *stream);
 
+/* get_potential in single precision that allocates no device memory.  No
+ * counterpart in the reference: it exists for callers that must not call
+ * cudaMalloc, such as a JAX / XLA FFI handler (XLA reserves most of the device
+ * memory up front, and cudaMalloc / cudaFree would also synchronise the device
+ * inside XLA's asynchronous schedule) or a host with a fixed memory budget.
+ * Same result as qj_get_potential on a QJ_FUSED_F32 plan, without a plan.
+ * rho, V: float32 device arrays [nx][ny][nz]; each axis 16, 32 or 64 cells
+ * (at most QJ_NOALLOC_MAX_CELLS), nz a multiple of 16; other sizes return
+ * QJ_ERR_ARG.  Its scratch is a fixed 2 MiB array held by every GPU that
+ * loads libqj until the process exits; the first call on a device looks up
+ * that array's device address, so make that first call before any stream
+ * capture.  All calls on a device share the array: calls that overlap on the
+ * GPU (unordered streams) race; calls on one stream are safe. */
+#define QJ_NOALLOC_MAX_AXIS 64
+#define QJ_NOALLOC_MAX_CELLS (64 * 64 * 64)
+int qj_get_potential_f32_noalloc(const qj_grid *grid, const qj_phys *phys,
+                                 const float *rho, float *V,
+                                 int self_interaction, void *stream);
+
 /* Bytes of device workspace the plan holds. */
 int64_t qj_plan_workspace_bytes(const qj_plan *plan);
 
