@@ -132,6 +132,7 @@ struct qj_plan {
   void *vals = nullptr, *uval = nullptr, *A = nullptr, *acc = nullptr;
   int *pstart = nullptr;
   int *n_unique = nullptr;
+  StarBufs sb{};  // fused path star data
   void *amax = nullptr, *dts = nullptr;  // real type scalars
   void *tmp_scalar = nullptr;
 };
@@ -244,6 +245,16 @@ FusedArgs fused_args(const qj_plan *P, int axis) {
   return a;
 }
 
+void set_stars(FusedArgs &a, const qj_plan *P) {
+  a.has_stars = 1;
+  a.sidx = P->sb.sidx;
+  a.sw0 = P->sb.sw0;
+  a.sw1 = P->sb.sw1;
+  a.perm = P->sb.perm;
+  a.bstart = P->sb.bstart;
+  a.A = P->sb.A;
+}
+
 int ensure_prop(qj_plan *P, double dtk, cudaStream_t st) {
   if (P->prop_dtk == dtk) return 0;
   const int m = std::max(P->n[0], std::max(P->n[1], P->n[2]));
@@ -280,21 +291,19 @@ int fused_kdk(qj_plan *P, float2 *psi, float *pos, float *vel, int n_s, double m
   const bool parts = n_s > 0;
   QJ_TRY(ensure_prop(P, dt, st));
   QJ_TRY(launch_diag_load(false, diag, P->amax, st));
+  if (parts) QJ_TRY(launch_set_scalar(false, P->dts, INFINITY, st));
   const double half_coef = P->ph.m_per_hbar * dt / 2.0;
   int q = 2;
   if (parts) {
     if (prof_on()) prof_mark_begin(st);
-    QJ_TRY(deposit_list(P, pos, n_s, m_s, nullptr, q, false, P->dts, st));
+    QJ_TRY(launch_stars_prepare(pos, n_s, nullptr, m_s, geom(P), q, P->sb, st));
+    QJ_TRY(launch_bucket_sort(n_s, n_pencils(P, q), P->sb, st));
     if (prof_on()) prof_mark_end(7, st);
   }
   {
     FusedArgs a = fused_args(P, q);
     a.psi = psi;
-    if (parts) {
-      a.pstart = P->pstart;
-      a.ukey = P->ukey;
-      a.uval = (const float *)P->uval;
-    }
+    if (parts) set_stars(a, P);
     QJ_TRY(launch_fused(M_DENSITY, P->n[q], a, st));
   }
   for (int k = 0; k <= nsteps; ++k) {
@@ -321,17 +330,11 @@ int fused_kdk(qj_plan *P, float2 *psi, float *pos, float *vel, int n_s, double m
       a.b_coeff = si ? (float)P->ph.b_coeff : 0.0f;
       a.v_ext = vext;
       a.do_drift = last ? 0 : 1;
-      if (parts) {
-        a.pstart = P->pstart;
-        a.ukey = P->ukey;
-        a.uval = (const float *)P->uval;
-        a.A = (float *)P->A;
-      }
+      if (parts) set_stars(a, P);
       QJ_TRY(launch_fused(M_KICK, P->n[q], a, st));
     }
     if (parts) {
       if (prof_on()) prof_mark_begin(st);
-      QJ_TRY(launch_gather_unique(false, pos, n_s, geom(P), P->A, P->cell_u, P->acc, st));
       UpdateArgs u;
       std::memset(&u, 0, sizeof(u));
       u.n = n_s;
@@ -340,17 +343,11 @@ int fused_kdk(qj_plan *P, float2 *psi, float *pos, float *vel, int n_s, double m
       u.k1 = !last;
       u.drift = !last;
       u.dts_bits = P->dts;
-      u.q_next = r;
-      u.keys = last ? nullptr : P->keys;
-      u.vals = P->vals;
+      u.q_next = last ? -1 : r;
       u.m_s = m_s;
-      QJ_TRY(launch_particles_update(false, pos, vel, P->acc, geom(P), u, st));
+      QJ_TRY(launch_update_fused(pos, vel, geom(P), u, P->sb, st));
+      if (!last) QJ_TRY(launch_bucket_sort(n_s, n_pencils(P, r), P->sb, st));
       if (prof_on()) prof_mark_end(8, st);
-      if (!last) {
-        if (prof_on()) prof_mark_begin(st);
-        QJ_TRY(deposit_list(P, pos, n_s, m_s, nullptr, r, true, P->dts, st));
-        if (prof_on()) prof_mark_end(7, st);
-      }
     }
     if (!last) {
       {
@@ -361,11 +358,7 @@ int fused_kdk(qj_plan *P, float2 *psi, float *pos, float *vel, int n_s, double m
       {
         FusedArgs a = fused_args(P, r);
         a.psi = psi;
-        if (parts) {
-          a.pstart = P->pstart;
-          a.ukey = P->ukey;
-          a.uval = (const float *)P->uval;
-        }
+        if (parts) set_stars(a, P);
         QJ_TRY(launch_fused(M_DRIFT_DENSITY, P->n[r], a, st));
       }
     }
@@ -568,6 +561,19 @@ int qj_plan_create(qj_plan **plan, const qj_grid *grid, const qj_phys *phys, int
   if ((rc = dev_alloc(P, &P->acc, 3 * (np8 / 8) * P->rsz))) return fail(rc);
   long long npen = 0;
   for (int a = 0; a < 3; ++a) npen = std::max(npen, P->ncell / n[a]);
+  if (!P->dbl) {
+    const size_t np = (size_t)std::max(1, max_particles);
+    StarBufs &b = P->sb;
+    if ((rc = dev_alloc_t(P, &b.sidx, np))) return fail(rc);
+    if ((rc = dev_alloc_t(P, &b.sw0, np))) return fail(rc);
+    if ((rc = dev_alloc_t(P, &b.sw1, np))) return fail(rc);
+    if ((rc = dev_alloc_t(P, &b.bkey, np))) return fail(rc);
+    if ((rc = dev_alloc_t(P, &b.perm, np))) return fail(rc);
+    if ((rc = dev_alloc_t(P, &b.skey, np))) return fail(rc);
+    if ((rc = dev_alloc_t(P, &b.sortbuf, 4 * np))) return fail(rc);
+    if ((rc = dev_alloc_t(P, &b.bstart, npen + 1))) return fail(rc);
+    b.A = (float *)P->A;
+  }
   if ((rc = dev_alloc_t(P, &P->pstart, npen + 1))) return fail(rc);
   if ((rc = dev_alloc_t(P, &P->n_unique, 1))) return fail(rc);
   if ((rc = dev_alloc(P, &P->amax, 8))) return fail(rc);
@@ -659,7 +665,17 @@ int qj_bin_stars(qj_plan *P, const void *pos, int n, double m_s, const void *mas
     set_error("qj_bin_stars: bad argument (n=%d, max_particles=%d)", n, P ? P->max_particles : 0);
     return QJ_ERR_ARG;
   }
-  return plain_bin(P, pos, n, m_s, masses, rho_s, (cudaStream_t)stream);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (P->dbl) return plain_bin(P, pos, n, m_s, masses, rho_s, st);
+  // single precision: the pencil-bucket deposit of the fused step
+  FusedArgs a = fused_args(P, 2);
+  a.rho_out = (float *)rho_s;
+  if (n > 0) {
+    QJ_TRY(launch_stars_prepare(pos, n, masses, m_s, geom(P), 2, P->sb, st));
+    QJ_TRY(launch_bucket_sort(n, n_pencils(P, 2), P->sb, st));
+    set_stars(a, P);
+  }
+  return launch_fused(M_DEPOSIT, P->n[2], a, st);
 }
 
 int qj_get_acceleration(qj_plan *P, const void *pos, int n, const void *rho, void *acc,

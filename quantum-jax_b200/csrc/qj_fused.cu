@@ -69,6 +69,24 @@ static int dispatch_mode(int n, const FusedArgs &a, cudaStream_t st) {
   return 1;
 }
 
+// The dense deposit runs along z only.
+static int dispatch_deposit(int n, const FusedArgs &a, cudaStream_t st) {
+  if (a.axis != 2) {
+    set_error("internal: deposit pass must run along z");
+    return 1;
+  }
+  switch (n) {
+    case 16: return run_fused<16, true, M_DEPOSIT>(a, st);
+    case 32: return run_fused<32, true, M_DEPOSIT>(a, st);
+    case 64: return run_fused<64, true, M_DEPOSIT>(a, st);
+    case 128: return run_fused<128, true, M_DEPOSIT>(a, st);
+    case 256: return run_fused<256, true, M_DEPOSIT>(a, st);
+    case 512: return run_fused<512, true, M_DEPOSIT>(a, st);
+  }
+  set_error("unsupported FFT length %d", n);
+  return 1;
+}
+
 static int launch_fused_impl(int mode, int n, const FusedArgs &a, cudaStream_t st) {
   switch (mode) {
     case M_DENSITY: return dispatch_mode<M_DENSITY>(n, a, st);
@@ -78,6 +96,7 @@ static int launch_fused_impl(int mode, int n, const FusedArgs &a, cudaStream_t s
     case M_KICK: return dispatch_mode<M_KICK>(n, a, st);
     case M_DRIFT: return dispatch_mode<M_DRIFT>(n, a, st);
     case M_DRIFT_DENSITY: return dispatch_mode<M_DRIFT_DENSITY>(n, a, st);
+    case M_DEPOSIT: return dispatch_deposit(n, a, st);
   }
   set_error("internal: bad pass mode %d", mode);
   return 1;

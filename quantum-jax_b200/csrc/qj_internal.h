@@ -92,6 +92,24 @@ struct UpdateArgs {
 int launch_particles_update(bool dbl, void *pos, void *vel, const void *acc, const CicGeomD &g,
                             const UpdateArgs &u, cudaStream_t st);
 
+// ----- pencil-bucket star data of the fused path -----
+struct StarBufs {
+  int4 *sidx;        // [n] lower CIC corner (wrapped)
+  float4 *sw0;       // [n] (w_i x, y, z, m / vol)
+  float4 *sw1;       // [n] (w_ip1 x, y, z, 0)
+  unsigned *bkey;    // [n] bucket = pencil of the lower corner (pass orientation)
+  unsigned *perm;    // [n] stars sorted by (bucket, star)
+  unsigned *skey;    // [n] sorted bucket keys
+  int *bstart;       // [n_buckets + 1]
+  unsigned *sortbuf; // [4 n] global sort scratch (large n)
+  float *A;          // [8 n][3] accelerations at the 8 corners of each star
+};
+int launch_stars_prepare(const void *pos, int n, const void *masses, double m_s,
+                         const CicGeomD &g, int q, const StarBufs &b, cudaStream_t st);
+int launch_bucket_sort(int n, int n_buckets, const StarBufs &b, cudaStream_t st);
+int launch_update_fused(void *pos, void *vel, const CicGeomD &g, const UpdateArgs &u,
+                        const StarBufs &b, cudaStream_t st);
+
 // ----- plain elementwise kernels (qj_plain.cu), R = float or double -----
 struct KTabs {
   const void *k[3];  // per-axis k tables of the real type

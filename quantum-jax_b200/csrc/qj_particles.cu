@@ -9,6 +9,7 @@
 // scatter-adds each (quantum-stars.py:212-247), so the float32 result matches
 // a float32 evaluation of the reference bit for bit.
 #include <cstdio>
+#include <mutex>
 
 #include "qj_internal.h"
 
@@ -428,6 +429,239 @@ int launch_particles_update(bool dbl, void *pos, void *vel, const void *acc, con
         (float *)pos, (float *)vel, (const float *)acc, u.n, cast_geom<float>(g), (float)u.dt,
         u.k2, u.k1, u.drift, (float *)u.dts_bits, u.q_next, u.keys, (float *)u.vals,
         (const float *)u.masses, (float)fac);
+  QJ_CK_LAUNCH();
+  return 0;
+}
+
+// ----- pencil-bucket deposit for the fused passes -----
+//
+// Each star is filed under the pencil (in the pass orientation q) that holds
+// its lower CIC corner.  A pencil pass then finds every star touching its
+// pencil in the four neighbouring buckets, and visits them in star order so
+// each cell still sums its contributions in the reference's order.
+
+// Corner number (reference order, quantum-stars.py:220-243) of the corner
+// with ip1 bits (bx, by, bz): index bx + 2 by + 4 bz.
+__constant__ int c_corner_of_bits[8] = {0, 1, 2, 4, 3, 5, 6, 7};
+
+__device__ __forceinline__ unsigned bucket_of(int ix, int iy, int iz, int q, const int n[3]) {
+  if (q == 2) return (unsigned)ix * (unsigned)n[1] + (unsigned)iy;
+  if (q == 0) return (unsigned)iy * (unsigned)n[2] + (unsigned)iz;
+  return (unsigned)ix * (unsigned)n[2] + (unsigned)iz;
+}
+
+// Per-star CIC data: lower corner (wrapped), weights w_i / w_ip1 per axis and
+// the deposit factor m / vol, all in the reference's float32 order.
+__device__ __forceinline__ void star_prepare(const float *pos, int s, const CicGeom<float> &g,
+                                             float fac, int q, int4 *sidx, float4 *sw0,
+                                             float4 *sw1, unsigned *bkey) {
+  int i0[3], i1[3];
+  float w0[3], w1[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) cic_axis<float>(pos[3 * s + d], g.d[d], g.n[d], i0[d], i1[d], w0[d], w1[d]);
+  sidx[s] = int4{i0[0], i0[1], i0[2], 0};
+  sw0[s] = float4{w0[0], w0[1], w0[2], fac};
+  sw1[s] = float4{w1[0], w1[1], w1[2], 0.0f};
+  bkey[s] = bucket_of(i0[0], i0[1], i0[2], q, g.n);
+}
+
+__global__ void k_stars_prepare(const float *pos, int n, const float *masses, float fac_all,
+                                CicGeom<float> g, int q, int4 *sidx, float4 *sw0, float4 *sw1,
+                                unsigned *bkey) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  star_prepare(pos, s, g, cic_fac<float>(masses, s, fac_all, g.vol), q, sidx, sw0, sw1, bkey);
+}
+
+int launch_stars_prepare(const void *pos, int n, const void *masses, double m_s,
+                         const CicGeomD &g, int q, const StarBufs &b, cudaStream_t st) {
+  if (n <= 0) return 0;
+  const int T = 128, B = (n + T - 1) / T;
+  const double fac = m_s / (g.d[0] * g.d[1] * g.d[2]);
+  k_stars_prepare<<<B, T, 0, st>>>((const float *)pos, n, (const float *)masses, (float)fac,
+                                   cast_geom<float>(g), q, b.sidx, b.sw0, b.sw1, b.bkey);
+  QJ_CK_LAUNCH();
+  return 0;
+}
+
+// Single-CTA stable LSD radix sort (8-bit digits) of the stars by bucket;
+// buffers in shared memory up to kSortSmemMax stars, else in global scratch.
+constexpr int kSortSmemMax = 8192;
+
+__global__ void __launch_bounds__(1024)
+    k_bucket_sort(const unsigned *bkey, int n, unsigned nbits, unsigned *gbuf, int use_smem,
+                  unsigned *perm, unsigned *skey) {
+  extern __shared__ unsigned dyn[];
+  __shared__ unsigned hist[32 * 256];
+  __shared__ unsigned dbase[256];
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  unsigned *buf = use_smem ? dyn : gbuf;
+  unsigned *kA = buf, *iA = buf + n, *kB = buf + 2 * n, *iB = buf + 3 * n;
+  const int chunk = (n + 31) / 32;
+  const int beg = min(n, w * chunk), end = min(n, beg + chunk);
+  const unsigned *kin = bkey;
+  const unsigned *iin = nullptr;
+  unsigned *kout = kA, *iout = iA;
+  for (unsigned shift = 0; shift < nbits; shift += 8) {
+    for (int i = tid; i < 32 * 256; i += 1024) hist[i] = 0;
+    __syncthreads();
+    for (int i = beg + lane; i < end; i += 32) atomicAdd(&hist[w * 256 + ((kin[i] >> shift) & 255u)], 1u);
+    __syncthreads();
+    if (tid < 256) {
+      unsigned sum = 0;
+      for (int ww = 0; ww < 32; ++ww) {
+        const unsigned c = hist[ww * 256 + tid];
+        hist[ww * 256 + tid] = sum;
+        sum += c;
+      }
+      dbase[tid] = sum;
+    }
+    __syncthreads();
+    if (w == 0) {
+      unsigned v[8], loc = 0;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        v[j] = dbase[lane * 8 + j];
+        loc += v[j];
+      }
+      unsigned incl = loc;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+      }
+      unsigned run = incl - loc;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const unsigned c = v[j];
+        dbase[lane * 8 + j] = run;
+        run += c;
+      }
+    }
+    __syncthreads();
+    if (tid < 256)
+      for (int ww = 0; ww < 32; ++ww) hist[ww * 256 + tid] += dbase[tid];
+    __syncthreads();
+    for (int i0 = beg; i0 < end; i0 += 32) {
+      const int i = i0 + lane;
+      const bool ok = i < end;
+      unsigned k = 0, id = 0, d = 256u + (unsigned)lane;
+      if (ok) {
+        k = kin[i];
+        id = iin ? iin[i] : (unsigned)i;
+        d = (k >> shift) & 255u;
+      }
+      const unsigned peers = __match_any_sync(0xffffffffu, d);
+      const unsigned rank = __popc(peers & ((1u << lane) - 1u));
+      if (ok) {
+        const unsigned p = hist[w * 256 + d] + rank;
+        kout[p] = k;
+        iout[p] = id;
+      }
+      __syncwarp();
+      if (ok && rank == 0) hist[w * 256 + d] += __popc(peers);
+      __syncwarp();
+    }
+    __syncthreads();
+    kin = kout;
+    iin = iout;
+    kout = (kout == kA) ? kB : kA;
+    iout = (iout == iA) ? iB : iA;
+  }
+  for (int i = tid; i < n; i += 1024) {
+    perm[i] = iin ? iin[i] : (unsigned)i;
+    skey[i] = kin[i];
+  }
+}
+
+// bstart[b] = first sorted position with bucket >= b, b = 0..n_buckets.
+__global__ void k_bucket_starts(const unsigned *skey, int n, int n_buckets, int *bstart) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b > n_buckets) return;
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (skey[mid] < (unsigned)b)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  bstart[b] = lo;
+}
+
+int launch_bucket_sort(int n, int n_buckets, const StarBufs &b, cudaStream_t st) {
+  if (n <= 0) return 0;
+  const unsigned nbits = cell_bits(n_buckets);
+  const int use_smem = n <= kSortSmemMax;
+  const size_t smem = use_smem ? (size_t)16 * n : 0;
+  static std::once_flag once;
+  static cudaError_t attr_err = cudaSuccess;
+  std::call_once(once, [&] {
+    attr_err = cudaFuncSetAttribute(k_bucket_sort, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    16 * kSortSmemMax);
+  });
+  QJ_CK(attr_err);
+  k_bucket_sort<<<1, 1024, smem, st>>>(b.bkey, n, nbits < 8 ? 8 : nbits, b.sortbuf, use_smem,
+                                       b.perm, b.skey);
+  QJ_CK_LAUNCH();
+  const int T = 256, B = (n_buckets + 1 + T - 1) / T;
+  k_bucket_starts<<<B, T, 0, st>>>(b.skey, n, n_buckets, b.bstart);
+  QJ_CK_LAUNCH();
+  return 0;
+}
+
+// Leapfrog update of the fused path.  acc = sum over the 8 corners, in the
+// order of quantum-stars.py:264-287, of (w_x w_y w_z) * a(corner), with the
+// corner accelerations A[8 s + c] written by the kick pass; then the half
+// kicks, dt_s, drift and (optionally) the CIC data of the new positions.
+__global__ void k_update_fused(float *pos, float *vel, const float *A, int n, CicGeom<float> g,
+                               float dt, int k2, int k1, int drift, float *dts, int q_next,
+                               const float *masses, float fac_all, int4 *sidx, float4 *sw0,
+                               float4 *sw1, unsigned *bkey) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const float4 w0 = sw0[s], w1 = sw1[s];
+  float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    const int bx = c_corner[c][0], by = c_corner[c][1], bz = c_corner[c][2];
+    const float wp = fmul_rn(fmul_rn(bx ? w1.x : w0.x, by ? w1.y : w0.y), bz ? w1.z : w0.z);
+    const float *ac = A + 3 * (8 * s + c);
+    a0 = fadd_rn(a0, fmul_rn(wp, ac[0]));
+    a1 = fadd_rn(a1, fmul_rn(wp, ac[1]));
+    a2 = fadd_rn(a2, fmul_rn(wp, ac[2]));
+  }
+  const float acc[3] = {a0, a1, a2};
+  float v[3];
+  float dmin = INFINITY;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    v[d] = vel[3 * s + d];
+    const float h = fdiv_rn(fmul_rn(acc[d], dt), 2.0f);
+    if (k2) {
+      v[d] = fadd_rn(v[d], h);
+      dmin = fminf(dmin, fabsf(fdiv_rn(g.d[0], v[d])));
+    }
+    if (k1) v[d] = fadd_rn(v[d], h);
+    vel[3 * s + d] = v[d];
+  }
+  if (k2) atomic_min_nonneg((unsigned int *)dts, dmin);
+  if (drift) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) pos[3 * s + d] = ref_mod(fadd_rn(pos[3 * s + d], fmul_rn(v[d], dt)), g.L[d]);
+    if (q_next >= 0)
+      star_prepare(pos, s, g, cic_fac<float>(masses, s, fac_all, g.vol), q_next, sidx, sw0, sw1, bkey);
+  }
+}
+
+int launch_update_fused(void *pos, void *vel, const CicGeomD &g, const UpdateArgs &u,
+                        const StarBufs &b, cudaStream_t st) {
+  if (u.n <= 0) return 0;
+  const int T = 128, B = (u.n + T - 1) / T;
+  const double fac = u.m_s / (g.d[0] * g.d[1] * g.d[2]);
+  k_update_fused<<<B, T, 0, st>>>((float *)pos, (float *)vel, b.A, u.n, cast_geom<float>(g),
+                                  (float)u.dt, u.k2, u.k1, u.drift, (float *)u.dts_bits, u.q_next,
+                                  (const float *)u.masses, (float)fac, b.sidx, b.sw0, b.sw1, b.bkey);
   QJ_CK_LAUNCH();
   return 0;
 }

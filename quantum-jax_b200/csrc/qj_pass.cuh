@@ -32,6 +32,7 @@ enum PassMode : int {
   M_KICK = 4,
   M_DRIFT = 5,
   M_DRIFT_DENSITY = 6,
+  M_DEPOSIT = 7,  // dense star density along z (bin_stars), no transform
 };
 
 struct FusedArgs {
@@ -48,11 +49,15 @@ struct FusedArgs {
   const float2 *prop;  // drift propagator of this axis, already scaled by 1/n
   const float *k[3];   // k value per index, per axis (Nyquist negative)
   const float *kt[3];  // k with the Nyquist entry set to 0 (odd derivatives)
-  // deposit / gather list in this pass' orientation
-  const int *pstart;
-  const unsigned *ukey;
-  const float *uval;
-  float *A;  // [n_unique][3] accelerations at the deposit cells (x, y, z)
+  // stars filed by the pencil of their lower CIC corner (this pass' axis)
+  int has_stars;
+  const int4 *sidx;
+  const float4 *sw0;
+  const float4 *sw1;
+  const unsigned *perm;
+  const int *bstart;
+  float *A;  // [8 n][3] accelerations at the 8 corners of each star (x, y, z)
+  float *rho_out;  // M_DEPOSIT: dense star density
   // float64 density partial sums
   double *part;
   const double *part_in;
@@ -107,17 +112,23 @@ __device__ __forceinline__ PencilPos pencil_pos(const FusedArgs &a, int p, int T
   return pp;
 }
 
+// Element e of a thread's pencil sits at base + (t + P e) * stride; grids
+// hold at most 512^3 = 2^27 cells, so 32-bit offsets are exact.
 template <int E, typename C>
 __device__ __forceinline__ void load_pencil(C (&v)[E], const C *__restrict__ f, long long base,
                                             long long stride, int t, int P) {
+  const unsigned b = (unsigned)base + (unsigned)t * (unsigned)stride;
+  const unsigned s = (unsigned)P * (unsigned)stride;
 #pragma unroll
-  for (int e = 0; e < E; ++e) v[e] = f[base + (long long)(t + P * e) * stride];
+  for (int e = 0; e < E; ++e) v[e] = f[b + (unsigned)e * s];
 }
 template <int E, typename C>
 __device__ __forceinline__ void store_pencil(const C (&v)[E], C *__restrict__ f, long long base,
                                              long long stride, int t, int P) {
+  const unsigned b = (unsigned)base + (unsigned)t * (unsigned)stride;
+  const unsigned s = (unsigned)P * (unsigned)stride;
 #pragma unroll
-  for (int e = 0; e < E; ++e) f[base + (long long)(t + P * e) * stride] = v[e];
+  for (int e = 0; e < E; ++e) f[b + (unsigned)e * s] = v[e];
 }
 
 // Register select with a runtime index (unrolled compare, no local memory).
@@ -156,26 +167,116 @@ __device__ __forceinline__ double block_sum(double x, double *sh) {
   return s;
 }
 
+// corner number (reference order) of the corner with ip1 bits b = bx + 2 by + 4 bz
+__device__ __forceinline__ int c_corner_of_bits_dev(int b) {
+  return b == 3 ? 4 : (b == 4 ? 3 : b);
+}
+
+__device__ __forceinline__ int sel3(int a, int b, int c, int i) { return i == 0 ? a : (i == 1 ? b : c); }
+__device__ __forceinline__ float sel3f(float a, float b, float c, int i) {
+  return i == 0 ? a : (i == 1 ? b : c);
+}
+
+// The four star buckets whose stars touch this pencil: lower corners at
+// (cu, cv), (cu-1, cv), (cu, cv-1), (cu-1, cv-1) in the cross-plane axes
+// (u, v) of the pass axis q.
+struct StarRanges {
+  int lo[4], hi[4];
+  int u, v, cu, cv;
+};
+__device__ __forceinline__ StarRanges star_ranges(const FusedArgs &a, const PencilPos &pp) {
+  StarRanges r;
+  const int q = a.axis;
+  r.u = q == 1 ? 0 : (q == 2 ? 0 : 1);
+  r.v = q == 2 ? 1 : 2;
+  const int nu = r.u == 0 ? a.nx : a.ny, nv = r.v == 1 ? a.ny : a.nz;
+  r.cu = pp.c[r.u];
+  r.cv = pp.c[r.v];
+  const int cum = r.cu == 0 ? nu - 1 : r.cu - 1, cvm = r.cv == 0 ? nv - 1 : r.cv - 1;
+  const int b[4] = {r.cu * nv + r.cv, cum * nv + r.cv, r.cu * nv + cvm, cum * nv + cvm};
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    r.lo[k] = a.bstart[b[k]];
+    r.hi[k] = a.bstart[b[k] + 1];
+  }
+  return r;
+}
+
+// Visit the stars touching this pencil; with ORDERED, in increasing star
+// index (a 4-way merge of the buckets, each already in star order).  For each
+// star and each of its two corners on the pencil (positions i0_q and
+// i0_q + 1), f(s, corner, m, wx, wy, wz, fac) is called on the thread that
+// owns position m.
+template <int N, bool ORDERED, class F>
+__device__ __forceinline__ void for_star_corners(const FusedArgs &a, StarRanges r, int t, int P, F &&f) {
+  const int q = a.axis;
+  while (true) {
+    int kb = -1;
+    unsigned s = 0xffffffffu;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (r.lo[k] < r.hi[k]) {
+        const unsigned sk = a.perm[r.lo[k]];
+        if (!ORDERED) {
+          if (kb < 0) {
+            kb = k;
+            s = sk;
+          }
+        } else if (sk < s) {
+          s = sk;
+          kb = k;
+        }
+      }
+    }
+    if (kb < 0) break;
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      if (k == kb) r.lo[k]++;
+    const int4 id = a.sidx[s];
+    const float4 w0 = a.sw0[s], w1 = a.sw1[s];
+    const int bu = (r.cu == sel3(id.x, id.y, id.z, r.u)) ? 0 : 1;
+    const int bv = (r.cv == sel3(id.x, id.y, id.z, r.v)) ? 0 : 1;
+    const int q0 = sel3(id.x, id.y, id.z, q);
+#pragma unroll
+    for (int cq = 0; cq < 2; ++cq) {
+      int m = q0 + cq;
+      if (m >= N) m -= N;
+      if (m % P == t) {
+        const int bx = q == 0 ? cq : (r.u == 0 ? bu : bv);
+        const int by = q == 1 ? cq : (r.u == 1 ? bu : bv);
+        const int bz = q == 2 ? cq : bv;
+        f(s, bx + 2 * by + 4 * bz, m, bx ? w1.x : w0.x, by ? w1.y : w0.y, bz ? w1.z : w0.z, w0.w);
+      }
+    }
+  }
+}
+
 // rho = |psi|^2 + rho_stars (+ rho_gas), element by element (float32 order
-// of quantum-stars.py:299 / quantum-gas-bh.py:542).  Adds the pencil's
-// deposit entries.  Returns the thread's float64 partial sum of rho.
+// of quantum-stars.py:299 / quantum-gas-bh.py:542).  The star density of a
+// cell is summed from zero in star order in the (still zero) imaginary slot,
+// then added: the order of the reference's sequential bin_stars.  Returns
+// the thread's float64 partial sum of rho.
 template <int N, int E>
 __device__ __forceinline__ double build_density(float2 (&v)[E], const FusedArgs &a,
                                                 const PencilPos &pp, int t, int P) {
 #pragma unroll
   for (int e = 0; e < E; ++e) v[e] = float2{v[e].x * v[e].x + v[e].y * v[e].y, 0.0f};
-  if (a.pstart) {
-    const int lo = a.pstart[pp.pid], hi = a.pstart[pp.pid + 1];
-    const unsigned kbase = (unsigned)pp.pid * (unsigned)N;
-    for (int k = lo; k < hi; ++k) {
-      const int i = (int)(a.ukey[k] - kbase);
-      if (i % P == t) reg_add<E>(v, i / P, a.uval[k]);
-    }
+  if (a.has_stars) {
+    for_star_corners<N, true>(a, star_ranges(a, pp), t, P,
+                              [&](unsigned, int, int m, float wx, float wy, float wz, float fac) {
+                                const float val = fmul_rn(fmul_rn(fmul_rn(wx, wy), wz), fac);
+                                const int e = m / P;
+#pragma unroll
+                                for (int qq = 0; qq < E; ++qq)
+                                  if (qq == e) v[qq].y = fadd_rn(v[qq].y, val);
+                              });
+#pragma unroll
+    for (int e = 0; e < E; ++e) v[e] = float2{v[e].x + v[e].y, 0.0f};
   }
   if (a.grho) {
 #pragma unroll
     for (int e = 0; e < E; ++e)
-      v[e].x = v[e].x + a.grho[pp.base + (long long)(t + P * e) * a.stride];
+      v[e].x = v[e].x + a.grho[(unsigned)pp.base + (unsigned)(t + P * e) * (unsigned)a.stride];
   }
   double s = 0.0;
 #pragma unroll
@@ -183,17 +284,35 @@ __device__ __forceinline__ double build_density(float2 (&v)[E], const FusedArgs 
   return s;
 }
 
+// sin and cos of theta (float64) for the kick phase.  theta is reduced in
+// float64 to r in [-pi/4, pi/4] with quadrant n = rint(2 theta / pi) and a
+// two-part pi/2 (Cody-Waite); sin r and cos r are their Taylor series to
+// degree 9 and 10 (truncation below 2e-10 for |r| <= pi/4), evaluated in
+// float32 by Horner's rule.
+__device__ __forceinline__ void sincos_reduced(double theta, float &sn, float &cs) {
+  const double n = rint(theta * 0.63661977236758134308);
+  const double r = (theta - n * 1.5707963267948965580e+00) - n * 6.1232339957367660359e-17;
+  const float x = (float)r, x2 = x * x;
+  const float s = x * (1.0f + x2 * (-1.6666667163e-01f +
+                            x2 * (8.3333337680e-03f + x2 * (-1.9841270114e-04f +
+                                                         x2 * 2.7557318845e-06f))));
+  const float c = 1.0f + x2 * (-0.5f + x2 * (4.1666667908e-02f +
+                                    x2 * (-1.3888889225e-03f + x2 * (2.4801587642e-05f +
+                                                                   x2 * -2.7557318845e-07f))));
+  const int q = (int)((long long)n & 3);
+  sn = q == 0 ? s : (q == 1 ? c : (q == 2 ? -s : -c));
+  cs = q == 0 ? c : (q == 1 ? -s : (q == 2 ? -c : s));
+}
+
+// exp(-i theta) * z
 __device__ __forceinline__ float2 phase_rotate(float2 z, double theta) {
-  // exp(-i theta) * z with theta reduced modulo 2 pi in float64 first.
-  const double twopi = 6.283185307179586476925286766559;
-  const double tr = theta - twopi * rint(theta * (1.0 / twopi));
   float s, c;
-  sincosf((float)tr, &s, &c);
+  sincos_reduced(theta, s, c);
   return float2{z.x * c + z.y * s, z.y * c - z.x * s};
 }
 
 template <int N, bool CONTIG, int MODE>
-__global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS)
+__global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CONTIG>::MINB)
     k_fused(FusedArgs a) {
   using SH = PassShape<N, CONTIG>;
   constexpr int E = SH::E, P = SH::P, TP = SH::TP, THREADS = SH::THREADS;
@@ -283,69 +402,84 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS)
     fft_pencil<N, +1>(v, t, smv, tw);
     store_pencil<E>(v, a.S2, base, st, t, P);
   } else if constexpr (MODE == M_KICK) {
-    float2 v1[E], v2[E], ps[E];
-    load_pencil<E>(v1, a.S1, base, st, t, P);
-    load_pencil<E>(v2, a.S2, base, st, t, P);
-    load_pencil<E>(ps, a.psi, base, st, t, P);
-    fft_pencil<N, +1>(v1, t, smv, tw);  // V + i a_r
-    fft_pencil<N, +1>(v2, t, smv, tw);  // a_q + i a_y
-    const int aq = a.axis, ar = 2 - a.axis;
-    // a_max over the three components
+    const int aq = a.axis;  // the kick axis; ar = 2 - aq is the Poisson axis
+    const unsigned gb = (unsigned)base + (unsigned)t * (unsigned)st, gs = (unsigned)P * (unsigned)st;
     float am = 0.0f;
+    float V[E];
+    {
+      // phase 1: S1 -> V + i a_r
+      float2 v1[E];
+      load_pencil<E>(v1, a.S1, base, st, t, P);
+      fft_pencil<N, +1>(v1, t, smv, tw);
 #pragma unroll
-    for (int e = 0; e < E; ++e)
-      am = fmaxf(am, fmaxf(fabsf(v1[e].y), fmaxf(fabsf(v2[e].x), fabsf(v2[e].y))));
-    // self-interaction needs rho = |psi|^2 + rho_stars at the kick
-    float rs[E];
-    if (a.b_coeff != 0.0f) {
+      for (int e = 0; e < E; ++e) {
+        V[e] = v1[e].x;
+        am = fmaxf(am, fabsf(v1[e].y));
+      }
+      if (a.has_stars)
+        for_star_corners<N, false>(a, star_ranges(a, pp), t, P,
+                                   [&](unsigned s, int cbits, int m, float, float, float, float) {
+                                     const float ar_ = reg_get<E>(v1, m / P).y;
+                                     a.A[3 * (8 * s + c_corner_of_bits_dev(cbits)) + (aq == 0 ? 2 : 0)] = ar_;
+                                   });
+      if (a.gv[0]) {  // gas half kick, quantum-gas-bh.py:255-266
+        float *g = a.gv[aq == 0 ? 2 : 0];
 #pragma unroll
-      for (int e = 0; e < E; ++e) rs[e] = ps[e].x * ps[e].x + ps[e].y * ps[e].y;
+        for (int e = 0; e < E; ++e) g[gb + e * gs] = g[gb + e * gs] + v1[e].y * a.gas_dt;
+      }
     }
-    // accelerations at the deposit cells of these pencils
-    if (a.pstart) {
-      const int lo = a.pstart[pp.pid], hi = a.pstart[pp.pid + 1];
-      const unsigned kbase = (unsigned)pp.pid * (unsigned)N;
-      for (int k = lo; k < hi; ++k) {
-        const int i = (int)(a.ukey[k] - kbase);
-        if (i % P == t) {
-          const int e = i / P;
-          const float2 s1 = reg_get<E>(v1, e), s2 = reg_get<E>(v2, e);
-          float acc[3];
-          acc[ar] = s1.y;
-          acc[aq] = s2.x;
-          acc[1] = s2.y;
-          a.A[3 * k + 0] = acc[0];
-          a.A[3 * k + 1] = acc[1];
-          a.A[3 * k + 2] = acc[2];
-          if (a.b_coeff != 0.0f) {
+    {
+      // phase 2: S2 -> a_q + i a_y
+      float2 v2[E];
+      load_pencil<E>(v2, a.S2, base, st, t, P);
+      fft_pencil<N, +1>(v2, t, smv, tw);
 #pragma unroll
-            for (int q = 0; q < E; ++q)
-              if (q == e) rs[q] = rs[q] + a.uval[k];
-          }
+      for (int e = 0; e < E; ++e) am = fmaxf(am, fmaxf(fabsf(v2[e].x), fabsf(v2[e].y)));
+      if (a.has_stars)
+        for_star_corners<N, false>(a, star_ranges(a, pp), t, P,
+                                   [&](unsigned s, int cbits, int m, float, float, float, float) {
+                                     const float2 w = reg_get<E>(v2, m / P);
+                                     float *dst = a.A + 3 * (8 * s + c_corner_of_bits_dev(cbits));
+                                     dst[aq] = w.x;
+                                     dst[1] = w.y;
+                                   });
+      if (a.gv[0]) {
+        float *gq = a.gv[aq], *gy = a.gv[1];
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+          gq[gb + e * gs] = gq[gb + e * gs] + v2[e].x * a.gas_dt;
+          gy[gb + e * gs] = gy[gb + e * gs] + v2[e].y * a.gas_dt;
         }
       }
     }
-    // gas half kick with the grid accelerations (quantum-gas-bh.py:255-266)
-    if (a.gv[0]) {
+    // phase 3: psi <- exp(-i c V) psi with V = Poisson + b rho + V_ext, then
+    // the drift along this axis
+    float2 ps[E];
+    load_pencil<E>(ps, a.psi, base, st, t, P);
+    if (a.b_coeff != 0.0f) {
+      // rho = |psi|^2 + rho_stars, the argument of get_potential (quantum-stars.py:193)
+      float rs[E];
 #pragma unroll
-      for (int e = 0; e < E; ++e) {
-        const long long idx = base + (long long)(t + P * e) * st;
-        float acc[3];
-        acc[ar] = v1[e].y;
-        acc[aq] = v2[e].x;
-        acc[1] = v2[e].y;
+      for (int e = 0; e < E; ++e) rs[e] = 0.0f;
+      if (a.has_stars)
+        for_star_corners<N, true>(a, star_ranges(a, pp), t, P,
+                                  [&](unsigned, int, int m, float wx, float wy, float wz, float fac) {
+                                    const float val = fmul_rn(fmul_rn(fmul_rn(wx, wy), wz), fac);
+                                    const int e = m / P;
 #pragma unroll
-        for (int d = 0; d < 3; ++d) a.gv[d][idx] = a.gv[d][idx] + acc[d] * a.gas_dt;
-      }
+                                    for (int qq = 0; qq < E; ++qq)
+                                      if (qq == e) rs[qq] = fadd_rn(rs[qq], val);
+                                  });
+#pragma unroll
+      for (int e = 0; e < E; ++e)
+        V[e] = V[e] + a.b_coeff * (ps[e].x * ps[e].x + ps[e].y * ps[e].y + rs[e]);
     }
-    // kick: psi <- exp(-i c V) psi, V = Poisson + b rho + V_ext
+    if (a.v_ext) {
 #pragma unroll
-    for (int e = 0; e < E; ++e) {
-      float V = v1[e].x;
-      if (a.b_coeff != 0.0f) V = V + a.b_coeff * rs[e];
-      if (a.v_ext) V = V + a.v_ext[base + (long long)(t + P * e) * st];
-      ps[e] = phase_rotate(ps[e], a.kick_coef * (double)V);
+      for (int e = 0; e < E; ++e) V[e] = V[e] + a.v_ext[gb + e * gs];
     }
+#pragma unroll
+    for (int e = 0; e < E; ++e) ps[e] = phase_rotate(ps[e], a.kick_coef * (double)V[e]);
     if (a.do_drift) {
       fft_pencil<N, -1>(ps, t, smv, tw);
 #pragma unroll
@@ -353,10 +487,29 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS)
       fft_pencil<N, +1>(ps, t, smv, tw);
     }
     store_pencil<E>(ps, a.psi, base, st, t, P);
-    // block max -> one atomic per warp
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) am = fmaxf(am, __shfl_xor_sync(0xffffffffu, am, o));
     if ((tid & 31) == 0) atomic_max_nonneg(a.amax_bits, am);
+  } else if constexpr (MODE == M_DEPOSIT) {
+    // bin_stars (quantum-stars.py:212-247): every cell sums its star
+    // contributions from zero in star order
+    float acc[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) acc[e] = 0.0f;
+    if (a.has_stars)
+      for_star_corners<N, true>(a, star_ranges(a, pp), t, P,
+                                [&](unsigned, int, int m, float wx, float wy, float wz, float fac) {
+                                  const float val = fmul_rn(fmul_rn(fmul_rn(wx, wy), wz), fac);
+                                  const int e = m / P;
+#pragma unroll
+                                  for (int qq = 0; qq < E; ++qq)
+                                    if (qq == e) acc[qq] = fadd_rn(acc[qq], val);
+                                });
+    const unsigned gb = (unsigned)base + (unsigned)t * (unsigned)st, gs = (unsigned)P * (unsigned)st;
+#pragma unroll
+    for (int e = 0; e < E; ++e) a.rho_out[gb + e * gs] = acc[e];
+    (void)smv;
+    (void)tw;
   } else if constexpr (MODE == M_DRIFT || MODE == M_DRIFT_DENSITY) {
     float2 v[E];
     load_pencil<E>(v, a.psi, base, st, t, P);

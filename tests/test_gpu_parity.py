@@ -222,3 +222,19 @@ def test_bad_arguments_raise():
     pos = torch.zeros((5, 3), dtype=torch.float32, device="cuda")
     with pytest.raises(qj.QjError):
         plan.bin_stars(pos, m_s=1.0)
+
+
+def test_fused_large_kick_phase():
+    """Kick phases of O(20) rad exercise the float64 quadrant reduction of
+    the kick's sin / cos (every quadrant is visited)."""
+    qj = qj_mod()
+    psi, pos, vel, g, p = O.stars_ic(32, 0, seed=8)
+    dt = O.default_dt(g, p)
+    V0 = O.get_potential(np.abs(psi) ** 2, g, p)
+    theta = p.m_per_hbar * dt / 2.0 * np.abs(V0).max()
+    p.G *= 20.0 / theta
+    got = run_qj(g, p, psi, pos, vel, dt, 2, qj.FUSED_F32)
+    ref = oracle_run(g, p, psi, pos, vel, dt, 2)
+    assert O.rel_l2(got[0], ref[0]) < 1e-4
+    got = run_qj(g, p, psi, pos, vel, dt, 2, qj.PLAIN_F64)
+    assert O.rel_l2(got[0], ref[0]) < 1e-10
