@@ -112,6 +112,31 @@ int qj_kdk_step(qj_plan *plan, void *psi, void *pos, void *vel, int n_s,
                 double m_s, double dt, int nsteps, int self_interaction,
                 const void *v_ext, qj_diag *diag, void *stream);
 
+/* nsteps x compute_step(psi, rho, vx, vy, vz, m_bh, pos, vel, t) of
+ * quantum-gas-bh.py:537-578: Schroedinger-Poisson + isothermal gas (MUSCL-
+ * Hancock, Rusanov; solve_hydro :269-337, apply_grav_accel :255-266) + black
+ * holes (CIC with per-particle masses m_bh [n_bh], do_accretion :497-530 of
+ * black hole 0).  rho == NULL drops the gas (quantum-bh.py:346-381).
+ * sigma_v: velocity floor of the accretion rate (cs in quantum-gas-bh.py:510,
+ * sigma in quantum-bh.py:319).  dm_accretion != 0 enables do_accretion.
+ * bondi_r_acc_mult > 0 adds the isothermal Bondi gas sink of
+ * quantum-fluid-accretion-test.py:454-494 after the hydro and black-hole
+ * drift (:534-536), with r_acc = bondi_r_acc_mult * dx.  Cubic grid and box
+ * only (as the reference).  Fields are updated in place; t_io (HOST, may be
+ * NULL) is advanced by nsteps * dt. */
+int qj_kdk_gas_bh_step(qj_plan *plan, void *psi, void *rho, void *vx, void *vy,
+                       void *vz, void *m_bh, void *pos, void *vel, int n_bh,
+                       double dt, int nsteps, double sigma_v, int dm_accretion,
+                       double bondi_r_acc_mult, double *t_io, void *stream);
+
+/* nsteps x compute_step(psi, a) of the comoving script, quantum-cosmo.py:169-196:
+ * per step dt = compute_dt(a, da) (:149-162, evaluated in float64 on the
+ * host), kin_fac and pot_fac (:173-174) scale the drift and kick phases;
+ * a += da.  No particles.  a_io: HOST pointer to the scale factor, advanced
+ * by nsteps * da on success. */
+int qj_kdk_cosmo(qj_plan *plan, void *psi, double *a_io, double da, double H0,
+                 double omega_m, double omega_l, int nsteps, void *stream);
+
 /* 3-D FFT of a complex [nx][ny][nz] array with the plan's pencil kernels
  * (direction -1 forward, unnormalised; +1 inverse, scaled by 1/(nx ny nz)),
  * i.e. jnp.fft.fftn / ifftn as called at quantum-stars.py:191-192,307-309.

@@ -564,29 +564,33 @@ def gasbh_compute_step(psi, rho, vx, vy, vz, m_bh, pos, vel, t, g: Grid, p: Phys
     if k is None:
         k = kgrid(g)
     L = np.array([g.Lx, g.Ly, g.Lz])
+    gas = rho is not None  # rho None: quantum-bh.py:346-381 (no gas)
     # (1/2) kick
     rho_bh = bin_stars(pos, g, m_bh)
-    rho_tot = np.abs(psi) ** 2 + rho_bh + rho
+    rho_tot = np.abs(psi) ** 2 + rho_bh + (rho if gas else 0.0)
     V = get_potential(rho_tot, g, p, k)
     psi = kick(psi, V, p, dt)
-    vx, vy, vz = apply_grav_accel(rho_tot, vx, vy, vz, dt / 2.0, g, p, k)
+    if gas:
+        vx, vy, vz = apply_grav_accel(rho_tot, vx, vy, vz, dt / 2.0, g, p, k)
     acc, _ = get_acceleration(pos, rho_tot, g, p, k)
     vel = vel + acc * dt / 2.0
     # drift
     psi = drift(psi, g, p, dt, k)
-    rho, vx, vy, vz = solve_hydro(rho, vx, vy, vz, dt, g.dx, p.cs)
+    if gas:
+        rho, vx, vy, vz = solve_hydro(rho, vx, vy, vz, dt, g.dx, p.cs)
     pos = pos + vel * dt
     pos = ref_mod(pos, L)
-    if bondi_r_acc_mult is not None:
+    if bondi_r_acc_mult is not None and gas:
         rho, M_new, *_ = bondi_sink(rho, m_bh[0], pos[0], g.dx, g.Lx, p.cs, p.G, dt,
                                     r_acc_mult=bondi_r_acc_mult)
         m_bh = np.array([M_new] + list(m_bh[1:]))
     # (1/2) kick
     rho_bh = bin_stars(pos, g, m_bh)
-    rho_tot = np.abs(psi) ** 2 + rho_bh + rho
+    rho_tot = np.abs(psi) ** 2 + rho_bh + (rho if gas else 0.0)
     V = get_potential(rho_tot, g, p, k)
     psi = kick(psi, V, p, dt)
-    vx, vy, vz = apply_grav_accel(rho_tot, vx, vy, vz, dt / 2.0, g, p, k)
+    if gas:
+        vx, vy, vz = apply_grav_accel(rho_tot, vx, vy, vz, dt / 2.0, g, p, k)
     acc, _ = get_acceleration(pos, rho_tot, g, p, k)
     vel = vel + acc * dt / 2.0
     # accretion

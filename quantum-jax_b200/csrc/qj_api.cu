@@ -133,8 +133,13 @@ struct qj_plan {
   int *pstart = nullptr;
   int *n_unique = nullptr;
   StarBufs sb{};  // fused path star data
+  // side stream for the star pipeline (overlaps the y drift pass)
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_kick = nullptr, ev_parts = nullptr;
   void *amax = nullptr, *dts = nullptr;  // real type scalars
   void *tmp_scalar = nullptr;
+  void *tmp_diag = nullptr;
+  void *gas_out[4] = {nullptr, nullptr, nullptr, nullptr};  // hydro output scratch
 };
 
 namespace {
@@ -286,13 +291,21 @@ int deposit_list(qj_plan *P, const void *pos, int n, double m_s, const void *mas
 // separate dt/2 half kicks and records dt_s between them, as the reference's
 // step boundary does.
 // ---------------------------------------------------------------------------
+// Per-step coefficients of a variable-step run (quantum-cosmo.py:173-181):
+// kick_half[n] = m_per_hbar dt_n pot_fac_n / 2, drift[n] = dt_n kin_fac_n.
+// Null = the constant-dt step of quantum-stars.py (pot_fac = kin_fac = 1).
+struct StepCoefs {
+  std::vector<double> kick_half, drift;
+};
+
 int fused_kdk(qj_plan *P, float2 *psi, float *pos, float *vel, int n_s, double m_s, double dt,
-              int nsteps, int si, const float *vext, double *diag, cudaStream_t st) {
+              int nsteps, int si, const float *vext, double *diag, cudaStream_t st,
+              const StepCoefs *sc = nullptr) {
   const bool parts = n_s > 0;
-  QJ_TRY(ensure_prop(P, dt, st));
+  auto half = [&](int n) { return sc ? sc->kick_half[n] : P->ph.m_per_hbar * dt / 2.0; };
+  auto drift_dt = [&](int n) { return sc ? sc->drift[n] : dt; };
   QJ_TRY(launch_diag_load(false, diag, P->amax, st));
   if (parts) QJ_TRY(launch_set_scalar(false, P->dts, INFINITY, st));
-  const double half_coef = P->ph.m_per_hbar * dt / 2.0;
   int q = 2;
   if (parts) {
     if (prof_on()) prof_mark_begin(st);
@@ -309,6 +322,7 @@ int fused_kdk(qj_plan *P, float2 *psi, float *pos, float *vel, int n_s, double m
   for (int k = 0; k <= nsteps; ++k) {
     const int r = 2 - q;
     const bool last = (k == nsteps);
+    if (!last) QJ_TRY(ensure_prop(P, drift_dt(k), st));
     {
       FusedArgs a = fused_args(P, 1);
       QJ_TRY(launch_fused(M_FFT_FWD, P->n[1], a, st));
@@ -326,7 +340,8 @@ int fused_kdk(qj_plan *P, float2 *psi, float *pos, float *vel, int n_s, double m
     {
       FusedArgs a = fused_args(P, q);
       a.psi = psi;
-      a.kick_coef = half_coef * ((k == 0 || last) ? 1.0 : 2.0);
+      // kick k = second half kick of step k-1 and first half kick of step k
+      a.kick_coef = (k > 0 ? half(k - 1) : 0.0) + (last ? 0.0 : half(k));
       a.b_coeff = si ? (float)P->ph.b_coeff : 0.0f;
       a.v_ext = vext;
       a.do_drift = last ? 0 : 1;
@@ -334,7 +349,12 @@ int fused_kdk(qj_plan *P, float2 *psi, float *pos, float *vel, int n_s, double m
       QJ_TRY(launch_fused(M_KICK, P->n[q], a, st));
     }
     if (parts) {
-      if (prof_on()) prof_mark_begin(st);
+      // fork: the star update and bucket sort run on the side stream while
+      // the y drift pass runs on st; joined before the next density build
+      QJ_CK(cudaEventRecord(P->ev_kick, st));
+      QJ_CK(cudaStreamWaitEvent(P->side, P->ev_kick, 0));
+      cudaStream_t pst = P->side;
+      if (prof_on()) prof_mark_begin(pst);
       UpdateArgs u;
       std::memset(&u, 0, sizeof(u));
       u.n = n_s;
@@ -345,9 +365,10 @@ int fused_kdk(qj_plan *P, float2 *psi, float *pos, float *vel, int n_s, double m
       u.dts_bits = P->dts;
       u.q_next = last ? -1 : r;
       u.m_s = m_s;
-      QJ_TRY(launch_update_fused(pos, vel, geom(P), u, P->sb, st));
-      if (!last) QJ_TRY(launch_bucket_sort(n_s, n_pencils(P, r), P->sb, st));
-      if (prof_on()) prof_mark_end(8, st);
+      QJ_TRY(launch_update_fused(pos, vel, geom(P), u, P->sb, pst));
+      if (!last) QJ_TRY(launch_bucket_sort(n_s, n_pencils(P, r), P->sb, pst));
+      if (prof_on()) prof_mark_end(8, pst);
+      QJ_CK(cudaEventRecord(P->ev_parts, pst));
     }
     if (!last) {
       {
@@ -358,12 +379,16 @@ int fused_kdk(qj_plan *P, float2 *psi, float *pos, float *vel, int n_s, double m
       {
         FusedArgs a = fused_args(P, r);
         a.psi = psi;
-        if (parts) set_stars(a, P);
+        if (parts) {
+          QJ_CK(cudaStreamWaitEvent(st, P->ev_parts, 0));
+          set_stars(a, P);
+        }
         QJ_TRY(launch_fused(M_DRIFT_DENSITY, P->n[r], a, st));
       }
     }
     q = r;
   }
+  if (parts) QJ_CK(cudaStreamWaitEvent(st, P->ev_parts, 0));
   return launch_diag_store(false, diag, P->amax, P->dts, parts ? 1 : 0, nsteps * dt, st);
 }
 
@@ -373,8 +398,8 @@ int fused_kdk(qj_plan *P, float2 *psi, float *pos, float *vel, int n_s, double m
 
 // get_potential(rho) -> V (rho given as rho_in, or |psi|^2 + rho_s).
 int plain_potential(qj_plan *P, const void *psi, const void *rho_s, const void *rho_in, void *V,
-                    int si, const void *vext, cudaStream_t st) {
-  QJ_TRY(launch_build_rho(P->dbl, psi, rho_s, nullptr, rho_in, 4.0 * M_PI * P->ph.G, P->ph.rho_bar,
+                    int si, const void *vext, cudaStream_t st, const void *rho_gas = nullptr) {
+  QJ_TRY(launch_build_rho(P->dbl, psi, rho_s, rho_gas, rho_in, 4.0 * M_PI * P->ph.G, P->ph.rho_bar,
                           P->rho_tot, P->c0, P->ncell, st));
   QJ_TRY(fft3d(P, P->c0, -1, st));
   QJ_TRY(launch_poisson_div(P->dbl, P->c0, ktabs(P), P->ncell, st));
@@ -407,11 +432,13 @@ int plain_bin(qj_plan *P, const void *pos, int n, double m_s, const void *masses
 }
 
 int plain_kdk(qj_plan *P, void *psi, void *pos, void *vel, int n_s, double m_s, double dt,
-              int nsteps, int si, const void *vext, double *diag, cudaStream_t st) {
+              int nsteps, int si, const void *vext, double *diag, cudaStream_t st,
+              const StepCoefs *sc = nullptr) {
   QJ_TRY(ensure_plain_ws(P));
   QJ_TRY(launch_diag_load(P->dbl, diag, P->amax, st));
-  const double coef = P->ph.m_per_hbar * dt / 2.0;
   for (int step = 0; step < nsteps; ++step) {
+    const double coef = sc ? sc->kick_half[step] : P->ph.m_per_hbar * dt / 2.0;
+    const double dtk = sc ? sc->drift[step] : dt;
     for (int half = 0; half < 2; ++half) {
       // (1/2) kick
       QJ_TRY(plain_bin(P, pos, n_s, m_s, nullptr, P->rho_s, st));
@@ -434,12 +461,181 @@ int plain_kdk(qj_plan *P, void *psi, void *pos, void *vel, int n_s, double m_s, 
       if (half == 0) {
         // drift (:307-309); the particle drift ran in the update above
         QJ_TRY(fft3d(P, psi, -1, st));
-        QJ_TRY(launch_drift_mul(P->dbl, psi, ktabs(P), dt, P->ph.m_per_hbar, P->ncell, st));
+        QJ_TRY(launch_drift_mul(P->dbl, psi, ktabs(P), dtk, P->ph.m_per_hbar, P->ncell, st));
         QJ_TRY(fft3d(P, psi, +1, st));
       }
     }
   }
   return launch_diag_store(P->dbl, diag, P->amax, P->dts, n_s > 0 ? 1 : 0, nsteps * dt, st);
+}
+
+
+// ---------------------------------------------------------------------------
+// Gas + black hole step, quantum-gas-bh.py:537-578 (quantum-bh.py:346-381
+// without gas).  The dark-matter accretion between the second half kick and
+// the next step's first half kick changes the density, so the two half kicks
+// of a step keep separate Poisson solves here.
+// ---------------------------------------------------------------------------
+struct GasArgs {
+  void *psi, *rho, *v[3], *m_bh, *pos, *vel;
+  int n_bh;
+  double dt;
+  double sigma_v;
+  int dm_accretion;
+  double bondi;  // r_acc_mult, <= 0 disables the gas sink
+};
+
+int ensure_gas_ws(qj_plan *P) {
+  for (int i = 0; i < 4; ++i)
+    if (!P->gas_out[i]) QJ_TRY(dev_alloc(P, &P->gas_out[i], P->ncell * P->rsz));
+  return 0;
+}
+
+int gas_hydro(qj_plan *P, const GasArgs &g, cudaStream_t st) {
+  const double dx = P->g.Lx / P->n[0];
+  QJ_TRY(launch_hydro(P->dbl, g.rho, g.v[0], g.v[1], g.v[2], P->gas_out[0], P->gas_out[1],
+                      P->gas_out[2], P->gas_out[3], P->n[0], dx, g.dt, P->ph.cs,
+                      (g.bondi > 0 && g.n_bh > 0) ? 1 : 0, st));
+  void *dst[4] = {g.rho, g.v[0], g.v[1], g.v[2]};
+  for (int i = 0; i < 4; ++i)
+    QJ_CK(cudaMemcpyAsync(dst[i], P->gas_out[i], P->ncell * P->rsz, cudaMemcpyDeviceToDevice, st));
+  return 0;
+}
+
+int fused_gas_step(qj_plan *P, const GasArgs &g, cudaStream_t st) {
+  const bool bh = g.n_bh > 0, gas = g.rho != nullptr;
+  const double dx = P->g.Lx / P->n[0];
+  const double half = P->ph.m_per_hbar * g.dt / 2.0;
+  QJ_TRY(ensure_prop(P, g.dt, st));
+  auto stars = [&](FusedArgs &a) {
+    if (bh) set_stars(a, P);
+    if (gas) {
+      a.grho = (const float *)g.rho;
+    }
+  };
+  auto poisson = [&](int q, int r) -> int {
+    FusedArgs a = fused_args(P, 1);
+    QJ_TRY(launch_fused(M_FFT_FWD, P->n[1], a, st));
+    a = fused_args(P, r);
+    a.part_in = P->part;
+    a.n_part = pass_blocks(P->n[q], q, P->n[0], P->n[1], P->n[2]);
+    QJ_TRY(launch_fused(M_POISSON, P->n[r], a, st));
+    a = fused_args(P, 1);
+    return launch_fused(M_IFFT2, P->n[1], a, st);
+  };
+  auto kick = [&](int q, int drift) -> int {
+    FusedArgs a = fused_args(P, q);
+    a.psi = (float2 *)g.psi;
+    a.kick_coef = half;
+    a.do_drift = drift;
+    if (bh) set_stars(a, P);
+    if (gas) {
+      for (int d = 0; d < 3; ++d) a.gv[d] = (float *)g.v[d];
+      a.gas_dt = (float)(g.dt / 2.0);
+    }
+    return launch_fused(M_KICK, P->n[q], a, st);
+  };
+  UpdateArgs u;
+  std::memset(&u, 0, sizeof(u));
+  u.n = g.n_bh;
+  u.dt = g.dt;
+  u.dts_bits = P->dts;
+  u.masses = g.m_bh;
+  // (1/2) kick
+  if (bh) {
+    QJ_TRY(launch_stars_prepare(g.pos, g.n_bh, g.m_bh, 0.0, geom(P), 2, P->sb, st));
+    QJ_TRY(launch_bucket_sort(g.n_bh, n_pencils(P, 2), P->sb, st));
+  }
+  {
+    FusedArgs a = fused_args(P, 2);
+    a.psi = (float2 *)g.psi;
+    stars(a);
+    QJ_TRY(launch_fused(M_DENSITY, P->n[2], a, st));
+  }
+  QJ_TRY(poisson(2, 0));
+  QJ_TRY(kick(2, 1));  // + drift along z
+  if (bh) {
+    u.k1 = 1;
+    u.drift = 1;
+    u.q_next = 0;
+    QJ_TRY(launch_update_fused(g.pos, g.vel, geom(P), u, P->sb, st));
+  }
+  {
+    FusedArgs a = fused_args(P, 1);
+    a.psi = (float2 *)g.psi;
+    QJ_TRY(launch_fused(M_DRIFT, P->n[1], a, st));
+  }
+  if (gas) QJ_TRY(gas_hydro(P, g, st));
+  if (bh && gas && g.bondi > 0)
+    QJ_TRY(launch_bondi(false, g.rho, g.pos, g.m_bh, P->n[0], dx, P->g.Lx, P->ph.cs, P->ph.G, g.dt,
+                        g.bondi, st));
+  if (bh) {
+    // deposit of the drifted black holes (their mass may have changed)
+    QJ_TRY(launch_stars_prepare(g.pos, g.n_bh, g.m_bh, 0.0, geom(P), 0, P->sb, st));
+    QJ_TRY(launch_bucket_sort(g.n_bh, n_pencils(P, 0), P->sb, st));
+  }
+  {
+    FusedArgs a = fused_args(P, 0);
+    a.psi = (float2 *)g.psi;
+    stars(a);
+    QJ_TRY(launch_fused(M_DRIFT_DENSITY, P->n[0], a, st));
+  }
+  // (1/2) kick
+  QJ_TRY(poisson(0, 2));
+  QJ_TRY(kick(0, 0));
+  if (bh) {
+    u.k1 = 0;
+    u.k2 = 1;
+    u.drift = 0;
+    u.q_next = -1;
+    QJ_TRY(launch_update_fused(g.pos, g.vel, geom(P), u, P->sb, st));
+    if (g.dm_accretion)
+      QJ_TRY(launch_accrete(false, g.psi, g.pos, g.vel, g.m_bh, P->n[0], dx, g.sigma_v, P->ph.G,
+                            P->ph.m_per_hbar, P->ph.c_light, g.dt, st));
+  }
+  return 0;
+}
+
+int plain_gas_step(qj_plan *P, const GasArgs &g, cudaStream_t st) {
+  const bool bh = g.n_bh > 0, gas = g.rho != nullptr;
+  const double dx = P->g.Lx / P->n[0];
+  const double coef = P->ph.m_per_hbar * g.dt / 2.0;
+  for (int half = 0; half < 2; ++half) {
+    QJ_TRY(plain_bin(P, g.pos, g.n_bh, 0.0, g.m_bh, P->rho_s, st));
+    QJ_TRY(plain_potential(P, g.psi, P->rho_s, nullptr, P->V, 0, nullptr, st, gas ? g.rho : nullptr));
+    QJ_TRY(launch_kick_plain(P->dbl, g.psi, P->V, coef, P->ncell, st));
+    if (gas) {  // apply_grav_accel (:255-266) from rho_tot
+      QJ_TRY(plain_accel(P, nullptr, P->tmp_scalar, st));
+      QJ_TRY(launch_gas_kick(P->dbl, g.v[0], g.v[1], g.v[2], P->ax, P->ay, P->az, g.dt / 2.0,
+                             P->ncell, st));
+    }
+    if (bh) {  // get_acceleration (:452-490)
+      QJ_TRY(plain_accel(P, nullptr, P->tmp_scalar, st));
+      QJ_TRY(launch_gather_dense(P->dbl, g.pos, g.n_bh, geom(P), P->ax, P->ay, P->az, P->acc, st));
+      UpdateArgs u;
+      std::memset(&u, 0, sizeof(u));
+      u.n = g.n_bh;
+      u.dt = g.dt;
+      u.k1 = half == 0;
+      u.k2 = half == 1;
+      u.drift = half == 0;
+      u.dts_bits = P->dts;
+      QJ_TRY(launch_particles_update(P->dbl, g.pos, g.vel, P->acc, geom(P), u, st));
+    }
+    if (half == 0) {
+      QJ_TRY(fft3d(P, g.psi, -1, st));
+      QJ_TRY(launch_drift_mul(P->dbl, g.psi, ktabs(P), g.dt, P->ph.m_per_hbar, P->ncell, st));
+      QJ_TRY(fft3d(P, g.psi, +1, st));
+      if (gas) QJ_TRY(gas_hydro(P, g, st));
+      if (bh && gas && g.bondi > 0)
+        QJ_TRY(launch_bondi(true, g.rho, g.pos, g.m_bh, P->n[0], dx, P->g.Lx, P->ph.cs, P->ph.G,
+                            g.dt, g.bondi, st));
+    }
+  }
+  if (bh && g.dm_accretion)
+    QJ_TRY(launch_accrete(true, g.psi, g.pos, g.vel, g.m_bh, P->n[0], dx, g.sigma_v, P->ph.G,
+                          P->ph.m_per_hbar, P->ph.c_light, g.dt, st));
+  return 0;
 }
 
 }  // namespace
@@ -573,6 +769,12 @@ int qj_plan_create(qj_plan **plan, const qj_grid *grid, const qj_phys *phys, int
     if ((rc = dev_alloc_t(P, &b.sortbuf, 4 * np))) return fail(rc);
     if ((rc = dev_alloc_t(P, &b.bstart, npen + 1))) return fail(rc);
     b.A = (float *)P->A;
+    int lo = 0, hi = 0;
+    cudaError_t e0 = cudaDeviceGetStreamPriorityRange(&lo, &hi);
+    if (e0 == cudaSuccess) e0 = cudaStreamCreateWithPriority(&P->side, cudaStreamNonBlocking, hi);
+    if (e0 == cudaSuccess) e0 = cudaEventCreateWithFlags(&P->ev_kick, cudaEventDisableTiming);
+    if (e0 == cudaSuccess) e0 = cudaEventCreateWithFlags(&P->ev_parts, cudaEventDisableTiming);
+    if (e0 != cudaSuccess) return fail(cuda_fail(e0, "side stream", __FILE__, __LINE__));
   }
   if ((rc = dev_alloc_t(P, &P->pstart, npen + 1))) return fail(rc);
   if ((rc = dev_alloc_t(P, &P->n_unique, 1))) return fail(rc);
@@ -587,6 +789,12 @@ int qj_plan_create(qj_plan **plan, const qj_grid *grid, const qj_phys *phys, int
 
 int qj_plan_destroy(qj_plan *P) {
   if (!P) return QJ_OK;
+  if (P->side) {
+    cudaStreamSynchronize(P->side);
+    cudaStreamDestroy(P->side);
+  }
+  if (P->ev_kick) cudaEventDestroy(P->ev_kick);
+  if (P->ev_parts) cudaEventDestroy(P->ev_parts);
   for (void *p : P->allocs) cudaFree(p);
   delete P;
   return QJ_OK;
@@ -691,6 +899,90 @@ int qj_get_acceleration(qj_plan *P, const void *pos, int n, const void *rho, voi
   QJ_TRY(plain_accel(P, rho, P->tmp_scalar, st));
   if (n > 0) QJ_TRY(launch_gather_dense(P->dbl, pos, n, geom(P), P->ax, P->ay, P->az, acc, st));
   if (a_max) QJ_TRY(launch_bits_to_double(P->dbl, P->tmp_scalar, a_max, st));
+  return QJ_OK;
+}
+
+// quantum-cosmo.py:149-162: dt from a 1000-point midpoint quadrature of
+// 1 / adot, adot = H0 sqrt(omega_m / a + omega_l a^2), in float64.
+static double cosmo_dt(double a, double da, double H0, double om, double ol) {
+  const int n = 1000;
+  const double h = 1.0 / n;
+  auto mean_inv = [&](double A) {
+    double s = 0.0;
+    for (int i = 0; i < n; ++i) {
+      const double at = A * (0.5 * h + i * h);
+      s += 1.0 / (H0 * std::sqrt(om / at + ol * at * at));
+    }
+    return s / n;
+  };
+  const double t = mean_inv(a) * (a - 0.0);
+  return mean_inv(a + da) * ((a + da) - 0.0) - t;
+}
+
+int qj_kdk_cosmo(qj_plan *P, void *psi, double *a_io, double da, double H0, double omega_m,
+                 double omega_l, int nsteps, void *stream) {
+  if (!P || !psi || !a_io || nsteps < 0 || !(da > 0) || !(*a_io > 0)) {
+    set_error("qj_kdk_cosmo: bad argument");
+    return QJ_ERR_ARG;
+  }
+  if (nsteps == 0) return QJ_OK;
+  StepCoefs sc;
+  double a = *a_io;
+  for (int n = 0; n < nsteps; ++n) {
+    // quantum-cosmo.py:173-176
+    const double kin_fac = 0.5 * (std::pow(a, -2.0) + std::pow(a + da, -2.0));
+    const double pot_fac = 0.5 * (1.0 / a + 1.0 / (a + da));
+    const double dt = cosmo_dt(a, da, H0, omega_m, omega_l);
+    sc.kick_half.push_back(P->ph.m_per_hbar * dt * pot_fac / 2.0);
+    sc.drift.push_back(dt * kin_fac);
+    a += da;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  if (!P->tmp_diag) QJ_TRY(dev_alloc(P, &P->tmp_diag, 3 * sizeof(double)));
+  int rc = P->dbl ? plain_kdk(P, psi, nullptr, nullptr, 0, 0.0, 1.0, nsteps, 0, nullptr,
+                              (double *)P->tmp_diag, st, &sc)
+                  : fused_kdk(P, (float2 *)psi, nullptr, nullptr, 0, 0.0, 1.0, nsteps, 0, nullptr,
+                              (double *)P->tmp_diag, st, &sc);
+  if (rc == 0) *a_io = a;
+  return rc;
+}
+
+int qj_kdk_gas_bh_step(qj_plan *P, void *psi, void *rho, void *vx, void *vy, void *vz, void *m_bh,
+                       void *pos, void *vel, int n_bh, double dt, int nsteps, double sigma_v,
+                       int dm_accretion, double bondi_r_acc_mult, double *t_io, void *stream) {
+  if (!P || !psi || nsteps < 0 || n_bh < 0 || (n_bh > 0 && (!m_bh || !pos || !vel)) ||
+      (rho && (!vx || !vy || !vz)) || !(dt > 0)) {
+    set_error("qj_kdk_gas_bh_step: bad argument");
+    return QJ_ERR_ARG;
+  }
+  if (P->n[0] != P->n[1] || P->n[0] != P->n[2] || P->g.Lx != P->g.Ly || P->g.Lx != P->g.Lz) {
+    set_error("qj_kdk_gas_bh_step: the gas / black-hole step needs a cubic grid and box");
+    return QJ_ERR_ARG;
+  }
+  if (n_bh > P->max_particles) {
+    set_error("qj_kdk_gas_bh_step: n_bh=%d exceeds max_particles=%d", n_bh, P->max_particles);
+    return QJ_ERR_ARG;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  QJ_TRY(ensure_gas_ws(P));
+  if (P->dbl) QJ_TRY(ensure_plain_ws(P));
+  GasArgs g;
+  g.psi = psi;
+  g.rho = rho;
+  g.v[0] = vx;
+  g.v[1] = vy;
+  g.v[2] = vz;
+  g.m_bh = m_bh;
+  g.pos = pos;
+  g.vel = vel;
+  g.n_bh = n_bh;
+  g.dt = dt;
+  g.sigma_v = sigma_v;
+  g.dm_accretion = dm_accretion;
+  g.bondi = bondi_r_acc_mult;
+  for (int s = 0; s < nsteps; ++s)
+    QJ_TRY(P->dbl ? plain_gas_step(P, g, st) : fused_gas_step(P, g, st));
+  if (t_io) *t_io += nsteps * dt;
   return QJ_OK;
 }
 

@@ -1,0 +1,327 @@
+// Isothermal gas and black-hole kernels (quantum-gas-bh.py, quantum-bh.py,
+// quantum-fluid-accretion-test.py), templated on the real type.
+//
+// k_hydro is one MUSCL-Hancock update of solve_hydro (quantum-gas-bh.py:269-337)
+// per cell.  The reference computes whole-grid arrays (gradients, limited
+// gradients, predicted primitives, face states, fluxes) with jnp.roll; here a
+// thread evaluates, for its cell and its six face neighbours, the limited
+// gradients and predicted primitives from the raw fields (read through L1),
+// then the fluxes through its six faces and the flux-form update, in the same
+// floating-point order as the reference.  The grid is cubic with spacing dx,
+// as in the reference.
+#include <cmath>
+
+#include "../../include/qj.h"
+#include "qj_internal.h"
+
+namespace qj {
+
+namespace {
+
+template <typename R> struct Prim {
+  R f[4];      // predicted primitives rho', vx', vy', vz'
+  R g[4][3];   // limited gradients of rho, vx, vy, vz along x, y, z
+};
+
+struct Idx3 {
+  int n;
+  __device__ __forceinline__ long long at(int x, int y, int z) const {
+    x = (x % n + n) % n;
+    y = (y % n + n) % n;
+    z = (z % n + n) % n;
+    return ((long long)x * n + y) * n + z;
+  }
+};
+
+// quantum-gas-bh.py:353-357
+template <typename R> __device__ __forceinline__ R adjust_denominator(R d) {
+  const R eps = (R)1.0e-12;
+  return d > (R)0 ? d + eps : (d < (R)0 ? d - eps : eps);
+}
+template <typename R> __device__ __forceinline__ R clamp01(R x) {
+  return fmax((R)0, fmin((R)1, x));
+}
+
+// Limited gradients and half-step primitives of cell (x, y, z):
+// get_gradient (:188-193), slope_limiter (:340-395), predictor (:283-299).
+template <typename R>
+__device__ Prim<R> cell_prim(const R *const F[4], const Idx3 &I, int x, int y, int z, R dx, R dt,
+                             R cs) {
+  Prim<R> P;
+  R c[4];
+  for (int v = 0; v < 4; ++v) c[v] = F[v][I.at(x, y, z)];
+  for (int v = 0; v < 4; ++v) {
+    for (int d = 0; d < 3; ++d) {
+      const int ex = d == 0, ey = d == 1, ez = d == 2;
+      const R fp = F[v][I.at(x + ex, y + ey, z + ez)];
+      const R fm = F[v][I.at(x - ex, y - ey, z - ez)];
+      R g = (fp - fm) / ((R)2 * dx);
+      const R denom = adjust_denominator(g);
+      g = clamp01(((c[v] - fm) / dx) / denom) * g;
+      g = clamp01((-(c[v] - fp) / dx) / denom) * g;
+      P.g[v][d] = g;
+    }
+  }
+  const R rho = c[0], vx = c[1], vy = c[2], vz = c[3];
+  const R h = (R)0.5 * dt;
+  P.f[0] = rho - h * (vx * P.g[0][0] + rho * P.g[1][0] + vy * P.g[0][1] + rho * P.g[2][1] +
+                      vz * P.g[0][2] + rho * P.g[3][2]);
+  for (int v = 1; v < 4; ++v)
+    P.f[v] = c[v] - h * (vx * P.g[v][0] + vy * P.g[v][1] + vz * P.g[v][2] +
+                         ((R)1 / rho) * P.g[0][v - 1] * cs * cs);
+  return P;
+}
+
+// get_flux (:226-252) with the rotated variable order of :316-324.  u = the
+// velocity component normal to the face; w1, w2 the tangential ones.
+template <typename R>
+__device__ __forceinline__ void rusanov(R rL, R uL, R aL, R bL, R rR, R uR, R aR, R bR, R cs,
+                                        R out[4]) {
+  const R rho_star = (R)0.5 * (rL + rR);
+  const R mu = (R)0.5 * (rL * uL + rR * uR);
+  const R ma = (R)0.5 * (rL * aL + rR * aR);
+  const R mb = (R)0.5 * (rL * bL + rR * bR);
+  const R P_star = rho_star * cs * cs;
+  R fM = mu;
+  R fU = mu * mu / rho_star + P_star;
+  R fA = mu * ma / rho_star;
+  R fB = mu * mb / rho_star;
+  const R C = fmax(cs + fabs(uL), cs + fabs(uR));
+  fM = fM - C * (R)0.5 * (rR - rL);
+  fU = fU - C * (R)0.5 * (rR * uR - rL * uL);
+  fA = fA - C * (R)0.5 * (rR * aR - rL * aL);
+  fB = fB - C * (R)0.5 * (rR * bR - rL * bL);
+  out[0] = fM;
+  out[1] = fU;
+  out[2] = fA;
+  out[3] = fB;
+}
+
+// Flux through the face between cell L and its +d neighbour R, returned in
+// conserved order (Mass, Momx, Momy, Momz).  Face states: extrap_to_face
+// (:196-209).
+template <typename R>
+__device__ void face_flux(const Prim<R> &L, const Prim<R> &Rt, int d, R dx, R cs, R out[4]) {
+  R fl[4], fr[4];
+  for (int v = 0; v < 4; ++v) {
+    fl[v] = L.f[v] + (R)0.5 * L.g[v][d] * dx;
+    fr[v] = Rt.f[v] - (R)0.5 * Rt.g[v][d] * dx;
+  }
+  R o[4];
+  if (d == 0) {
+    rusanov(fl[0], fl[1], fl[2], fl[3], fr[0], fr[1], fr[2], fr[3], cs, o);
+    out[0] = o[0]; out[1] = o[1]; out[2] = o[2]; out[3] = o[3];
+  } else if (d == 1) {  // (rho, vy, vz, vx) -> (Mass, Momy, Momz, Momx)
+    rusanov(fl[0], fl[2], fl[3], fl[1], fr[0], fr[2], fr[3], fr[1], cs, o);
+    out[0] = o[0]; out[2] = o[1]; out[3] = o[2]; out[1] = o[3];
+  } else {  // (rho, vz, vx, vy) -> (Mass, Momz, Momx, Momy)
+    rusanov(fl[0], fl[3], fl[1], fl[2], fr[0], fr[3], fr[1], fr[2], cs, o);
+    out[0] = o[0]; out[3] = o[1]; out[1] = o[2]; out[2] = o[3];
+  }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(128)
+    k_hydro(const R *rho, const R *vx, const R *vy, const R *vz, R *orho, R *ovx, R *ovy, R *ovz,
+            int n, R dx, R dt, R cs, R vol, R fac, int clamp_rho) {
+  const long long ncell = (long long)n * n * n;
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= ncell) return;
+  const int z = (int)(i % n), y = (int)((i / n) % n), x = (int)(i / ((long long)n * n));
+  const R *const F[4] = {rho, vx, vy, vz};
+  const Idx3 I{n};
+  const Prim<R> C = cell_prim(F, I, x, y, z, dx, dt, cs);
+  // conserved (:170-176)
+  R U[4];
+  U[0] = rho[i] * vol;
+  U[1] = rho[i] * vx[i] * vol;
+  U[2] = rho[i] * vy[i] * vol;
+  U[3] = rho[i] * vz[i] * vol;
+  // apply_fluxes (:212-223): per axis, F += -fac * flux(+face); F += fac * flux(-face)
+  R up[3][4], dn[3][4];
+  for (int d = 0; d < 3; ++d) {
+    const int ex = d == 0, ey = d == 1, ez = d == 2;
+    const Prim<R> Pp = cell_prim(F, I, x + ex, y + ey, z + ez, dx, dt, cs);
+    const Prim<R> Pm = cell_prim(F, I, x - ex, y - ey, z - ez, dx, dt, cs);
+    face_flux(C, Pp, d, dx, cs, up[d]);
+    face_flux(Pm, C, d, dx, cs, dn[d]);
+  }
+  for (int v = 0; v < 4; ++v) {
+    R u = U[v];
+    for (int d = 0; d < 3; ++d) {
+      u = u + -fac * up[d][v];
+      u = u + fac * dn[d][v];
+    }
+    U[v] = u;
+  }
+  // get_primitive (:179-185)
+  R r = U[0] / vol;
+  if (clamp_rho) r = fmax((R)0, r);
+  orho[i] = r;
+  ovx[i] = U[1] / U[0];
+  ovy[i] = U[2] / U[0];
+  ovz[i] = U[3] / U[0];
+}
+
+// do_accretion (quantum-gas-bh.py:497-530; quantum-bh.py:306-339 with sigma)
+template <typename R>
+__global__ void k_accrete(cplx<R> *psi, const R *pos, const R *vel, R *m_bh, int n, R dx, R vol,
+                          R sigma_v, R G, R m_per_hbar, R c_light, R dt) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  int idx[3];
+  for (int d = 0; d < 3; ++d) {
+    const R i = floor((pos[d] - (R)0.5 * dx) / dx);
+    R m = ref_mod(i, (R)n);
+    idx[d] = (m >= (R)0 && m < (R)n) ? (int)m : 0;
+  }
+  const long long c = ((long long)idx[0] * n + idx[1]) * n + idx[2];
+  const cplx<R> p = psi[c];
+  const R amp = hypot(p.x, p.y);
+  const R theta = atan2(p.y, p.x);
+  const R v = sqrt(sigma_v * sigma_v + vel[0] * vel[0] + vel[1] * vel[1] + vel[2] * vel[2]);
+  const R pi = (R)3.14159265358979323846;
+  const R xi = (R)2 * pi * G * m_bh[0] * m_per_hbar / v;
+  const R GM = G * m_bh[0];
+  const R dM_dt = (R)32 * pi * pi * (GM * GM * GM) * m_per_hbar * amp * amp /
+                  (c_light * c_light * c_light * v * ((R)1 - exp(-xi)));
+  const R new_amp = fabs(amp) - sqrt(dM_dt * dt / vol);
+  psi[c] = cplx<R>{new_amp * cos(theta), new_amp * sin(theta)};
+  m_bh[0] = m_bh[0] + dM_dt * dt;
+}
+
+// bh_bondi_step_no_vrel (quantum-fluid-accretion-test.py:454-494): Gaussian
+// kernel inside r_acc = r_acc_mult dx around the black hole, ambient density,
+// isothermal Bondi rate, capped removal.  Only cells with R^2 <= r_acc^2
+// contribute to the reference's sums, so one CTA covers the neighbourhood
+// (K = ceil(r_acc / dx) + 1 cells each way) with fixed-order reductions.
+template <typename R>
+__global__ void __launch_bounds__(256)
+    k_bondi(R *rho, const R *pos, R *m_bh, int n, R dx, R L, R cs, R G, R dt, R r_acc_mult,
+            R lam, R fmax_frac, int K) {
+  __shared__ double red[3][256];
+  const int w = 2 * K + 1;
+  const int tot = w * w * w;
+  const R M = m_bh[0];
+  const R r_B = G * M / (cs * cs);
+  const R r_acc = r_acc_mult * dx;
+  const R rK = fmin(fmax(r_B, (R)0.25 * dx), (R)0.5 * r_acc);
+  int cidx[3];
+  for (int d = 0; d < 3; ++d) cidx[d] = (int)floor(pos[d] / dx);
+  double sW = 0, sWr = 0, sM = 0;
+  for (int j = threadIdx.x; j < tot; j += blockDim.x) {
+    const int o0 = j / (w * w) - K, o1 = (j / w) % w - K, o2 = j % w - K;
+    const int ii[3] = {((cidx[0] + o0) % n + n) % n, ((cidx[1] + o1) % n + n) % n,
+                       ((cidx[2] + o2) % n + n) % n};
+    R R2 = 0;
+    for (int d = 0; d < 3; ++d) {
+      const R xs = ((R)ii[d] + (R)0.5) * dx;
+      const R dd = fabs(xs - pos[d]);
+      const R pd = fmin(dd, L - dd);
+      R2 = R2 + pd * pd;
+    }
+    if (R2 <= r_acc * r_acc) {
+      const long long c = ((long long)ii[0] * n + ii[1]) * n + ii[2];
+      const R W = exp((R)-0.5 * R2 / (rK * rK));
+      sW += (double)W;
+      sWr += (double)(W * rho[c]);
+      sM += (double)rho[c];
+    }
+  }
+  red[0][threadIdx.x] = sW;
+  red[1][threadIdx.x] = sWr;
+  red[2][threadIdx.x] = sM;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s)
+      for (int k = 0; k < 3; ++k) red[k][threadIdx.x] += red[k][threadIdx.x + s];
+    __syncthreads();
+  }
+  const double sumW = red[0][0] + 1e-30;
+  const double sumWRho = red[1][0] + 1e-30;
+  const double rho_inf = red[1][0] / sumW;
+  const double GMd = (double)G * (double)M;
+  const double dMdt = 4.0 * 3.14159265358979323846 * (double)lam * GMd * GMd * rho_inf /
+                      ((double)cs * cs * cs);
+  const double dM = dMdt * (double)dt;
+  const double M_avail = red[2][0] * (double)dx * dx * dx;
+  const double dM_cap = fmin(dM, (double)fmax_frac * M_avail);
+  __syncthreads();
+  for (int j = threadIdx.x; j < tot; j += blockDim.x) {
+    const int o0 = j / (w * w) - K, o1 = (j / w) % w - K, o2 = j % w - K;
+    const int ii[3] = {((cidx[0] + o0) % n + n) % n, ((cidx[1] + o1) % n + n) % n,
+                       ((cidx[2] + o2) % n + n) % n};
+    R R2 = 0;
+    for (int d = 0; d < 3; ++d) {
+      const R xs = ((R)ii[d] + (R)0.5) * dx;
+      const R dd = fabs(xs - pos[d]);
+      const R pd = fmin(dd, L - dd);
+      R2 = R2 + pd * pd;
+    }
+    if (R2 <= r_acc * r_acc) {
+      const long long c = ((long long)ii[0] * n + ii[1]) * n + ii[2];
+      const R W = exp((R)-0.5 * R2 / (rK * rK));
+      const double phi = (double)(W * rho[c]) / sumWRho;
+      rho[c] = (R)fmax(0.0, (double)rho[c] - dM_cap / ((double)dx * dx * dx) * phi);
+    }
+  }
+  if (threadIdx.x == 0) m_bh[0] = (R)((double)M + dM_cap);
+}
+
+}  // namespace
+
+int launch_hydro(bool dbl, const void *rho, const void *vx, const void *vy, const void *vz,
+                 void *orho, void *ovx, void *ovy, void *ovz, int n, double dx, double dt,
+                 double cs, int clamp_rho, cudaStream_t st) {
+  const long long ncell = (long long)n * n * n;
+  const int T = 128;
+  const int B = (int)((ncell + T - 1) / T);
+  const double vol = dx * dx * dx, fac = dt * dx * dx;
+  if (dbl)
+    k_hydro<double><<<B, T, 0, st>>>((const double *)rho, (const double *)vx, (const double *)vy,
+                                     (const double *)vz, (double *)orho, (double *)ovx,
+                                     (double *)ovy, (double *)ovz, n, dx, dt, cs, vol, fac, clamp_rho);
+  else
+    k_hydro<float><<<B, T, 0, st>>>((const float *)rho, (const float *)vx, (const float *)vy,
+                                    (const float *)vz, (float *)orho, (float *)ovx, (float *)ovy,
+                                    (float *)ovz, n, (float)dx, (float)dt, (float)cs, (float)vol,
+                                    (float)fac, clamp_rho);
+  QJ_CK_LAUNCH();
+  return 0;
+}
+
+int launch_accrete(bool dbl, void *psi, const void *pos, const void *vel, void *m_bh, int n,
+                   double dx, double sigma_v, double G, double m_per_hbar, double c_light,
+                   double dt, cudaStream_t st) {
+  const double vol = dx * dx * dx;
+  if (dbl)
+    k_accrete<double><<<1, 32, 0, st>>>((double2 *)psi, (const double *)pos, (const double *)vel,
+                                        (double *)m_bh, n, dx, vol, sigma_v, G, m_per_hbar,
+                                        c_light, dt);
+  else
+    k_accrete<float><<<1, 32, 0, st>>>((float2 *)psi, (const float *)pos, (const float *)vel,
+                                       (float *)m_bh, n, (float)dx, (float)vol, (float)sigma_v,
+                                       (float)G, (float)m_per_hbar, (float)c_light, (float)dt);
+  QJ_CK_LAUNCH();
+  return 0;
+}
+
+int launch_bondi(bool dbl, void *rho, const void *pos, void *m_bh, int n, double dx, double L,
+                 double cs, double G, double dt, double r_acc_mult, cudaStream_t st) {
+  const int K = (int)std::ceil(r_acc_mult) + 1;
+  if (2 * K + 1 > n) {
+    set_error("Bondi sink: accretion radius %g cells is too large for a %d^3 grid", r_acc_mult, n);
+    return QJ_ERR_ARG;
+  }
+  const double lam = std::exp(1.5) / 4.0, fmaxf_ = 0.25;
+  if (dbl)
+    k_bondi<double><<<1, 256, 0, st>>>((double *)rho, (const double *)pos, (double *)m_bh, n, dx, L,
+                                       cs, G, dt, r_acc_mult, lam, fmaxf_, K);
+  else
+    k_bondi<float><<<1, 256, 0, st>>>((float *)rho, (const float *)pos, (float *)m_bh, n, (float)dx,
+                                      (float)L, (float)cs, (float)G, (float)dt,
+                                      (float)r_acc_mult, (float)lam, (float)fmaxf_, K);
+  QJ_CK_LAUNCH();
+  return 0;
+}
+
+}  // namespace qj

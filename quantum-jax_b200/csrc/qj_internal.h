@@ -132,6 +132,16 @@ int launch_amax3(bool dbl, const void *ax, const void *ay, const void *az, long 
 int launch_gas_kick(bool dbl, void *vx, void *vy, void *vz, const void *ax, const void *ay,
                     const void *az, double dt, long long ncell, cudaStream_t st);
 
+// ----- gas and black hole (qj_gas.cu) -----
+int launch_hydro(bool dbl, const void *rho, const void *vx, const void *vy, const void *vz,
+                 void *orho, void *ovx, void *ovy, void *ovz, int n, double dx, double dt,
+                 double cs, int clamp_rho, cudaStream_t st);
+int launch_accrete(bool dbl, void *psi, const void *pos, const void *vel, void *m_bh, int n,
+                   double dx, double sigma_v, double G, double m_per_hbar, double c_light,
+                   double dt, cudaStream_t st);
+int launch_bondi(bool dbl, void *rho, const void *pos, void *m_bh, int n, double dx, double L,
+                 double cs, double G, double dt, double r_acc_mult, cudaStream_t st);
+
 // ----- small scalar kernels (qj_particles.cu) -----
 int launch_diag_load(bool dbl, const void *diag, void *amax_bits, cudaStream_t st);
 int launch_diag_store(bool dbl, void *diag, const void *amax_bits, const void *dts_bits,

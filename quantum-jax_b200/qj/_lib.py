@@ -49,6 +49,11 @@ SIGNATURES = {
     "qj_kdk_step": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_double, c_double,
                             c_int, c_int, c_void_p, c_void_p, c_void_p]),
     "qj_fft3d": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
+    "qj_kdk_gas_bh_step": (c_int, [c_void_p] + [c_void_p] * 8 + [c_int, c_double, c_int, c_double,
+                                                                 c_int, c_double,
+                                                                 ctypes.POINTER(c_double), c_void_p]),
+    "qj_kdk_cosmo": (c_int, [c_void_p, c_void_p, ctypes.POINTER(c_double), c_double, c_double,
+                             c_double, c_double, c_int, c_void_p]),
     "qj_get_potential_f32_noalloc": (c_int, [ctypes.POINTER(QjGrid), ctypes.POINTER(QjPhys),
                                              c_void_p, c_void_p, c_int, c_void_p]),
     "qj_plan_workspace_bytes": (c_int64, [c_void_p]),

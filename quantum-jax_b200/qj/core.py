@@ -179,6 +179,44 @@ class Plan:
         check(lib().qj_fft3d(self._h, _ptr(x), _ptr(out), 1 if inverse else -1, _stream()))
         return out
 
+    def kdk_gas_bh(self, psi, rho, vx, vy, vz, m_bh, pos, vel, dt, nsteps=1, t=0.0,
+                   sigma_v=None, dm_accretion=True, bondi_r_acc_mult=None):
+        """nsteps x compute_step(psi, rho, vx, vy, vz, m_bh, pos, vel, t) of
+        quantum-gas-bh.py:537-578, in place; returns t.  rho=None: no gas
+        (quantum-bh.py).  bondi_r_acc_mult: optional isothermal Bondi gas sink
+        (quantum-fluid-accretion-test.py:454-494)."""
+        self._field(psi, "psi", complex_=True)
+        gas = rho is not None
+        if gas:
+            for name, f in (("rho", rho), ("vx", vx), ("vy", vy), ("vz", vz)):
+                self._field(f, name)
+        n_bh = 0
+        if pos is not None:
+            self._particles(pos, "pos")
+            n_bh = pos.shape[0]
+            self._particles(vel, "vel", n_bh)
+            if m_bh.dtype != self.rdtype or m_bh.shape != (n_bh,) or not m_bh.is_cuda:
+                raise ValueError("m_bh must be a CUDA [n_bh] tensor of the plan's real type")
+        t_io = ctypes.c_double(float(t))
+        sv = self.phys.cs if sigma_v is None else float(sigma_v)
+        check(lib().qj_kdk_gas_bh_step(
+            self._h, _ptr(psi), _ptr(rho) if gas else None, _ptr(vx) if gas else None,
+            _ptr(vy) if gas else None, _ptr(vz) if gas else None,
+            _ptr(m_bh) if n_bh else None, _ptr(pos) if n_bh else None,
+            _ptr(vel) if n_bh else None, n_bh, float(dt), int(nsteps), sv,
+            int(bool(dm_accretion)), float(bondi_r_acc_mult or 0.0), ctypes.byref(t_io),
+            _stream()))
+        return t_io.value
+
+    def kdk_cosmo(self, psi, a, da, H0, omega_m, omega_l, nsteps=1):
+        """nsteps x compute_step(psi, a) of quantum-cosmo.py:169-196, in place;
+        returns the new scale factor a."""
+        self._field(psi, "psi", complex_=True)
+        a_io = ctypes.c_double(float(a))
+        check(lib().qj_kdk_cosmo(self._h, _ptr(psi), ctypes.byref(a_io), float(da), float(H0),
+                                 float(omega_m), float(omega_l), int(nsteps), _stream()))
+        return a_io.value
+
     def kdk_step(self, psi, pos, vel, diag, dt, nsteps=1, m_s=0.0, self_interaction=False,
                  v_ext=None):
         """nsteps x compute_step (quantum-stars.py:295-330), in place.

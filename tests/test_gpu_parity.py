@@ -224,6 +224,32 @@ def test_bad_arguments_raise():
         plan.bin_stars(pos, m_s=1.0)
 
 
+@pytest.mark.parametrize("dbl", [False, True])
+def test_cosmo_step(dbl):
+    """quantum-cosmo.py:169-196 with the script's constants (h = 1, m22 = 2.5,
+    omega_m = 0.27, omega_l = 0.73) on a 32^3 box of the script's size."""
+    qj = qj_mod()
+    G = 4.30241002e-6
+    H0 = 0.1
+    om, ol = 0.27, 0.73
+    rho_crit = 3.0 * H0**2 / (8.0 * np.pi * G)
+    m_per_hbar = 2.5e-22 * 8.96215334e-67 / 1.71818134e-87
+    g = O.Grid(32, 32, 32, 1000.0, 1000.0, 1000.0)
+    p = O.Phys(m_per_hbar=m_per_hbar, G=G, rho_bar=om * rho_crit)
+    psi = np.sqrt(p.rho_bar * (1.0 + 0.1 * O.delta_field(32, 7))).astype(np.complex128)
+    a0, da = 1.0 / 128.0, 1.0e-4
+    ref, a = psi, a0
+    for _ in range(6):
+        ref, a = O.cosmo_compute_step(ref, a, da, g, p, H0, om, ol)
+    plan = make_plan(g, p, qj.PLAIN_F64 if dbl else qj.FUSED_F32, 1)
+    ps = cuda(psi, torch.complex128 if dbl else torch.complex64)
+    a1 = plan.kdk_cosmo(ps, a0, da, H0, om, ol, 4)
+    a2 = plan.kdk_cosmo(ps, a1, da, H0, om, ol, 2)
+    torch.cuda.synchronize()
+    assert a2 == pytest.approx(a, rel=1e-14)
+    assert O.rel_l2(ps.cpu().numpy(), ref) < (1e-11 if dbl else 1e-5)
+
+
 def test_fused_large_kick_phase():
     """Kick phases of O(20) rad exercise the float64 quadrant reduction of
     the kick's sin / cos (every quadrant is visited)."""
