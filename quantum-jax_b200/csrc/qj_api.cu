@@ -113,6 +113,7 @@ struct qj_plan {
   int64_t ws_bytes = 0;
   // tables
   void *tw[3] = {nullptr, nullptr, nullptr};  // float2 / double2
+  float2 *tws[3] = {nullptr, nullptr, nullptr};  // stage twiddle tables (fused passes)
   double *kd[3] = {nullptr, nullptr, nullptr};
   float *kf[3] = {nullptr, nullptr, nullptr};
   float *ktf[3] = {nullptr, nullptr, nullptr};
@@ -236,7 +237,7 @@ FusedArgs fused_args(const qj_plan *P, int axis) {
   a.R = P->R;
   a.S1 = P->S1;
   a.S2 = P->S2;
-  a.tw = (const float2 *)P->tw[axis];
+  a.tw = P->tws[axis];
   a.prop = P->prop[axis];
   for (int d = 0; d < 3; ++d) {
     a.k[d] = P->kf[d];
@@ -734,6 +735,10 @@ int qj_plan_create(qj_plan **plan, const qj_grid *grid, const qj_phys *phys, int
       }
       if ((rc = dev_alloc(P, &P->tw[a], N * sizeof(float2)))) break;
       e = cudaMemcpy(P->tw[a], w.data(), N * sizeof(float2), cudaMemcpyHostToDevice);
+      const std::vector<float2> ts = stage_twiddles(N);
+      if (e == cudaSuccess && !(rc = dev_alloc_t(P, &P->tws[a], ts.size())))
+        e = cudaMemcpy(P->tws[a], ts.data(), ts.size() * sizeof(float2), cudaMemcpyHostToDevice);
+      if (rc) break;
     }
     if (e != cudaSuccess) rc = cuda_fail(e, "cudaMemcpy(twiddles)", __FILE__, __LINE__);
   }

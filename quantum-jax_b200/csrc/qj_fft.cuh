@@ -145,18 +145,36 @@ template <int N> __host__ __device__ constexpr int stage_ns(int s) {
 //  Strided passes: layout [N][TP] (pencils fastest; lanes run over pencils).
 //  Contiguous passes: layout [TP][N + N/16] (elements fastest, padded so the
 //  radix-r scatter of the first stage is bank-conflict free).
+// A strided pencil's P threads span several warps (the CTA synchronises); a
+// contiguous pencil's P <= 32 threads sit inside one warp, whose private rows
+// need only a warp barrier.
 template <typename C, int TP> struct SmemStrided {
   C *base;  // &sm[p]
   __device__ __forceinline__ C ld(int idx) const { return base[idx * TP]; }
   __device__ __forceinline__ void st(int idx, C v) const { base[idx * TP] = v; }
+  __device__ __forceinline__ static void sync() { __syncthreads(); }
 };
 template <typename C> struct SmemContig {
   C *row;  // &sm[p * (N + N/16)]
   __device__ __forceinline__ C ld(int idx) const { return row[idx + (idx >> 4)]; }
   __device__ __forceinline__ void st(int idx, C v) const { row[idx + (idx >> 4)] = v; }
+  __device__ __forceinline__ static void sync() { __syncwarp(); }
 };
 
-template <int N, int DIR, int S, typename C, class SM> struct FftStages {
+// Stage twiddle tables: for stage s > 0 (Ns = product of earlier radices,
+// radix r), entry (q - 1) * Ns + jm holds w_N^(jm q N / (Ns r)); the stages
+// are concatenated.  Threads of one stage read consecutive jm, so the table is
+// bank-conflict free when staged in shared memory.
+template <int N> __host__ __device__ constexpr int stage_tw_off(int s) {
+  int off = 0;
+  for (int i = 1; i < s; ++i) off += stage_ns<N>(i) * (FftPlan<N>::radix(i) - 1);
+  return off;
+}
+template <int N> __host__ __device__ constexpr int stage_tw_size() {
+  return stage_tw_off<N>(FftPlan<N>::NS);
+}
+
+template <int N, int DIR, int S, typename C, class SM, bool TWS> struct FftStages {
   using PL = FftPlan<N>;
   static constexpr int E = PL::E, P = N / E;
   static constexpr int r = PL::radix(S);
@@ -184,7 +202,11 @@ template <int N, int DIR, int S, typename C, class SM> struct FftStages {
         const int jm = j % Ns;
 #pragma unroll
         for (int q = 1; q < r; ++q) {
-          const C w = __ldg(&tw[jm * q * (N / (Ns * r))]);
+          C w;
+          if constexpr (TWS)
+            w = tw[stage_tw_off<N>(S) + (q - 1) * Ns + jm];
+          else
+            w = __ldg(&tw[jm * q * (N / (Ns * r))]);
           a[q] = DIR < 0 ? cmul(a[q], w) : cmulc(a[q], w);
         }
       }
@@ -193,7 +215,7 @@ template <int N, int DIR, int S, typename C, class SM> struct FftStages {
       for (int q = 0; q < r; ++q) v[u + q * B] = a[q];
     }
     if constexpr (S + 1 < PL::NS) {
-      __syncthreads();  // every thread has finished reading the buffer
+      SM::sync();  // every thread of the pencil has finished reading its rows
 #pragma unroll
       for (int u = 0; u < B; ++u) {
         const int j = t + P * u;
@@ -201,19 +223,20 @@ template <int N, int DIR, int S, typename C, class SM> struct FftStages {
 #pragma unroll
         for (int q = 0; q < r; ++q) sm.st(idxD + q * Ns, v[u + q * B]);
       }
-      __syncthreads();
-      FftStages<N, DIR, S + 1, C, SM>::run(v, t, sm, tw);
+      SM::sync();
+      FftStages<N, DIR, S + 1, C, SM, TWS>::run(v, t, sm, tw);
     }
   }
 };
 
 // Transform the pencil held by the P threads of a group.  Every thread of the
-// CTA must call this the same number of times (it contains __syncthreads when
-// the plan has more than one stage).
-template <int N, int DIR, typename C, class SM>
+// CTA (strided) or warp (contiguous) must call this the same number of times.
+// TWS: tw is the stage twiddle table (usually in shared memory); otherwise the
+// flat table w[m] = exp(-2 pi i m / N) in global memory.
+template <int N, int DIR, bool TWS = false, typename C, class SM>
 __device__ __forceinline__ void fft_pencil(C (&v)[FftPlan<N>::E], int t, const SM &sm,
                                            const C *__restrict__ tw) {
-  FftStages<N, DIR, 0, C, SM>::run(v, t, sm, tw);
+  FftStages<N, DIR, 0, C, SM, TWS>::run(v, t, sm, tw);
 }
 
 // Launch shape of a pencil pass over length N.

@@ -1,5 +1,8 @@
 // Instantiations and launchers of the fused single-precision pencil passes.
+#include <cmath>
+#include <cstdlib>
 #include <mutex>
+#include <vector>
 
 #include "qj_internal.h"
 
@@ -16,6 +19,33 @@ static int grid_of(const FusedArgs &a) {
   return (a.axis == 0 ? a.ny : a.nx) * (a.nz / 16);
 }
 
+// Stage twiddle table of length n (see stage_tw_off), long double, rounded once.
+template <int N> static std::vector<float2> stage_table() {
+  std::vector<float2> t(stage_tw_size<N>() > 0 ? stage_tw_size<N>() : 1);
+  for (int s = 1; s < FftPlan<N>::NS; ++s) {
+    const int ns = stage_ns<N>(s), r = FftPlan<N>::radix(s);
+    for (int q = 1; q < r; ++q)
+      for (int jm = 0; jm < ns; ++jm) {
+        const long long m = (long long)jm * q * (N / (ns * r));
+        const long double th = -2.0L * 3.14159265358979323846264338327950288L * m / N;
+        t[stage_tw_off<N>(s) + (q - 1) * ns + jm] = float2{(float)cosl(th), (float)sinl(th)};
+      }
+  }
+  return t;
+}
+
+std::vector<float2> stage_twiddles(int n) {
+  switch (n) {
+    case 16: return stage_table<16>();
+    case 32: return stage_table<32>();
+    case 64: return stage_table<64>();
+    case 128: return stage_table<128>();
+    case 256: return stage_table<256>();
+    case 512: return stage_table<512>();
+  }
+  return {};
+}
+
 int pass_blocks(int n_axis, int axis, int nx, int ny, int nz) {
   if (axis == 2) {
     const int E = (n_axis == 32 || n_axis == 64) ? 8 : 16;
@@ -29,7 +59,7 @@ int pass_blocks(int n_axis, int axis, int nx, int ny, int nz) {
 template <int N, bool CONTIG, int MODE>
 static int run_fused(const FusedArgs &a, cudaStream_t st) {
   using SH = PassShape<N, CONTIG>;
-  const size_t smem = SH::template smem_bytes<float2>();
+  const size_t smem = SH::template smem_bytes<float2>() + stage_tw_size<N>() * sizeof(float2);
   static std::once_flag once;
   static cudaError_t attr_err = cudaSuccess;
   std::call_once(once, [&] {
@@ -37,7 +67,21 @@ static int run_fused(const FusedArgs &a, cudaStream_t st) {
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   });
   QJ_CK(attr_err);
-  k_fused<N, CONTIG, MODE><<<grid_of<N, CONTIG>(a), SH::THREADS, smem, st>>>(a);
+  // L2 prefetch distance: the CTAs resident at once (occupancy x SMs) times
+  // QJ_L2_PREFETCH_WAVES (default 1; 0 disables).
+  static int ahead = -1;
+  if (ahead < 0) {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fused<N, CONTIG, MODE>, SH::THREADS, smem);
+    const char *env = getenv("QJ_L2_PREFETCH_WAVES");
+    const int waves = env ? atoi(env) : 0;
+    ahead = waves > 0 ? waves * sms * (per_sm > 0 ? per_sm : 1) : 0;
+  }
+  FusedArgs b = a;
+  b.ahead = ahead;
+  k_fused<N, CONTIG, MODE><<<grid_of<N, CONTIG>(a), SH::THREADS, smem, st>>>(b);
   QJ_CK_LAUNCH();
   return 0;
 }

@@ -5,6 +5,7 @@
 #include <stdint.h>
 
 #include <atomic>
+#include <vector>
 
 #include "qj_pass.cuh"
 
@@ -37,6 +38,8 @@ void prof_mark_begin(cudaStream_t st);
 void prof_mark_end(int bucket, cudaStream_t st);
 
 bool fft_length_supported(int n);
+// Stage twiddle table of the fused passes for length n (host, float2).
+std::vector<float2> stage_twiddles(int n);
 
 // ----- pencil passes (qj_fused.cu, qj_fftpass.cu) -----
 // Launch one fused single-precision pass of `mode` along `a.axis` (length n).

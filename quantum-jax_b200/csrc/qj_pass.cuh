@@ -45,7 +45,7 @@ struct FusedArgs {
   float2 *R;
   float2 *S1;
   float2 *S2;
-  const float2 *tw;    // twiddles of this axis' length
+  const float2 *tw;    // stage twiddle table of this axis' length (stage_tw_off)
   const float2 *prop;  // drift propagator of this axis, already scaled by 1/n
   const float *k[3];   // k value per index, per axis (Nyquist negative)
   const float *kt[3];  // k with the Nyquist entry set to 0 (odd derivatives)
@@ -75,6 +75,9 @@ struct FusedArgs {
   const float *grho;
   float *gv[3];
   float gas_dt;
+  // L2 prefetch distance in CTAs (0 = off): each CTA prefetches the input
+  // tile of CTA blockIdx.x + ahead, one resident wave later
+  int ahead;
 };
 
 // Per-thread position of a pencil in the grid.
@@ -120,7 +123,7 @@ __device__ __forceinline__ void load_pencil(C (&v)[E], const C *__restrict__ f, 
   const unsigned b = (unsigned)base + (unsigned)t * (unsigned)stride;
   const unsigned s = (unsigned)P * (unsigned)stride;
 #pragma unroll
-  for (int e = 0; e < E; ++e) v[e] = f[b + (unsigned)e * s];
+  for (int e = 0; e < E; ++e) v[e] = __ldcs(&f[b + (unsigned)e * s]);  // read once: evict first
 }
 template <int E, typename C>
 __device__ __forceinline__ void store_pencil(const C (&v)[E], C *__restrict__ f, long long base,
@@ -311,9 +314,45 @@ __device__ __forceinline__ float2 phase_rotate(float2 z, double theta) {
   return float2{z.x * c + z.y * s, z.y * c - z.x * s};
 }
 
+// Bring the tile of CTA `blk` of field f into L2 (cp.async.bulk.prefetch.L2:
+// no registers, no shared memory, no completion to wait for).  Strided tiles
+// are N rows of 16 complex64 (128 B); contiguous tiles are TP rows of N.
+template <int N, bool CONTIG>
+__device__ __forceinline__ void prefetch_tile(const float2 *f, const FusedArgs &a, int blk) {
+  using SH = PassShape<N, CONTIG>;
+  const int tid = threadIdx.x;
+  if (CONTIG) {
+    if (tid < SH::TP) {
+      const float2 *row = f + (long long)(blk * SH::TP + tid) * a.nz;
+      asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(row), "r"(N * 8) : "memory");
+    }
+  } else {
+    for (int i = tid; i < N; i += SH::THREADS) {
+      const int o = blk / a.ztiles;
+      const float2 *row = f + (long long)o * a.outer_stride + (blk % a.ztiles) * 16 + (long long)i * a.stride;
+      asm volatile("cp.async.bulk.prefetch.L2.global [%0], 128;" ::"l"(row) : "memory");
+    }
+  }
+}
+
 template <int N, bool CONTIG, int MODE>
 __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CONTIG>::MINB)
     k_fused(FusedArgs a) {
+  if (a.ahead > 0 && (int)blockIdx.x + a.ahead < (int)gridDim.x) {
+    const int nb = blockIdx.x + a.ahead;
+    if constexpr (MODE == M_DENSITY || MODE == M_DRIFT || MODE == M_DRIFT_DENSITY) {
+      prefetch_tile<N, CONTIG>(a.psi, a, nb);
+    } else if constexpr (MODE == M_FFT_FWD || MODE == M_POISSON) {
+      prefetch_tile<N, CONTIG>(a.R, a, nb);
+    } else if constexpr (MODE == M_IFFT2) {
+      prefetch_tile<N, CONTIG>(a.S1, a, nb);
+      prefetch_tile<N, CONTIG>(a.S2, a, nb);
+    } else if constexpr (MODE == M_KICK) {
+      prefetch_tile<N, CONTIG>(a.S1, a, nb);
+      prefetch_tile<N, CONTIG>(a.S2, a, nb);
+      prefetch_tile<N, CONTIG>(a.psi, a, nb);
+    }
+  }
   using SH = PassShape<N, CONTIG>;
   constexpr int E = SH::E, P = SH::P, TP = SH::TP, THREADS = SH::THREADS;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -337,7 +376,11 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CO
     smv.row = sm + p * SH::ROW;
   else
     smv.base = sm + p;
-  const float2 *tw = a.tw;
+  // the stage twiddle table of this axis, staged after the exchange rows
+  float2 *tw_s = sm + SH::template smem_bytes<float2>() / sizeof(float2);
+  for (int i = tid; i < stage_tw_size<N>(); i += THREADS) tw_s[i] = a.tw[i];
+  __syncthreads();
+  const float2 *tw = tw_s;
 
   if constexpr (MODE == M_DENSITY) {
     float2 v[E];
@@ -345,12 +388,12 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CO
     double s = build_density<N, E>(v, a, pp, t, P);
     s = block_sum<THREADS>(s, red);
     if (tid == 0) a.part[blockIdx.x] = s;
-    fft_pencil<N, -1>(v, t, smv, tw);
+    fft_pencil<N, -1, true>(v, t, smv, tw);
     store_pencil<E>(v, a.R, base, st, t, P);
   } else if constexpr (MODE == M_FFT_FWD) {
     float2 v[E];
     load_pencil<E>(v, a.R, base, st, t, P);
-    fft_pencil<N, -1>(v, t, smv, tw);
+    fft_pencil<N, -1, true>(v, t, smv, tw);
     store_pencil<E>(v, a.R, base, st, t, P);
   } else if constexpr (MODE == M_POISSON) {
     float2 v[E];
@@ -362,7 +405,7 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CO
       for (int i = tid; i < a.n_part; i += THREADS) s += a.part_in[i];
       mean = block_sum<THREADS>(s, red) * a.inv_ncell;
     }
-    fft_pencil<N, -1>(v, t, smv, tw);
+    fft_pencil<N, -1, true>(v, t, smv, tw);
     const int ax = a.axis;            // r: 0 or 2
     const int aq = 2 - ax;            // the other non-y axis
     const float kq2 = a.k[aq][pp.c[aq]] * a.k[aq][pp.c[aq]];
@@ -389,17 +432,17 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CO
       // (kty - i ktq) * vh
       w[e] = float2{kty * vh.x + ktq * vh.y, kty * vh.y - ktq * vh.x};
     }
-    fft_pencil<N, +1>(v, t, smv, tw);
+    fft_pencil<N, +1, true>(v, t, smv, tw);
     store_pencil<E>(v, a.S1, base, st, t, P);
-    fft_pencil<N, +1>(w, t, smv, tw);
+    fft_pencil<N, +1, true>(w, t, smv, tw);
     store_pencil<E>(w, a.S2, base, st, t, P);
   } else if constexpr (MODE == M_IFFT2) {
     float2 v[E];
     load_pencil<E>(v, a.S1, base, st, t, P);
-    fft_pencil<N, +1>(v, t, smv, tw);
+    fft_pencil<N, +1, true>(v, t, smv, tw);
     store_pencil<E>(v, a.S1, base, st, t, P);
     load_pencil<E>(v, a.S2, base, st, t, P);
-    fft_pencil<N, +1>(v, t, smv, tw);
+    fft_pencil<N, +1, true>(v, t, smv, tw);
     store_pencil<E>(v, a.S2, base, st, t, P);
   } else if constexpr (MODE == M_KICK) {
     const int aq = a.axis;  // the kick axis; ar = 2 - aq is the Poisson axis
@@ -410,7 +453,7 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CO
       // phase 1: S1 -> V + i a_r
       float2 v1[E];
       load_pencil<E>(v1, a.S1, base, st, t, P);
-      fft_pencil<N, +1>(v1, t, smv, tw);
+      fft_pencil<N, +1, true>(v1, t, smv, tw);
 #pragma unroll
       for (int e = 0; e < E; ++e) {
         V[e] = v1[e].x;
@@ -432,7 +475,7 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CO
       // phase 2: S2 -> a_q + i a_y
       float2 v2[E];
       load_pencil<E>(v2, a.S2, base, st, t, P);
-      fft_pencil<N, +1>(v2, t, smv, tw);
+      fft_pencil<N, +1, true>(v2, t, smv, tw);
 #pragma unroll
       for (int e = 0; e < E; ++e) am = fmaxf(am, fmaxf(fabsf(v2[e].x), fabsf(v2[e].y)));
       if (a.has_stars)
@@ -481,10 +524,10 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CO
 #pragma unroll
     for (int e = 0; e < E; ++e) ps[e] = phase_rotate(ps[e], a.kick_coef * (double)V[e]);
     if (a.do_drift) {
-      fft_pencil<N, -1>(ps, t, smv, tw);
+      fft_pencil<N, -1, true>(ps, t, smv, tw);
 #pragma unroll
       for (int e = 0; e < E; ++e) ps[e] = cmul(ps[e], __ldg(&a.prop[t + P * e]));
-      fft_pencil<N, +1>(ps, t, smv, tw);
+      fft_pencil<N, +1, true>(ps, t, smv, tw);
     }
     store_pencil<E>(ps, a.psi, base, st, t, P);
 #pragma unroll
@@ -513,16 +556,16 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CO
   } else if constexpr (MODE == M_DRIFT || MODE == M_DRIFT_DENSITY) {
     float2 v[E];
     load_pencil<E>(v, a.psi, base, st, t, P);
-    fft_pencil<N, -1>(v, t, smv, tw);
+    fft_pencil<N, -1, true>(v, t, smv, tw);
 #pragma unroll
     for (int e = 0; e < E; ++e) v[e] = cmul(v[e], __ldg(&a.prop[t + P * e]));
-    fft_pencil<N, +1>(v, t, smv, tw);
+    fft_pencil<N, +1, true>(v, t, smv, tw);
     store_pencil<E>(v, a.psi, base, st, t, P);
     if constexpr (MODE == M_DRIFT_DENSITY) {
       double s = build_density<N, E>(v, a, pp, t, P);
       s = block_sum<THREADS>(s, red);
       if (tid == 0) a.part[blockIdx.x] = s;
-      fft_pencil<N, -1>(v, t, smv, tw);
+      fft_pencil<N, -1, true>(v, t, smv, tw);
       store_pencil<E>(v, a.R, base, st, t, P);
     }
   }
