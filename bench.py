@@ -59,6 +59,10 @@ def parse():
     ap.add_argument("--plain-steps", type=int, default=10)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--adj-n", type=int, default=128)
+    ap.add_argument("--adj-steps", type=int, default=200)
+    ap.add_argument("--adj-ckpt", type=int, default=20)
     ap.add_argument("--e2e-sub", type=int, default=10,
                     help="steps per public-API call in the e2e leg (the reference's nt_sub)")
     return ap.parse_args()
@@ -367,6 +371,56 @@ def main():
                                f"host-sync interval nt_sub)"}
         step.plan.close()
 
+    # ---------------- adjoint / forward time (128^3, 200 steps, ckpt 20) -------
+    adjoint = None
+    if not a.no_adjoint:
+        from qj.autograd import kdk_evolve
+
+        na, steps_a, K = a.adj_n, a.adj_steps, a.adj_ckpt
+        psi_a, _, _, ga, pa = O.stars_ic(na, 0, seed=0)
+        dta = O.default_dt(ga, pa)
+        plan_a = qj.Plan(qj.Grid(na, na, na), qj.Phys(m_per_hbar=1.0, G=pa.G, rho_bar=pa.rho_bar),
+                         qj.FUSED_F32, 1)
+        s = torch.as_tensor(np.abs(psi_a), dtype=torch.float32, device=dev)
+        th = torch.as_tensor(0.5 * O.delta_field(na, 21), dtype=torch.float32,
+                             device=dev).requires_grad_(True)
+        psi2, *_ = O.stars_ic(na, 0, seed=1)
+        tgt = torch.as_tensor(np.abs(psi2) ** 2, dtype=torch.float32, device=dev)
+
+        def fwd():
+            return kdk_evolve(th, s, plan_a, dta, steps_a, K)
+
+        def run_bwd(psiT):
+            L = torch.mean((torch.abs(psiT) ** 2 - tgt) ** 2)
+            L.backward()
+
+        run_bwd(fwd())  # warm-up
+        barrier()
+        psi_plain = torch.polar(s, th.detach()).to(torch.complex64)
+        diag_a = torch.tensor([0.0, 0.0, dta], dtype=torch.float64, device=dev)
+        e0.record(stream)
+        plan_a.kdk_step(psi_plain, None, None, diag_a, dta, steps_a)
+        e1.record(stream)
+        barrier()
+        f_ms = e0.elapsed_time(e1)
+        e0.record(stream)
+        psiT = fwd()
+        e1.record(stream)
+        barrier()
+        fc_ms = e0.elapsed_time(e1)
+        th.grad = None
+        e0.record(stream)
+        run_bwd(psiT)
+        e1.record(stream)
+        barrier()
+        b_ms = e0.elapsed_time(e1)
+        adjoint = {"grid": [na] * 3, "steps": steps_a, "checkpoint_every": K,
+                   "forward_ms": f_ms, "forward_with_checkpoints_ms": fc_ms,
+                   "backward_ms": b_ms, "adjoint_over_forward": b_ms / f_ms,
+                   "note": "backward = chunk recompute from checkpoints + reverse sweep "
+                           "(two Poisson solves per kick); forward = qj_kdk_step, psi only"}
+        plan_a.close()
+
     cb = None
     if rank == 0 and world == 1 and not a.no_cpu:
         cb = cpu_baseline(n, n_s, 2)
@@ -390,7 +444,8 @@ def main():
                              "pos_rel_l2_vs_f64": pos_err,
                              "f64_path": "plain float64 GPU path (matches the oracle to 1e-11)"},
                 "roofline": roofline, "step_roofline": step_roof, "passes": per_pass,
-                "gpu_launches": launches, "clocks": clk, "e2e": e2e, "cpu_baseline": cb}
+                "gpu_launches": launches, "clocks": clk, "e2e": e2e, "cpu_baseline": cb,
+                "adjoint": adjoint}
         print(json.dumps(line), flush=True)
     fused.close()
     if dist is not None:

@@ -72,11 +72,19 @@ typedef struct qj_diag {
 
 /* Create / destroy a plan.  Replaces the module-level set-up of
  * quantum-stars.py:61-157 (grid, k-grid, constants).  Supported lengths per
- * axis: 16, 32, 64, 128, 256, 512; nz must be a multiple of 16.
+ * axis: 16, 32, 64, 96, 128, 256, 512; nz must be a multiple of 16.
  * max_particles bounds n_s of later calls (workspace is sized for it). */
 int qj_plan_create(qj_plan **plan, const qj_grid *grid, const qj_phys *phys,
                    int precision, int max_particles);
 int qj_plan_destroy(qj_plan *plan);
+/* A batched plan holds nbox independent boxes of one grid (QJ_FUSED_F32 only;
+ * the IC-ensemble form of the step, one script run per box in the reference).
+ * Its qj_kdk_step takes psi [nbox][nx][ny][nz], pos / vel [nbox][n_s][3] and
+ * nbox qj_diag records; every pass launch covers all boxes.  The other entry
+ * points need nbox == 1. */
+int qj_plan_create_batched(qj_plan **plan, const qj_grid *grid,
+                           const qj_phys *phys, int precision,
+                           int max_particles, int nbox);
 /* Update rho_bar / b_coeff / G / m_per_hbar / cs of an existing plan. */
 int qj_plan_set_phys(qj_plan *plan, const qj_phys *phys);
 
@@ -129,6 +137,23 @@ int qj_kdk_gas_bh_step(qj_plan *plan, void *psi, void *rho, void *vx, void *vy,
                        double dt, int nsteps, double sigma_v, int dm_accretion,
                        double bondi_r_acc_mult, double *t_io, void *stream);
 
+/* Gradient of the psi-only KDK step (no particles; optional self-interaction
+ * and static V_ext).  The reference claims differentiability (README.md:7)
+ * but has no jax.grad call site; this is the reverse sweep of qj_kdk_step.
+ * qj_kdk_forward_ckpt: advances psi by nsteps in chunks of K steps (one
+ * qj_kdk_step call each) and copies psi at the start of chunk j into
+ * ckpt + j (ckpt: ceil(nsteps / K) complex [nx][ny][nz] arrays).
+ * qj_kdk_adjoint: g holds dL/dRe psi_T + i dL/dIm psi_T on entry and
+ * dL/dRe psi_0 + i dL/dIm psi_0 on return; it recomputes each chunk from its
+ * checkpoint and runs the adjoint kicks (two Poisson solves each) and drifts
+ * backwards. */
+int qj_kdk_forward_ckpt(qj_plan *plan, void *psi, int nsteps, int K, void *ckpt,
+                        double dt, int self_interaction, const void *v_ext,
+                        void *stream);
+int qj_kdk_adjoint(qj_plan *plan, const void *ckpt, void *g, int nsteps, int K,
+                   double dt, int self_interaction, const void *v_ext,
+                   void *stream);
+
 /* nsteps x compute_step(psi, a) of the comoving script, quantum-cosmo.py:169-196:
  * per step dt = compute_dt(a, da) (:149-162, evaluated in float64 on the
  * host), kin_fac and pot_fac (:173-174) scale the drift and kick phases;
@@ -162,6 +187,22 @@ int qj_fft3d(qj_plan *plan, const void *in, void *out, int direction,
 int qj_get_potential_f32_noalloc(const qj_grid *grid, const qj_phys *phys,
                                  const float *rho, float *V,
                                  int self_interaction, void *stream);
+
+/* Ensembles of uneven boxes (no reference counterpart: the reference runs one
+ * box per process).  One batched plan per box size; qj_ensemble_step advances
+ * every plan's boxes by nsteps, each plan on its own stream, joined on
+ * `stream`.  With use_graph, the `chunk`-step body is captured once into a
+ * CUDA graph (recaptured when pointers or sizes change) and replayed
+ * nsteps / chunk times; a remainder runs directly.  Arrays are indexed by
+ * plan: psi[i], pos[i], vel[i] (device), n_s[i], m_s[i], dt[i] (host),
+ * diag[i] (device, nbox records). */
+typedef struct qj_ensemble qj_ensemble;
+int qj_ensemble_create(qj_ensemble **ens, qj_plan *const *plans, int nplans);
+int qj_ensemble_destroy(qj_ensemble *ens);
+int qj_ensemble_step(qj_ensemble *ens, void *const *psi, void *const *pos,
+                     void *const *vel, const int *n_s, const double *m_s,
+                     const double *dt, qj_diag *const *diag, int nsteps,
+                     int chunk, int use_graph, void *stream);
 
 /* Bytes of device workspace the plan holds. */
 int64_t qj_plan_workspace_bytes(const qj_plan *plan);

@@ -106,6 +106,9 @@ struct qj_plan {
   int prec;
   bool dbl;
   int max_particles;
+  int nbox = 1;  // boxes of a batched plan (fused single precision only)
+  int part_stride = 0, bstart_stride = 0;
+  int cur_stars = 0;  // stars per box of the running step
   int n[3];
   long long ncell;
   size_t rsz, csz;  // bytes of one real / complex element
@@ -141,6 +144,9 @@ struct qj_plan {
   void *tmp_scalar = nullptr;
   void *tmp_diag = nullptr;
   void *gas_out[4] = {nullptr, nullptr, nullptr, nullptr};  // hydro output scratch
+  // adjoint: recomputed chunk states
+  void *adj_psi = nullptr, *adj_states = nullptr;
+  int adj_cap = 0;
 };
 
 namespace {
@@ -248,6 +254,11 @@ FusedArgs fused_args(const qj_plan *P, int axis) {
   a.rho_bar = P->ph.rho_bar;
   a.inv_ncell = 1.0 / (double)P->ncell;
   a.amax_bits = (unsigned *)P->amax;
+  a.nbox = P->nbox;
+  a.box_cells = P->ncell;
+  a.box_stars = P->cur_stars;
+  a.box_bstart = P->bstart_stride;
+  a.box_part = P->part_stride;
   return a;
 }
 
@@ -301,17 +312,19 @@ struct StepCoefs {
 
 int fused_kdk(qj_plan *P, float2 *psi, float *pos, float *vel, int n_s, double m_s, double dt,
               int nsteps, int si, const float *vext, double *diag, cudaStream_t st,
-              const StepCoefs *sc = nullptr) {
+              const StepCoefs *sc = nullptr, void *save = nullptr) {
   const bool parts = n_s > 0;
+  const int nb = P->nbox;  // boxes: fields [nb][nx][ny][nz], stars [nb][n_s][3]
+  P->cur_stars = n_s;
   auto half = [&](int n) { return sc ? sc->kick_half[n] : P->ph.m_per_hbar * dt / 2.0; };
   auto drift_dt = [&](int n) { return sc ? sc->drift[n] : dt; };
-  QJ_TRY(launch_diag_load(false, diag, P->amax, st));
-  if (parts) QJ_TRY(launch_set_scalar(false, P->dts, INFINITY, st));
+  QJ_TRY(launch_diag_load(false, diag, P->amax, st, nb));
+  if (parts) QJ_TRY(launch_set_scalar(false, P->dts, INFINITY, st, nb));
   int q = 2;
   if (parts) {
     if (prof_on()) prof_mark_begin(st);
-    QJ_TRY(launch_stars_prepare(pos, n_s, nullptr, m_s, geom(P), q, P->sb, st));
-    QJ_TRY(launch_bucket_sort(n_s, n_pencils(P, q), P->sb, st));
+    QJ_TRY(launch_stars_prepare(pos, n_s * nb, nullptr, m_s, geom(P), q, P->sb, st));
+    QJ_TRY(launch_bucket_sort(n_s, n_pencils(P, q), P->sb, st, nb, P->bstart_stride));
     if (prof_on()) prof_mark_end(7, st);
   }
   {
@@ -358,7 +371,8 @@ int fused_kdk(qj_plan *P, float2 *psi, float *pos, float *vel, int n_s, double m
       if (prof_on()) prof_mark_begin(pst);
       UpdateArgs u;
       std::memset(&u, 0, sizeof(u));
-      u.n = n_s;
+      u.n = n_s * nb;
+      u.box_stars = n_s;
       u.dt = dt;
       u.k2 = k > 0;
       u.k1 = !last;
@@ -367,7 +381,8 @@ int fused_kdk(qj_plan *P, float2 *psi, float *pos, float *vel, int n_s, double m
       u.q_next = last ? -1 : r;
       u.m_s = m_s;
       QJ_TRY(launch_update_fused(pos, vel, geom(P), u, P->sb, pst));
-      if (!last) QJ_TRY(launch_bucket_sort(n_s, n_pencils(P, r), P->sb, pst));
+      if (!last)
+        QJ_TRY(launch_bucket_sort(n_s, n_pencils(P, r), P->sb, pst, nb, P->bstart_stride));
       if (prof_on()) prof_mark_end(8, pst);
       QJ_CK(cudaEventRecord(P->ev_parts, pst));
     }
@@ -386,11 +401,14 @@ int fused_kdk(qj_plan *P, float2 *psi, float *pos, float *vel, int n_s, double m
         }
         QJ_TRY(launch_fused(M_DRIFT_DENSITY, P->n[r], a, st));
       }
+      if (save)  // the state after drift k (before kick k + 1), for the adjoint
+        QJ_CK(cudaMemcpyAsync((char *)save + (size_t)k * P->ncell * P->csz, psi,
+                              P->ncell * P->csz, cudaMemcpyDeviceToDevice, st));
     }
     q = r;
   }
   if (parts) QJ_CK(cudaStreamWaitEvent(st, P->ev_parts, 0));
-  return launch_diag_store(false, diag, P->amax, P->dts, parts ? 1 : 0, nsteps * dt, st);
+  return launch_diag_store(false, diag, P->amax, P->dts, parts ? 1 : 0, nsteps * dt, st, nb);
 }
 
 // ---------------------------------------------------------------------------
@@ -434,7 +452,7 @@ int plain_bin(qj_plan *P, const void *pos, int n, double m_s, const void *masses
 
 int plain_kdk(qj_plan *P, void *psi, void *pos, void *vel, int n_s, double m_s, double dt,
               int nsteps, int si, const void *vext, double *diag, cudaStream_t st,
-              const StepCoefs *sc = nullptr) {
+              const StepCoefs *sc = nullptr, void *save = nullptr) {
   QJ_TRY(ensure_plain_ws(P));
   QJ_TRY(launch_diag_load(P->dbl, diag, P->amax, st));
   for (int step = 0; step < nsteps; ++step) {
@@ -464,10 +482,77 @@ int plain_kdk(qj_plan *P, void *psi, void *pos, void *vel, int n_s, double m_s, 
         QJ_TRY(fft3d(P, psi, -1, st));
         QJ_TRY(launch_drift_mul(P->dbl, psi, ktabs(P), dtk, P->ph.m_per_hbar, P->ncell, st));
         QJ_TRY(fft3d(P, psi, +1, st));
+        if (save)
+          QJ_CK(cudaMemcpyAsync((char *)save + (size_t)step * P->ncell * P->csz, psi,
+                                P->ncell * P->csz, cudaMemcpyDeviceToDevice, st));
       }
     }
   }
   return launch_diag_store(P->dbl, diag, P->amax, P->dts, n_s > 0 ? 1 : 0, nsteps * dt, st);
+}
+
+// ---------------------------------------------------------------------------
+// Adjoint of the psi-only KDK step (no particles).  A run of nsteps is split
+// into chunks of K steps; each chunk is one qj_kdk_step call, i.e. kicks
+// [c/2, c, ..., c, c/2] (c = m_per_hbar dt) around K drifts.  Each kick is
+// psi' = exp(-i c_j V[|psi|^2]) psi with V = (L + b) |psi|^2 + V_ext and L the
+// Poisson operator (real, symmetric).  With the gradient g = dL/dRe + i dL/dIm,
+// its adjoint is
+//     g <- exp(+i c_j V) g + 2 [(L + b) mu] psi,   mu = c_j Im(conj(g) psi'),
+// one Poisson solve for V and one for (L + b) mu.  A drift's adjoint is the
+// drift with -dt.  psi is checkpointed at chunk starts; the reverse sweep
+// recomputes each chunk forward, saving the state before every kick.
+// ---------------------------------------------------------------------------
+int kdk_chunk(qj_plan *P, void *psi, int m, double dt, int si, const void *vext, cudaStream_t st,
+              void *save) {
+  if (!P->tmp_diag) QJ_TRY(dev_alloc(P, &P->tmp_diag, 3 * sizeof(double)));
+  QJ_CK(cudaMemsetAsync(P->tmp_diag, 0, 3 * sizeof(double), st));
+  if (P->dbl)
+    return plain_kdk(P, psi, nullptr, nullptr, 0, 0.0, dt, m, si, vext, (double *)P->tmp_diag, st,
+                     nullptr, save);
+  return fused_kdk(P, (float2 *)psi, nullptr, nullptr, 0, 0.0, dt, m, si, (const float *)vext,
+                   (double *)P->tmp_diag, st, nullptr, save);
+}
+
+int adjoint_sweep(qj_plan *P, const void *ckpt, void *g, int nsteps, int K, double dt, int si,
+                  const void *vext, cudaStream_t st) {
+  QJ_TRY(ensure_plain_ws(P));
+  const size_t fb = P->ncell * P->csz;
+  if (!P->adj_psi) QJ_TRY(dev_alloc(P, &P->adj_psi, fb));
+  if (P->adj_cap < K) {
+    QJ_TRY(dev_alloc(P, &P->adj_states, (size_t)K * fb));
+    P->adj_cap = K;
+  }
+  const int nseg = (nsteps + K - 1) / K;
+  const double half = P->ph.m_per_hbar * dt / 2.0;
+  void *mu = P->ax, *W = P->ay;
+  for (int seg = nseg - 1; seg >= 0; --seg) {
+    const int m = std::min(K, nsteps - seg * K);
+    const void *c0 = (const char *)ckpt + (size_t)seg * fb;
+    QJ_CK(cudaMemcpyAsync(P->adj_psi, c0, fb, cudaMemcpyDeviceToDevice, st));
+    QJ_TRY(kdk_chunk(P, P->adj_psi, m, dt, si, vext, st, P->adj_states));
+    for (int j = m; j >= 0; --j) {
+      const void *pre = j == 0 ? c0 : (const char *)P->adj_states + (size_t)(j - 1) * fb;
+      const double coef = half * ((j == 0 || j == m) ? 1.0 : 2.0);
+      QJ_TRY(plain_potential(P, pre, nullptr, nullptr, P->V, si, vext, st));
+      QJ_TRY(launch_adj_mu(P->dbl, g, pre, P->V, coef, mu, P->ncell, st));
+      // W = (L + b) mu: the Poisson operator without the rho_bar shift
+      QJ_TRY(launch_build_rho(P->dbl, nullptr, nullptr, nullptr, mu, 4.0 * M_PI * P->ph.G, 0.0,
+                              nullptr, P->c0, P->ncell, st));
+      QJ_TRY(fft3d(P, P->c0, -1, st));
+      QJ_TRY(launch_poisson_div(P->dbl, P->c0, ktabs(P), P->ncell, st));
+      QJ_TRY(fft3d(P, P->c0, +1, st));
+      QJ_TRY(launch_real_part(P->dbl, P->c0, 1.0, si ? mu : nullptr, P->ph.b_coeff, nullptr, W,
+                              P->ncell, st));
+      QJ_TRY(launch_adj_update(P->dbl, g, pre, P->V, W, coef, P->ncell, st));
+      if (j > 0) {  // adjoint of drift j - 1
+        QJ_TRY(fft3d(P, g, -1, st));
+        QJ_TRY(launch_drift_mul(P->dbl, g, ktabs(P), -dt, P->ph.m_per_hbar, P->ncell, st));
+        QJ_TRY(fft3d(P, g, +1, st));
+      }
+    }
+  }
+  return 0;
 }
 
 
@@ -648,13 +733,31 @@ extern "C" {
 
 const char *qj_last_error(void) { return g_err.c_str(); }
 
+// Entry points other than qj_kdk_step work on single-box plans.
+#define QJ_ONE_BOX(P, name)                                                     \
+  do {                                                                          \
+    if ((P) && (P)->nbox != 1) {                                                \
+      set_error("%s: batched plans (nbox > 1) support qj_kdk_step only", name); \
+      return QJ_ERR_ARG;                                                        \
+    }                                                                           \
+  } while (0)
+
 int qj_plan_create(qj_plan **plan, const qj_grid *grid, const qj_phys *phys, int precision,
                    int max_particles) {
+  return qj_plan_create_batched(plan, grid, phys, precision, max_particles, 1);
+}
+
+int qj_plan_create_batched(qj_plan **plan, const qj_grid *grid, const qj_phys *phys, int precision,
+                           int max_particles, int nbox) {
   if (!plan || !grid || !phys) {
     set_error("qj_plan_create: null argument");
     return QJ_ERR_ARG;
   }
   *plan = nullptr;
+  if (nbox < 1 || nbox > 65535 || (nbox > 1 && precision != QJ_FUSED_F32)) {
+    set_error("qj_plan_create_batched: nbox must be in [1, 65535], batches need QJ_FUSED_F32");
+    return QJ_ERR_ARG;
+  }
   if (precision != QJ_PLAIN_F64 && precision != QJ_FUSED_F32) {
     set_error("qj_plan_create: precision must be QJ_PLAIN_F64 or QJ_FUSED_F32");
     return QJ_ERR_ARG;
@@ -662,7 +765,8 @@ int qj_plan_create(qj_plan **plan, const qj_grid *grid, const qj_phys *phys, int
   const int n[3] = {grid->nx, grid->ny, grid->nz};
   for (int a = 0; a < 3; ++a) {
     if (!fft_length_supported(n[a])) {
-      set_error("qj_plan_create: axis %d length %d unsupported (16, 32, 64, 128, 256, 512)", a, n[a]);
+      set_error("qj_plan_create: axis %d length %d unsupported (16, 32, 64, 96, 128, 256, 512)", a,
+                n[a]);
       return QJ_ERR_ARG;
     }
   }
@@ -743,13 +847,15 @@ int qj_plan_create(qj_plan **plan, const qj_grid *grid, const qj_phys *phys, int
     if (e != cudaSuccess) rc = cuda_fail(e, "cudaMemcpy(twiddles)", __FILE__, __LINE__);
   }
   if (rc) return fail(rc);
+  P->nbox = nbox;
   if (!P->dbl) {
-    if ((rc = dev_alloc_t(P, &P->R, P->ncell))) return fail(rc);
-    if ((rc = dev_alloc_t(P, &P->S1, P->ncell))) return fail(rc);
-    if ((rc = dev_alloc_t(P, &P->S2, P->ncell))) return fail(rc);
+    if ((rc = dev_alloc_t(P, &P->R, P->ncell * nbox))) return fail(rc);
+    if ((rc = dev_alloc_t(P, &P->S1, P->ncell * nbox))) return fail(rc);
+    if ((rc = dev_alloc_t(P, &P->S2, P->ncell * nbox))) return fail(rc);
     int nb = 0;
     for (int a = 0; a < 3; ++a) nb = std::max(nb, pass_blocks(n[a], a, n[0], n[1], n[2]));
-    if ((rc = dev_alloc_t(P, &P->part, nb))) return fail(rc);
+    P->part_stride = nb;
+    if ((rc = dev_alloc_t(P, &P->part, (size_t)nb * nbox))) return fail(rc);
   } else {
     if ((rc = ensure_plain_ws(P))) return fail(rc);
   }
@@ -758,12 +864,13 @@ int qj_plan_create(qj_plan **plan, const qj_grid *grid, const qj_phys *phys, int
     if ((rc = dev_alloc_t(P, b, np8))) return fail(rc);
   if ((rc = dev_alloc(P, &P->vals, np8 * P->rsz))) return fail(rc);
   if ((rc = dev_alloc(P, &P->uval, np8 * P->rsz))) return fail(rc);
-  if ((rc = dev_alloc(P, &P->A, 3 * np8 * P->rsz))) return fail(rc);
+  if ((rc = dev_alloc(P, &P->A, 3 * np8 * P->rsz * nbox))) return fail(rc);
   if ((rc = dev_alloc(P, &P->acc, 3 * (np8 / 8) * P->rsz))) return fail(rc);
   long long npen = 0;
   for (int a = 0; a < 3; ++a) npen = std::max(npen, P->ncell / n[a]);
+  P->bstart_stride = (int)(npen + 1);
   if (!P->dbl) {
-    const size_t np = (size_t)std::max(1, max_particles);
+    const size_t np = (size_t)std::max(1, max_particles) * nbox;
     StarBufs &b = P->sb;
     if ((rc = dev_alloc_t(P, &b.sidx, np))) return fail(rc);
     if ((rc = dev_alloc_t(P, &b.sw0, np))) return fail(rc);
@@ -772,7 +879,7 @@ int qj_plan_create(qj_plan **plan, const qj_grid *grid, const qj_phys *phys, int
     if ((rc = dev_alloc_t(P, &b.perm, np))) return fail(rc);
     if ((rc = dev_alloc_t(P, &b.skey, np))) return fail(rc);
     if ((rc = dev_alloc_t(P, &b.sortbuf, 4 * np))) return fail(rc);
-    if ((rc = dev_alloc_t(P, &b.bstart, npen + 1))) return fail(rc);
+    if ((rc = dev_alloc_t(P, &b.bstart, (size_t)(npen + 1) * nbox))) return fail(rc);
     b.A = (float *)P->A;
     int lo = 0, hi = 0;
     cudaError_t e0 = cudaDeviceGetStreamPriorityRange(&lo, &hi);
@@ -783,8 +890,8 @@ int qj_plan_create(qj_plan **plan, const qj_grid *grid, const qj_phys *phys, int
   }
   if ((rc = dev_alloc_t(P, &P->pstart, npen + 1))) return fail(rc);
   if ((rc = dev_alloc_t(P, &P->n_unique, 1))) return fail(rc);
-  if ((rc = dev_alloc(P, &P->amax, 8))) return fail(rc);
-  if ((rc = dev_alloc(P, &P->dts, 8))) return fail(rc);
+  if ((rc = dev_alloc(P, &P->amax, 8 * (size_t)nbox))) return fail(rc);
+  if ((rc = dev_alloc(P, &P->dts, 8 * (size_t)nbox))) return fail(rc);
   if ((rc = dev_alloc(P, &P->tmp_scalar, 8))) return fail(rc);
   cudaError_t e = cudaDeviceSynchronize();
   if (e != cudaSuccess) return fail(cuda_fail(e, "plan init", __FILE__, __LINE__));
@@ -853,6 +960,7 @@ int qj_profile_read(double *ms, int64_t *count, int nbuckets) {
 }
 
 int qj_fft3d(qj_plan *P, const void *in, void *out, int direction, void *stream) {
+  QJ_ONE_BOX(P, "qj_fft3d");
   if (!P || !in || !out || (direction != -1 && direction != 1)) {
     set_error("qj_fft3d: bad argument");
     return QJ_ERR_ARG;
@@ -863,6 +971,7 @@ int qj_fft3d(qj_plan *P, const void *in, void *out, int direction, void *stream)
 }
 
 int qj_get_potential(qj_plan *P, const void *rho, void *V, int self_interaction, void *stream) {
+  QJ_ONE_BOX(P, "qj_get_potential");
   if (!P || !rho || !V) {
     set_error("qj_get_potential: null argument");
     return QJ_ERR_ARG;
@@ -874,6 +983,7 @@ int qj_get_potential(qj_plan *P, const void *rho, void *V, int self_interaction,
 
 int qj_bin_stars(qj_plan *P, const void *pos, int n, double m_s, const void *masses, void *rho_s,
                  void *stream) {
+  QJ_ONE_BOX(P, "qj_bin_stars");
   if (!P || !rho_s || (n > 0 && !pos) || n < 0 || n > P->max_particles) {
     set_error("qj_bin_stars: bad argument (n=%d, max_particles=%d)", n, P ? P->max_particles : 0);
     return QJ_ERR_ARG;
@@ -893,6 +1003,7 @@ int qj_bin_stars(qj_plan *P, const void *pos, int n, double m_s, const void *mas
 
 int qj_get_acceleration(qj_plan *P, const void *pos, int n, const void *rho, void *acc,
                         double *a_max, void *stream) {
+  QJ_ONE_BOX(P, "qj_get_acceleration");
   if (!P || !rho || (n > 0 && (!pos || !acc)) || n < 0 || n > P->max_particles) {
     set_error("qj_get_acceleration: bad argument (n=%d, max_particles=%d)", n,
               P ? P->max_particles : 0);
@@ -926,6 +1037,7 @@ static double cosmo_dt(double a, double da, double H0, double om, double ol) {
 
 int qj_kdk_cosmo(qj_plan *P, void *psi, double *a_io, double da, double H0, double omega_m,
                  double omega_l, int nsteps, void *stream) {
+  QJ_ONE_BOX(P, "qj_kdk_cosmo");
   if (!P || !psi || !a_io || nsteps < 0 || !(da > 0) || !(*a_io > 0)) {
     set_error("qj_kdk_cosmo: bad argument");
     return QJ_ERR_ARG;
@@ -955,6 +1067,7 @@ int qj_kdk_cosmo(qj_plan *P, void *psi, double *a_io, double da, double H0, doub
 int qj_kdk_gas_bh_step(qj_plan *P, void *psi, void *rho, void *vx, void *vy, void *vz, void *m_bh,
                        void *pos, void *vel, int n_bh, double dt, int nsteps, double sigma_v,
                        int dm_accretion, double bondi_r_acc_mult, double *t_io, void *stream) {
+  QJ_ONE_BOX(P, "qj_kdk_gas_bh_step");
   if (!P || !psi || nsteps < 0 || n_bh < 0 || (n_bh > 0 && (!m_bh || !pos || !vel)) ||
       (rho && (!vx || !vy || !vz)) || !(dt > 0)) {
     set_error("qj_kdk_gas_bh_step: bad argument");
@@ -991,6 +1104,32 @@ int qj_kdk_gas_bh_step(qj_plan *P, void *psi, void *rho, void *vx, void *vy, voi
   return QJ_OK;
 }
 
+int qj_kdk_forward_ckpt(qj_plan *P, void *psi, int nsteps, int K, void *ckpt, double dt,
+                        int self_interaction, const void *v_ext, void *stream) {
+  QJ_ONE_BOX(P, "qj_kdk_forward_ckpt");
+  if (!P || !psi || !ckpt || nsteps <= 0 || K <= 0 || !(dt > 0)) {
+    set_error("qj_kdk_forward_ckpt: bad argument");
+    return QJ_ERR_ARG;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t fb = P->ncell * P->csz;
+  for (int s0 = 0, seg = 0; s0 < nsteps; s0 += K, ++seg) {
+    QJ_CK(cudaMemcpyAsync((char *)ckpt + (size_t)seg * fb, psi, fb, cudaMemcpyDeviceToDevice, st));
+    QJ_TRY(kdk_chunk(P, psi, std::min(K, nsteps - s0), dt, self_interaction, v_ext, st, nullptr));
+  }
+  return QJ_OK;
+}
+
+int qj_kdk_adjoint(qj_plan *P, const void *ckpt, void *g, int nsteps, int K, double dt,
+                   int self_interaction, const void *v_ext, void *stream) {
+  QJ_ONE_BOX(P, "qj_kdk_adjoint");
+  if (!P || !ckpt || !g || nsteps <= 0 || K <= 0 || !(dt > 0)) {
+    set_error("qj_kdk_adjoint: bad argument");
+    return QJ_ERR_ARG;
+  }
+  return adjoint_sweep(P, ckpt, g, nsteps, K, dt, self_interaction, v_ext, (cudaStream_t)stream);
+}
+
 int qj_kdk_step(qj_plan *P, void *psi, void *pos, void *vel, int n_s, double m_s, double dt,
                 int nsteps, int self_interaction, const void *v_ext, qj_diag *diag,
                 void *stream) {
@@ -1013,6 +1152,167 @@ int qj_kdk_step(qj_plan *P, void *psi, void *pos, void *vel, int n_s, double m_s
                      (double *)diag, st);
   return fused_kdk(P, (float2 *)psi, (float *)pos, (float *)vel, n_s, m_s, dt, nsteps,
                    self_interaction, (const float *)v_ext, (double *)diag, st);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Ensembles: several batched plans (one per box size) stepped concurrently,
+// one stream each, with the fork/join step body captured once into a CUDA
+// graph and replayed.
+// ---------------------------------------------------------------------------
+struct qj_ensemble {
+  std::vector<qj_plan *> plans;
+  std::vector<cudaStream_t> streams;
+  cudaStream_t origin = nullptr;
+  cudaEvent_t fork = nullptr, done = nullptr, caller = nullptr;
+  std::vector<cudaEvent_t> joins;
+  cudaGraphExec_t exec = nullptr;
+  std::vector<const void *> key;  // pointers and sizes the graph was captured with
+};
+
+namespace {
+
+struct EnsArgs {
+  void *const *psi;
+  void *const *pos;
+  void *const *vel;
+  const int *n_s;
+  const double *m_s;
+  const double *dt;
+  qj_diag *const *diag;
+};
+
+int ensemble_body(qj_ensemble *E, const EnsArgs &a, int m) {
+  QJ_CK(cudaEventRecord(E->fork, E->origin));
+  for (size_t i = 0; i < E->plans.size(); ++i) {
+    QJ_CK(cudaStreamWaitEvent(E->streams[i], E->fork, 0));
+    QJ_TRY(fused_kdk(E->plans[i], (float2 *)a.psi[i], (float *)a.pos[i], (float *)a.vel[i],
+                     a.n_s[i], a.m_s[i], a.dt[i], m, 0, nullptr, (double *)a.diag[i],
+                     E->streams[i]));
+    QJ_CK(cudaEventRecord(E->joins[i], E->streams[i]));
+    QJ_CK(cudaStreamWaitEvent(E->origin, E->joins[i], 0));
+  }
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int qj_ensemble_create(qj_ensemble **ens, qj_plan *const *plans, int nplans) {
+  if (!ens || !plans || nplans <= 0) {
+    set_error("qj_ensemble_create: bad argument");
+    return QJ_ERR_ARG;
+  }
+  *ens = nullptr;
+  for (int i = 0; i < nplans; ++i) {
+    if (!plans[i] || plans[i]->dbl) {
+      set_error("qj_ensemble_create: plan %d is null or not QJ_FUSED_F32", i);
+      return QJ_ERR_ARG;
+    }
+  }
+  qj_ensemble *E = new qj_ensemble();
+  E->plans.assign(plans, plans + nplans);
+  cudaError_t e = cudaStreamCreateWithFlags(&E->origin, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&E->fork, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&E->done, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&E->caller, cudaEventDisableTiming);
+  for (int i = 0; i < nplans && e == cudaSuccess; ++i) {
+    cudaStream_t s = nullptr;
+    cudaEvent_t j = nullptr;
+    e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&j, cudaEventDisableTiming);
+    E->streams.push_back(s);
+    E->joins.push_back(j);
+  }
+  if (e != cudaSuccess) {
+    qj_ensemble_destroy(E);
+    return cuda_fail(e, "qj_ensemble_create", __FILE__, __LINE__);
+  }
+  *ens = E;
+  return QJ_OK;
+}
+
+int qj_ensemble_destroy(qj_ensemble *E) {
+  if (!E) return QJ_OK;
+  if (E->origin) cudaStreamSynchronize(E->origin);
+  if (E->exec) cudaGraphExecDestroy(E->exec);
+  for (cudaStream_t s : E->streams)
+    if (s) cudaStreamDestroy(s);
+  for (cudaEvent_t j : E->joins)
+    if (j) cudaEventDestroy(j);
+  if (E->fork) cudaEventDestroy(E->fork);
+  if (E->done) cudaEventDestroy(E->done);
+  if (E->caller) cudaEventDestroy(E->caller);
+  if (E->origin) cudaStreamDestroy(E->origin);
+  delete E;
+  return QJ_OK;
+}
+
+int qj_ensemble_step(qj_ensemble *E, void *const *psi, void *const *pos, void *const *vel,
+                     const int *n_s, const double *m_s, const double *dt, qj_diag *const *diag,
+                     int nsteps, int chunk, int use_graph, void *stream) {
+  if (!E || !psi || !n_s || !m_s || !dt || !diag || nsteps < 0 || chunk <= 0) {
+    set_error("qj_ensemble_step: bad argument");
+    return QJ_ERR_ARG;
+  }
+  const size_t np = E->plans.size();
+  for (size_t i = 0; i < np; ++i) {
+    if (!psi[i] || !diag[i] || n_s[i] < 0 || n_s[i] > E->plans[i]->max_particles ||
+        (n_s[i] > 0 && (!pos || !vel || !pos[i] || !vel[i])) || !(dt[i] > 0)) {
+      set_error("qj_ensemble_step: bad arguments for plan %d", (int)i);
+      return QJ_ERR_ARG;
+    }
+  }
+  if (nsteps == 0) return QJ_OK;
+  EnsArgs a{psi, pos, vel, n_s, m_s, dt, diag};
+  cudaStream_t st = (cudaStream_t)stream;
+  QJ_CK(cudaEventRecord(E->caller, st));
+  QJ_CK(cudaStreamWaitEvent(E->origin, E->caller, 0));
+  const int full = nsteps / chunk, rem = nsteps % chunk;
+  if (use_graph && full > 0) {
+    std::vector<const void *> key;
+    for (size_t i = 0; i < np; ++i) {
+      key.push_back(psi[i]);
+      key.push_back(n_s[i] ? pos[i] : nullptr);
+      key.push_back(n_s[i] ? vel[i] : nullptr);
+      key.push_back(diag[i]);
+      key.push_back((const void *)(intptr_t)n_s[i]);
+      key.push_back((const void *)(intptr_t)chunk);
+      long long mb, db;
+      std::memcpy(&mb, &m_s[i], 8);
+      std::memcpy(&db, &dt[i], 8);
+      key.push_back((const void *)(intptr_t)mb);
+      key.push_back((const void *)(intptr_t)db);
+    }
+    if (!E->exec || key != E->key) {
+      if (E->exec) {
+        QJ_CK(cudaGraphExecDestroy(E->exec));
+        E->exec = nullptr;
+      }
+      cudaGraph_t g = nullptr;
+      QJ_CK(cudaStreamBeginCapture(E->origin, cudaStreamCaptureModeThreadLocal));
+      const int rc = ensemble_body(E, a, chunk);
+      cudaError_t ce = cudaStreamEndCapture(E->origin, &g);
+      if (rc) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+      }
+      QJ_CK(ce);
+      ce = cudaGraphInstantiate(&E->exec, g, 0);
+      cudaGraphDestroy(g);
+      QJ_CK(ce);
+      E->key = key;
+    }
+    for (int c = 0; c < full; ++c) QJ_CK(cudaGraphLaunch(E->exec, E->origin));
+  } else {
+    for (int c = 0; c < full; ++c) QJ_TRY(ensemble_body(E, a, chunk));
+  }
+  if (rem) QJ_TRY(ensemble_body(E, a, rem));
+  QJ_CK(cudaEventRecord(E->done, E->origin));
+  QJ_CK(cudaStreamWaitEvent(st, E->done, 0));
+  return QJ_OK;
 }
 
 }  // extern "C"

@@ -122,6 +122,12 @@ template <> struct FftPlan<64> {
   static constexpr int E = 8, NS = 2;
   __host__ __device__ static constexpr int radix(int) { return 8; }
 };
+template <> struct FftPlan<96> {  // 96 = 4 * 4 * 2 * 3, 12 elements per thread
+  static constexpr int E = 12, NS = 4;
+  __host__ __device__ static constexpr int radix(int s) {
+    return s == 0 ? 4 : (s == 1 ? 4 : (s == 2 ? 2 : 3));
+  }
+};
 template <> struct FftPlan<128> {
   static constexpr int E = 16, NS = 2;
   __host__ __device__ static constexpr int radix(int s) { return s == 0 ? 16 : 8; }

@@ -32,6 +32,7 @@ static int dispatch(int n, const FftArgs &a, cudaStream_t st) {
     QJ_CASE(16)
     QJ_CASE(32)
     QJ_CASE(64)
+    QJ_CASE(96)
     QJ_CASE(128)
     QJ_CASE(256)
     QJ_CASE(512)

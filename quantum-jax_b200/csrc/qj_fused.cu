@@ -9,7 +9,7 @@
 namespace qj {
 
 bool fft_length_supported(int n) {
-  return n == 16 || n == 32 || n == 64 || n == 128 || n == 256 || n == 512;
+  return n == 16 || n == 32 || n == 64 || n == 96 || n == 128 || n == 256 || n == 512;
 }
 
 template <int N, bool CONTIG>
@@ -39,6 +39,7 @@ std::vector<float2> stage_twiddles(int n) {
     case 16: return stage_table<16>();
     case 32: return stage_table<32>();
     case 64: return stage_table<64>();
+    case 96: return stage_table<96>();
     case 128: return stage_table<128>();
     case 256: return stage_table<256>();
     case 512: return stage_table<512>();
@@ -48,7 +49,7 @@ std::vector<float2> stage_twiddles(int n) {
 
 int pass_blocks(int n_axis, int axis, int nx, int ny, int nz) {
   if (axis == 2) {
-    const int E = (n_axis == 32 || n_axis == 64) ? 8 : 16;
+    const int E = (n_axis == 32 || n_axis == 64) ? 8 : (n_axis == 96 ? 12 : 16);
     const int P = n_axis / E;
     const int TP = P >= 256 ? 1 : 256 / P;
     return (nx * ny) / TP;
@@ -81,7 +82,8 @@ static int run_fused(const FusedArgs &a, cudaStream_t st) {
   }
   FusedArgs b = a;
   b.ahead = ahead;
-  k_fused<N, CONTIG, MODE><<<grid_of<N, CONTIG>(a), SH::THREADS, smem, st>>>(b);
+  const dim3 grid(grid_of<N, CONTIG>(a), a.nbox > 1 ? a.nbox : 1);
+  k_fused<N, CONTIG, MODE><<<grid, SH::THREADS, smem, st>>>(b);
   QJ_CK_LAUNCH();
   return 0;
 }
@@ -104,6 +106,7 @@ static int dispatch_mode(int n, const FusedArgs &a, cudaStream_t st) {
     QJ_CASE(16)
     QJ_CASE(32)
     QJ_CASE(64)
+    QJ_CASE(96)
     QJ_CASE(128)
     QJ_CASE(256)
     QJ_CASE(512)
@@ -123,6 +126,7 @@ static int dispatch_deposit(int n, const FusedArgs &a, cudaStream_t st) {
     case 16: return run_fused<16, true, M_DEPOSIT>(a, st);
     case 32: return run_fused<32, true, M_DEPOSIT>(a, st);
     case 64: return run_fused<64, true, M_DEPOSIT>(a, st);
+    case 96: return run_fused<96, true, M_DEPOSIT>(a, st);
     case 128: return run_fused<128, true, M_DEPOSIT>(a, st);
     case 256: return run_fused<256, true, M_DEPOSIT>(a, st);
     case 512: return run_fused<512, true, M_DEPOSIT>(a, st);

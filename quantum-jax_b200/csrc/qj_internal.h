@@ -91,6 +91,7 @@ struct UpdateArgs {
   void *vals;
   const void *masses;
   double m_s;
+  int box_stars;  // stars per box of a batched plan (0 = n)
 };
 int launch_particles_update(bool dbl, void *pos, void *vel, const void *acc, const CicGeomD &g,
                             const UpdateArgs &u, cudaStream_t st);
@@ -109,7 +110,10 @@ struct StarBufs {
 };
 int launch_stars_prepare(const void *pos, int n, const void *masses, double m_s,
                          const CicGeomD &g, int q, const StarBufs &b, cudaStream_t st);
-int launch_bucket_sort(int n, int n_buckets, const StarBufs &b, cudaStream_t st);
+// n stars per box, nbox boxes (one sort CTA each), bucket starts per box at
+// stride bstride.
+int launch_bucket_sort(int n, int n_buckets, const StarBufs &b, cudaStream_t st, int nbox = 1,
+                       int bstride = 0);
 int launch_update_fused(void *pos, void *vel, const CicGeomD &g, const UpdateArgs &u,
                         const StarBufs &b, cudaStream_t st);
 
@@ -135,6 +139,11 @@ int launch_amax3(bool dbl, const void *ax, const void *ay, const void *az, long 
 int launch_gas_kick(bool dbl, void *vx, void *vy, void *vz, const void *ax, const void *ay,
                     const void *az, double dt, long long ncell, cudaStream_t st);
 
+int launch_adj_mu(bool dbl, const void *g, const void *psi, const void *V, double coef, void *mu,
+                  long long ncell, cudaStream_t st);
+int launch_adj_update(bool dbl, void *g, const void *psi, const void *V, const void *W, double coef,
+                      long long ncell, cudaStream_t st);
+
 // ----- gas and black hole (qj_gas.cu) -----
 int launch_hydro(bool dbl, const void *rho, const void *vx, const void *vy, const void *vz,
                  void *orho, void *ovx, void *ovy, void *ovz, int n, double dx, double dt,
@@ -146,10 +155,11 @@ int launch_bondi(bool dbl, void *rho, const void *pos, void *m_bh, int n, double
                  double cs, double G, double dt, double r_acc_mult, cudaStream_t st);
 
 // ----- small scalar kernels (qj_particles.cu) -----
-int launch_diag_load(bool dbl, const void *diag, void *amax_bits, cudaStream_t st);
+// diag: nbox records (t, a_max, dt_s); amax / dts: nbox scalars
+int launch_diag_load(bool dbl, const void *diag, void *amax_bits, cudaStream_t st, int nbox = 1);
 int launch_diag_store(bool dbl, void *diag, const void *amax_bits, const void *dts_bits,
-                      int has_particles, double t_add, cudaStream_t st);
-int launch_set_scalar(bool dbl, void *dst, double v, cudaStream_t st);
+                      int has_particles, double t_add, cudaStream_t st, int nbox = 1);
+int launch_set_scalar(bool dbl, void *dst, double v, cudaStream_t st, int count = 1);
 int launch_bits_to_double(bool dbl, const void *bits, double *out, cudaStream_t st);
 
 }  // namespace qj

@@ -495,6 +495,13 @@ __global__ void __launch_bounds__(1024)
   __shared__ unsigned hist[32 * 256];
   __shared__ unsigned dbase[256];
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  {  // one CTA per box of a batched plan
+    const long long box = blockIdx.x;
+    bkey += box * n;
+    gbuf += box * 4 * n;
+    perm += box * n;
+    skey += box * n;
+  }
   unsigned *buf = use_smem ? dyn : gbuf;
   unsigned *kA = buf, *iA = buf + n, *kB = buf + 2 * n, *iB = buf + 3 * n;
   const int chunk = (n + 31) / 32;
@@ -575,9 +582,12 @@ __global__ void __launch_bounds__(1024)
 }
 
 // bstart[b] = first sorted position with bucket >= b, b = 0..n_buckets.
-__global__ void k_bucket_starts(const unsigned *skey, int n, int n_buckets, int *bstart) {
+__global__ void k_bucket_starts(const unsigned *skey, int n, int n_buckets, int *bstart,
+                                int bstride) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b > n_buckets) return;
+  skey += (long long)blockIdx.y * n;
+  bstart += (long long)blockIdx.y * bstride;
   int lo = 0, hi = n;
   while (lo < hi) {
     const int mid = (lo + hi) >> 1;
@@ -589,7 +599,8 @@ __global__ void k_bucket_starts(const unsigned *skey, int n, int n_buckets, int 
   bstart[b] = lo;
 }
 
-int launch_bucket_sort(int n, int n_buckets, const StarBufs &b, cudaStream_t st) {
+int launch_bucket_sort(int n, int n_buckets, const StarBufs &b, cudaStream_t st, int nbox,
+                       int bstride) {
   if (n <= 0) return 0;
   const unsigned nbits = cell_bits(n_buckets);
   const int use_smem = n <= kSortSmemMax;
@@ -601,11 +612,11 @@ int launch_bucket_sort(int n, int n_buckets, const StarBufs &b, cudaStream_t st)
                                     16 * kSortSmemMax);
   });
   QJ_CK(attr_err);
-  k_bucket_sort<<<1, 1024, smem, st>>>(b.bkey, n, nbits < 8 ? 8 : nbits, b.sortbuf, use_smem,
-                                       b.perm, b.skey);
+  k_bucket_sort<<<nbox, 1024, smem, st>>>(b.bkey, n, nbits < 8 ? 8 : nbits, b.sortbuf, use_smem,
+                                          b.perm, b.skey);
   QJ_CK_LAUNCH();
   const int T = 256, B = (n_buckets + 1 + T - 1) / T;
-  k_bucket_starts<<<B, T, 0, st>>>(b.skey, n, n_buckets, b.bstart);
+  k_bucket_starts<<<dim3(B, nbox), T, 0, st>>>(b.skey, n, n_buckets, b.bstart, bstride);
   QJ_CK_LAUNCH();
   return 0;
 }
@@ -617,9 +628,10 @@ int launch_bucket_sort(int n, int n_buckets, const StarBufs &b, cudaStream_t st)
 __global__ void k_update_fused(float *pos, float *vel, const float *A, int n, CicGeom<float> g,
                                float dt, int k2, int k1, int drift, float *dts, int q_next,
                                const float *masses, float fac_all, int4 *sidx, float4 *sw0,
-                               float4 *sw1, unsigned *bkey) {
+                               float4 *sw1, unsigned *bkey, int box_stars) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
+  dts += s / box_stars;  // dt_s of this star's box
   const float4 w0 = sw0[s], w1 = sw1[s];
   float a0 = 0.f, a1 = 0.f, a2 = 0.f;
 #pragma unroll
@@ -661,7 +673,8 @@ int launch_update_fused(void *pos, void *vel, const CicGeomD &g, const UpdateArg
   const double fac = u.m_s / (g.d[0] * g.d[1] * g.d[2]);
   k_update_fused<<<B, T, 0, st>>>((float *)pos, (float *)vel, b.A, u.n, cast_geom<float>(g),
                                   (float)u.dt, u.k2, u.k1, u.drift, (float *)u.dts_bits, u.q_next,
-                                  (const float *)u.masses, (float)fac, b.sidx, b.sw0, b.sw1, b.bkey);
+                                  (const float *)u.masses, (float)fac, b.sidx, b.sw0, b.sw1, b.bkey,
+                                  u.box_stars > 0 ? u.box_stars : u.n);
   QJ_CK_LAUNCH();
   return 0;
 }
@@ -669,43 +682,52 @@ int launch_update_fused(void *pos, void *vel, const CicGeomD &g, const UpdateArg
 // ----- scalar state kernels -----
 // amax / dt_s are kept as the real type's bit pattern (non-negative values,
 // ordered like unsigned integers) so atomicMax / atomicMin are exact.
-template <typename R> __global__ void k_diag_load(const double *diag, R *amax) {
-  *amax = (R)diag[1];
+template <typename R> __global__ void k_diag_load(const double *diag, R *amax, int nbox) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b < nbox) amax[b] = (R)diag[3 * b + 1];
 }
 template <typename R>
 __global__ void k_diag_store(double *diag, const R *amax, const R *dts, int has_particles,
-                             double t_add) {
-  diag[0] += t_add;
-  diag[1] = (double)*amax;
-  diag[2] = has_particles ? (double)*dts : (double)INFINITY;
+                             double t_add, int nbox) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nbox) return;
+  diag[3 * b + 0] += t_add;
+  diag[3 * b + 1] = (double)amax[b];
+  diag[3 * b + 2] = has_particles ? (double)dts[b] : (double)INFINITY;
 }
-template <typename R> __global__ void k_set_scalar(R *dst, double v) { *dst = (R)v; }
+template <typename R> __global__ void k_set_scalar(R *dst, double v, int count) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b < count) dst[b] = (R)v;
+}
 template <typename R> __global__ void k_to_double(const R *src, double *out) { *out = (double)*src; }
 
-int launch_diag_load(bool dbl, const void *diag, void *amax_bits, cudaStream_t st) {
+int launch_diag_load(bool dbl, const void *diag, void *amax_bits, cudaStream_t st, int nbox) {
+  const int B = (nbox + 127) / 128;
   if (dbl)
-    k_diag_load<double><<<1, 1, 0, st>>>((const double *)diag, (double *)amax_bits);
+    k_diag_load<double><<<B, 128, 0, st>>>((const double *)diag, (double *)amax_bits, nbox);
   else
-    k_diag_load<float><<<1, 1, 0, st>>>((const double *)diag, (float *)amax_bits);
+    k_diag_load<float><<<B, 128, 0, st>>>((const double *)diag, (float *)amax_bits, nbox);
   QJ_CK_LAUNCH();
   return 0;
 }
 int launch_diag_store(bool dbl, void *diag, const void *amax_bits, const void *dts_bits,
-                      int has_particles, double t_add, cudaStream_t st) {
+                      int has_particles, double t_add, cudaStream_t st, int nbox) {
+  const int B = (nbox + 127) / 128;
   if (dbl)
-    k_diag_store<double><<<1, 1, 0, st>>>((double *)diag, (const double *)amax_bits,
-                                          (const double *)dts_bits, has_particles, t_add);
+    k_diag_store<double><<<B, 128, 0, st>>>((double *)diag, (const double *)amax_bits,
+                                            (const double *)dts_bits, has_particles, t_add, nbox);
   else
-    k_diag_store<float><<<1, 1, 0, st>>>((double *)diag, (const float *)amax_bits,
-                                         (const float *)dts_bits, has_particles, t_add);
+    k_diag_store<float><<<B, 128, 0, st>>>((double *)diag, (const float *)amax_bits,
+                                           (const float *)dts_bits, has_particles, t_add, nbox);
   QJ_CK_LAUNCH();
   return 0;
 }
-int launch_set_scalar(bool dbl, void *dst, double v, cudaStream_t st) {
+int launch_set_scalar(bool dbl, void *dst, double v, cudaStream_t st, int count) {
+  const int B = (count + 127) / 128;
   if (dbl)
-    k_set_scalar<double><<<1, 1, 0, st>>>((double *)dst, v);
+    k_set_scalar<double><<<B, 128, 0, st>>>((double *)dst, v, count);
   else
-    k_set_scalar<float><<<1, 1, 0, st>>>((float *)dst, v);
+    k_set_scalar<float><<<B, 128, 0, st>>>((float *)dst, v, count);
   QJ_CK_LAUNCH();
   return 0;
 }

@@ -78,7 +78,35 @@ struct FusedArgs {
   // L2 prefetch distance in CTAs (0 = off): each CTA prefetches the input
   // tile of CTA blockIdx.x + ahead, one resident wave later
   int ahead;
+  // batched boxes (blockIdx.y = box): per-box strides of the fields (cells),
+  // stars, bucket starts, partial sums; a_max is per box
+  int nbox;  // launch grid.y (0 or 1 = one box)
+  long long box_cells;
+  int box_stars;
+  int box_bstart;
+  int box_part;
 };
+
+// Offset a pass' pointers to box blockIdx.y of a batched plan.
+__device__ __forceinline__ void select_box(FusedArgs &a) {
+  const int b = blockIdx.y;
+  if (b == 0) return;
+  const long long c = (long long)b * a.box_cells;
+  if (a.psi) a.psi += c;
+  if (a.R) a.R += c;
+  if (a.S1) a.S1 += c;
+  if (a.S2) a.S2 += c;
+  if (a.part) a.part += (long long)b * a.box_part;
+  if (a.part_in) a.part_in += (long long)b * a.box_part;
+  if (a.amax_bits) a.amax_bits += b;
+  const long long s = (long long)b * a.box_stars;
+  if (a.sidx) a.sidx += s;
+  if (a.sw0) a.sw0 += s;
+  if (a.sw1) a.sw1 += s;
+  if (a.perm) a.perm += s;
+  if (a.A) a.A += 24 * s;
+  if (a.bstart) a.bstart += (long long)b * a.box_bstart;
+}
 
 // Per-thread position of a pencil in the grid.
 struct PencilPos {
@@ -338,6 +366,7 @@ __device__ __forceinline__ void prefetch_tile(const float2 *f, const FusedArgs &
 template <int N, bool CONTIG, int MODE>
 __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CONTIG>::MINB)
     k_fused(FusedArgs a) {
+  select_box(a);
   if (a.ahead > 0 && (int)blockIdx.x + a.ahead < (int)gridDim.x) {
     const int nb = blockIdx.x + a.ahead;
     if constexpr (MODE == M_DENSITY || MODE == M_DRIFT || MODE == M_DRIFT_DENSITY) {

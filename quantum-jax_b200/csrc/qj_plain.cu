@@ -154,6 +154,70 @@ __global__ void k_gas_kick(R *vx, R *vy, R *vz, const R *ax, const R *ay, const 
   }
 }
 
+// ----- adjoint of the kick psi' = exp(-i c V[|psi|^2]) psi -----
+// (real adjoint with the gradient convention g = dL/dRe + i dL/dIm)
+template <typename R> __device__ __forceinline__ void phase_sc(double th, R &s, R &c) {
+  if constexpr (sizeof(R) == 8) {
+    sincos(th, &s, &c);
+  } else {
+    float sf, cf;
+    sincos_reduced(th, sf, cf);
+    s = sf;
+    c = cf;
+  }
+}
+
+// mu = c Im(conj(g) psi'), psi' = exp(-i c V) psi
+template <typename R>
+__global__ void k_adj_mu(const cplx<R> *g, const cplx<R> *psi, const R *V, double coef, R *mu,
+                         long long n) {
+  GRID_LOOP(i, n) {
+    R s, c;
+    phase_sc<R>(coef * (double)V[i], s, c);
+    const cplx<R> z = psi[i];
+    const cplx<R> zp = cplx<R>{z.x * c + z.y * s, z.y * c - z.x * s};
+    const cplx<R> w = g[i];
+    mu[i] = (R)coef * (w.x * zp.y - w.y * zp.x);
+  }
+}
+
+// g <- exp(+i c V) g + 2 W psi
+template <typename R>
+__global__ void k_adj_update(cplx<R> *g, const cplx<R> *psi, const R *V, const R *W, double coef,
+                             long long n) {
+  GRID_LOOP(i, n) {
+    R s, c;
+    phase_sc<R>(coef * (double)V[i], s, c);
+    const cplx<R> w = g[i];
+    const R two_w = (R)2 * W[i];
+    g[i] = cplx<R>{w.x * c - w.y * s + two_w * psi[i].x, w.y * c + w.x * s + two_w * psi[i].y};
+  }
+}
+
+int launch_adj_mu(bool dbl, const void *g, const void *psi, const void *V, double coef, void *mu,
+                  long long ncell, cudaStream_t st) {
+  if (dbl)
+    k_adj_mu<double><<<grid_blocks(ncell), 256, 0, st>>>((const double2 *)g, (const double2 *)psi,
+                                                         (const double *)V, coef, (double *)mu, ncell);
+  else
+    k_adj_mu<float><<<grid_blocks(ncell), 256, 0, st>>>((const float2 *)g, (const float2 *)psi,
+                                                        (const float *)V, coef, (float *)mu, ncell);
+  QJ_CK_LAUNCH();
+  return 0;
+}
+
+int launch_adj_update(bool dbl, void *g, const void *psi, const void *V, const void *W, double coef,
+                      long long ncell, cudaStream_t st) {
+  if (dbl)
+    k_adj_update<double><<<grid_blocks(ncell), 256, 0, st>>>(
+        (double2 *)g, (const double2 *)psi, (const double *)V, (const double *)W, coef, ncell);
+  else
+    k_adj_update<float><<<grid_blocks(ncell), 256, 0, st>>>(
+        (float2 *)g, (const float2 *)psi, (const float *)V, (const float *)W, coef, ncell);
+  QJ_CK_LAUNCH();
+  return 0;
+}
+
 int launch_build_rho(bool dbl, const void *psi, const void *rho_s, const void *rho_gas,
                      const void *rho_in, double fourpiG, double rho_bar, void *rho_tot,
                      void *cbuf, long long ncell, cudaStream_t st) {

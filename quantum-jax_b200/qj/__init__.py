@@ -2,4 +2,4 @@
 quantum-jax, behind the C ABI of libqj.so (include/qj.h)."""
 
 from ._lib import QjError, lib  # noqa: F401
-from .core import FUSED_F32, PLAIN_F64, Grid, Phys, Plan, StarsStep  # noqa: F401
+from .core import FUSED_F32, PLAIN_F64, Ensemble, Grid, Phys, Plan, StarsStep  # noqa: F401

@@ -40,6 +40,14 @@ SIGNATURES = {
     "qj_plan_create": (c_int, [ctypes.POINTER(c_void_p), ctypes.POINTER(QjGrid),
                                ctypes.POINTER(QjPhys), c_int, c_int]),
     "qj_plan_destroy": (c_int, [c_void_p]),
+    "qj_plan_create_batched": (c_int, [ctypes.POINTER(c_void_p), ctypes.POINTER(QjGrid),
+                                       ctypes.POINTER(QjPhys), c_int, c_int, c_int]),
+    "qj_ensemble_create": (c_int, [ctypes.POINTER(c_void_p), ctypes.POINTER(c_void_p), c_int]),
+    "qj_ensemble_destroy": (c_int, [c_void_p]),
+    "qj_ensemble_step": (c_int, [c_void_p, ctypes.POINTER(c_void_p), ctypes.POINTER(c_void_p),
+                                 ctypes.POINTER(c_void_p), ctypes.POINTER(c_int),
+                                 ctypes.POINTER(c_double), ctypes.POINTER(c_double),
+                                 ctypes.POINTER(c_void_p), c_int, c_int, c_int, c_void_p]),
     "qj_plan_set_phys": (c_int, [c_void_p, ctypes.POINTER(QjPhys)]),
     "qj_last_error": (ctypes.c_char_p, []),
     "qj_get_potential": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
@@ -52,6 +60,10 @@ SIGNATURES = {
     "qj_kdk_gas_bh_step": (c_int, [c_void_p] + [c_void_p] * 8 + [c_int, c_double, c_int, c_double,
                                                                  c_int, c_double,
                                                                  ctypes.POINTER(c_double), c_void_p]),
+    "qj_kdk_forward_ckpt": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, c_double, c_int,
+                                    c_void_p, c_void_p]),
+    "qj_kdk_adjoint": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_double, c_int,
+                               c_void_p, c_void_p]),
     "qj_kdk_cosmo": (c_int, [c_void_p, c_void_p, ctypes.POINTER(c_double), c_double, c_double,
                              c_double, c_double, c_int, c_void_p]),
     "qj_get_potential_f32_noalloc": (c_int, [ctypes.POINTER(QjGrid), ctypes.POINTER(QjPhys),

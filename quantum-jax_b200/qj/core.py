@@ -81,18 +81,19 @@ class Plan:
     ``PLAIN_F64`` (complex128 / float64, unfused reference-order kernels).
     """
 
-    def __init__(self, grid: Grid, phys: Phys, precision=FUSED_F32, max_particles=4096):
+    def __init__(self, grid: Grid, phys: Phys, precision=FUSED_F32, max_particles=4096, nbox=1):
         self.grid = grid
         self.phys = phys
         self.precision = precision
         self.max_particles = int(max_particles)
+        self.nbox = int(nbox)
         self.rdtype = torch.float32 if precision == FUSED_F32 else torch.float64
         self.cdtype = torch.complex64 if precision == FUSED_F32 else torch.complex128
         self._h = ctypes.c_void_p()
         g = _lib.QjGrid(grid.nx, grid.ny, grid.nz, grid.Lx, grid.Ly, grid.Lz)
-        check(lib().qj_plan_create(ctypes.byref(self._h), ctypes.byref(g),
-                                   ctypes.byref(self._phys_struct()), int(precision),
-                                   self.max_particles))
+        check(lib().qj_plan_create_batched(ctypes.byref(self._h), ctypes.byref(g),
+                                           ctypes.byref(self._phys_struct()), int(precision),
+                                           self.max_particles, self.nbox))
 
     def _phys_struct(self):
         p = self.phys
@@ -221,15 +222,32 @@ class Plan:
                  v_ext=None):
         """nsteps x compute_step (quantum-stars.py:295-330), in place.
 
-        diag: CUDA float64 tensor [3] = (t, a_max, dt_s), updated in place."""
-        self._field(psi, "psi", complex_=True)
+        diag: CUDA float64 tensor [3] = (t, a_max, dt_s), updated in place.
+        A batched plan takes psi [nbox, nx, ny, nz], pos / vel [nbox, n_s, 3]
+        and diag [nbox, 3]."""
         n_s = 0
-        if pos is not None:
-            self._particles(pos, "pos")
-            n_s = pos.shape[0]
-            self._particles(vel, "vel", n_s)
-        if diag.dtype != torch.float64 or diag.numel() != 3 or not diag.is_cuda:
-            raise ValueError("diag must be a CUDA float64 tensor of 3 elements")
+        if self.nbox == 1:
+            self._field(psi, "psi", complex_=True)
+            if pos is not None:
+                self._particles(pos, "pos")
+                n_s = pos.shape[0]
+                self._particles(vel, "vel", n_s)
+        else:
+            shape = (self.nbox,) + self.grid.shape
+            if (not psi.is_cuda or psi.dtype != self.cdtype or tuple(psi.shape) != shape
+                    or not psi.is_contiguous()):
+                raise ValueError(f"psi must be a contiguous CUDA {self.cdtype} {shape} tensor")
+            if pos is not None:
+                for name, t in (("pos", pos), ("vel", vel)):
+                    if (not t.is_cuda or t.dtype != self.rdtype or t.dim() != 3
+                            or t.shape[0] != self.nbox or t.shape[2] != 3
+                            or not t.is_contiguous()):
+                        raise ValueError(f"{name} must be a contiguous [nbox, n_s, 3] tensor")
+                n_s = pos.shape[1]
+                if tuple(vel.shape) != tuple(pos.shape):
+                    raise ValueError("vel must match pos")
+        if diag.dtype != torch.float64 or diag.numel() != 3 * self.nbox or not diag.is_cuda:
+            raise ValueError("diag must be a CUDA float64 tensor of 3 * nbox elements")
         if v_ext is not None:
             self._field(v_ext, "v_ext")
         check(lib().qj_kdk_step(self._h, _ptr(psi), _ptr(pos) if n_s else None,
@@ -237,6 +255,45 @@ class Plan:
                                 int(nsteps), int(bool(self_interaction)), _ptr(v_ext),
                                 _ptr(diag), _stream()))
         return psi, pos, vel, diag
+
+
+class Ensemble:
+    """Independent boxes of uneven size stepped together: one batched plan per
+    size, each on its own stream, with the step body captured once in a CUDA
+    graph and replayed (qj_ensemble_step)."""
+
+    def __init__(self, plans):
+        self.plans = list(plans)
+        self._h = ctypes.c_void_p()
+        arr = (ctypes.c_void_p * len(self.plans))(*[p._h.value for p in self.plans])
+        check(lib().qj_ensemble_create(ctypes.byref(self._h), arr, len(self.plans)))
+
+    def step(self, psi, pos, vel, diag, dt, m_s, nsteps, chunk=10, graph=True):
+        """psi / pos / vel / diag: per-plan tensors as for a batched
+        Plan.kdk_step; dt, m_s: per-plan floats."""
+        n = len(self.plans)
+        P = ctypes.c_void_p * n
+        n_s = [0 if p is None else int(p.shape[1] if p.dim() == 3 else p.shape[0]) for p in pos]
+        check(lib().qj_ensemble_step(
+            self._h, P(*[t.data_ptr() for t in psi]),
+            P(*[0 if t is None else t.data_ptr() for t in pos]),
+            P(*[0 if t is None else t.data_ptr() for t in vel]),
+            (ctypes.c_int * n)(*n_s), (ctypes.c_double * n)(*[float(x) for x in m_s]),
+            (ctypes.c_double * n)(*[float(x) for x in dt]),
+            P(*[t.data_ptr() for t in diag]), int(nsteps), int(chunk), int(bool(graph)),
+            _stream()))
+
+    def close(self):
+        if self._h:
+            torch.cuda.synchronize()
+            lib().qj_ensemble_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class StarsStep:
