@@ -60,6 +60,9 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--ens-steps", type=int, default=100)
+    ap.add_argument("--ens-chunk", type=int, default=10)
     ap.add_argument("--adj-n", type=int, default=128)
     ap.add_argument("--adj-steps", type=int, default=200)
     ap.add_argument("--adj-ckpt", type=int, default=20)
@@ -421,6 +424,93 @@ def main():
                            "(two Poisson solves per kick); forward = qj_kdk_step, psi only"}
         plan_a.close()
 
+    # ---------------- ensemble: 16x64^3 + 8x96^3 + 8x128^3, 256 stars each -----
+    ensemble = None
+    if not a.no_ensemble:
+        groups = [(64, 16), (96, 8), (128, 8)]
+        ens_steps, seed = a.ens_steps, 100
+        plans, state, singles = [], [], []
+        for n_e, nb in groups:
+            ics = []
+            for b in range(nb):
+                ics.append(O.stars_ic(n_e, 256, seed=seed))
+                seed += 1
+            g_e, p_e = ics[0][3], ics[0][4]
+            dt_e = O.default_dt(g_e, p_e)
+            pl = qj.Plan(qj.Grid(n_e, n_e, n_e),
+                         qj.Phys(m_per_hbar=1.0, G=p_e.G, rho_bar=p_e.rho_bar), qj.FUSED_F32, 256,
+                         nbox=nb)
+            psi_e = torch.as_tensor(np.stack([i[0] for i in ics]), dtype=torch.complex64,
+                                    device=dev).contiguous()
+            pos_e = torch.as_tensor(np.stack([i[1] for i in ics]), dtype=torch.float32,
+                                    device=dev).contiguous()
+            vel_e = torch.zeros_like(pos_e)
+            diag_e = torch.tensor([[0.0, 0.0, dt_e]] * nb, dtype=torch.float64, device=dev)
+            plans.append(pl)
+            state.append([psi_e, pos_e, vel_e, diag_e, dt_e, p_e.m_s])
+            singles.append(qj.Plan(qj.Grid(n_e, n_e, n_e),
+                                   qj.Phys(m_per_hbar=1.0, G=p_e.G, rho_bar=p_e.rho_bar),
+                                   qj.FUSED_F32, 256))
+        ens = qj.Ensemble(plans)
+        init = [[t.clone() if isinstance(t, torch.Tensor) else t for t in s] for s in state]
+
+        def ens_run(m):
+            ens.step([s[0] for s in state], [s[1] for s in state], [s[2] for s in state],
+                     [s[3] for s in state], [s[4] for s in state], [s[5] for s in state], m,
+                     chunk=a.ens_chunk, graph=True)
+
+        ens_run(a.ens_chunk)  # capture + warm-up
+        barrier()
+        e0.record(stream)
+        ens_run(ens_steps)
+        e1.record(stream)
+        barrier()
+        ens_ms = e0.elapsed_time(e1)
+        cells = sum(n_e**3 * nb for n_e, nb in groups)
+        # one by one: each box alone through a single-box plan, same steps
+        views = []
+        for gi, (n_e, nb) in enumerate(groups):
+            for b in range(nb):
+                s = init[gi]
+                views.append((singles[gi], s[0][b].clone(), s[1][b].clone(), s[2][b].clone(),
+                              s[3][b].clone(), s[4], s[5]))
+        for v in views[:1] + views[16:17] + views[24:25]:  # warm-up each size
+            v[0].kdk_step(v[1], v[2], v[3], v[4], v[5], 2, v[6])
+        barrier()
+        e0.record(stream)
+        for v in views:
+            v[0].kdk_step(v[1], v[2], v[3], v[4], v[5], ens_steps, v[6])
+        e1.record(stream)
+        barrier()
+        seq_ms = e0.elapsed_time(e1)
+        # per-box error of the ensemble against the float64 path (first box of each size)
+        errs = {}
+        for gi, (n_e, nb) in enumerate(groups):
+            pl64 = qj.Plan(qj.Grid(n_e, n_e, n_e),
+                           qj.Phys(m_per_hbar=1.0, G=plans[gi].phys.G, rho_bar=plans[gi].phys.rho_bar),
+                           qj.PLAIN_F64, 256)
+            s0 = init[gi]
+            ps64 = s0[0][0].to(torch.complex128).contiguous()
+            po64 = s0[1][0].double().contiguous()
+            ve64 = s0[2][0].double().contiguous()
+            d64 = torch.tensor([0.0, 0.0, s0[4]], dtype=torch.float64, device=dev)
+            pl64.kdk_step(ps64, po64, ve64, d64, s0[4], a.ens_chunk + ens_steps, s0[5])
+            torch.cuda.synchronize()
+            got = state[gi][0][0].to(torch.complex128)
+            errs[f"{n_e}^3"] = float(torch.linalg.vector_norm(got - ps64) /
+                                     torch.linalg.vector_norm(ps64))
+            pl64.close()
+        ensemble = {"boxes": "16x64^3 + 8x96^3 + 8x128^3, 256 stars each",
+                    "cells": cells, "steps": ens_steps, "graph_chunk": a.ens_chunk,
+                    "ensemble_cell_steps_per_s": cells * ens_steps / (ens_ms * 1e-3),
+                    "one_by_one_cell_steps_per_s": cells * ens_steps / (seq_ms * 1e-3),
+                    "speedup": seq_ms / ens_ms,
+                    "psi_rel_l2_vs_f64_first_box": errs,
+                    "error_steps": a.ens_chunk + ens_steps}
+        ens.close()
+        for pl in plans + singles:
+            pl.close()
+
     cb = None
     if rank == 0 and world == 1 and not a.no_cpu:
         cb = cpu_baseline(n, n_s, 2)
@@ -445,7 +535,7 @@ def main():
                              "f64_path": "plain float64 GPU path (matches the oracle to 1e-11)"},
                 "roofline": roofline, "step_roofline": step_roof, "passes": per_pass,
                 "gpu_launches": launches, "clocks": clk, "e2e": e2e, "cpu_baseline": cb,
-                "adjoint": adjoint}
+                "adjoint": adjoint, "ensemble": ensemble}
         print(json.dumps(line), flush=True)
     fused.close()
     if dist is not None:

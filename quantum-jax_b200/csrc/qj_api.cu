@@ -88,10 +88,12 @@ __global__ void k_prop_tables(float2 *p0, float2 *p1, float2 *p2, const double *
   const int N[3] = {n0, n1, n2};
   for (int a = 0; a < 3; ++a) {
     if (i < N[a]) {
+      // stored as d = exp(i th) - 1 = (-2 sin^2(th/2), sin th): the pass applies
+      // psi + psi d, so the unit part is exact and small phases keep full
+      // relative precision (the 1/n of ifftn is applied separately)
       const double th = -dtk * K[a][i] * K[a][i] / (2.0 * mph);
-      double s, c;
-      sincos(th, &s, &c);
-      P[a][i] = float2{(float)(c / N[a]), (float)(s / N[a])};
+      const double sh = sin(0.5 * th);
+      P[a][i] = float2{(float)(-2.0 * sh * sh), (float)sin(th)};
     }
   }
 }
@@ -145,7 +147,7 @@ struct qj_plan {
   void *tmp_diag = nullptr;
   void *gas_out[4] = {nullptr, nullptr, nullptr, nullptr};  // hydro output scratch
   // adjoint: recomputed chunk states
-  void *adj_psi = nullptr, *adj_states = nullptr;
+  void *adj_psi = nullptr, *adj_states = nullptr, *adj_V = nullptr;
   int adj_cap = 0;
 };
 
@@ -245,6 +247,7 @@ FusedArgs fused_args(const qj_plan *P, int axis) {
   a.S2 = P->S2;
   a.tw = P->tws[axis];
   a.prop = P->prop[axis];
+  a.prop_scale = 1.0f / (float)P->n[axis];
   for (int d = 0; d < 3; ++d) {
     a.k[d] = P->kf[d];
     a.kt[d] = P->ktf[d];
@@ -312,7 +315,7 @@ struct StepCoefs {
 
 int fused_kdk(qj_plan *P, float2 *psi, float *pos, float *vel, int n_s, double m_s, double dt,
               int nsteps, int si, const float *vext, double *diag, cudaStream_t st,
-              const StepCoefs *sc = nullptr, void *save = nullptr) {
+              const StepCoefs *sc = nullptr, void *save = nullptr, float *vsave = nullptr) {
   const bool parts = n_s > 0;
   const int nb = P->nbox;  // boxes: fields [nb][nx][ny][nz], stars [nb][n_s][3]
   P->cur_stars = n_s;
@@ -359,6 +362,7 @@ int fused_kdk(qj_plan *P, float2 *psi, float *pos, float *vel, int n_s, double m
       a.b_coeff = si ? (float)P->ph.b_coeff : 0.0f;
       a.v_ext = vext;
       a.do_drift = last ? 0 : 1;
+      if (vsave) a.v_out = vsave + (size_t)k * P->ncell;  // V of kick k (adjoint)
       if (parts) set_stars(a, P);
       QJ_TRY(launch_fused(M_KICK, P->n[q], a, st));
     }
@@ -504,14 +508,14 @@ int plain_kdk(qj_plan *P, void *psi, void *pos, void *vel, int n_s, double m_s, 
 // recomputes each chunk forward, saving the state before every kick.
 // ---------------------------------------------------------------------------
 int kdk_chunk(qj_plan *P, void *psi, int m, double dt, int si, const void *vext, cudaStream_t st,
-              void *save) {
+              void *save, float *vsave = nullptr) {
   if (!P->tmp_diag) QJ_TRY(dev_alloc(P, &P->tmp_diag, 3 * sizeof(double)));
   QJ_CK(cudaMemsetAsync(P->tmp_diag, 0, 3 * sizeof(double), st));
   if (P->dbl)
     return plain_kdk(P, psi, nullptr, nullptr, 0, 0.0, dt, m, si, vext, (double *)P->tmp_diag, st,
                      nullptr, save);
   return fused_kdk(P, (float2 *)psi, nullptr, nullptr, 0, 0.0, dt, m, si, (const float *)vext,
-                   (double *)P->tmp_diag, st, nullptr, save);
+                   (double *)P->tmp_diag, st, nullptr, save, vsave);
 }
 
 int adjoint_sweep(qj_plan *P, const void *ckpt, void *g, int nsteps, int K, double dt, int si,
@@ -521,6 +525,9 @@ int adjoint_sweep(qj_plan *P, const void *ckpt, void *g, int nsteps, int K, doub
   if (!P->adj_psi) QJ_TRY(dev_alloc(P, &P->adj_psi, fb));
   if (P->adj_cap < K) {
     QJ_TRY(dev_alloc(P, &P->adj_states, (size_t)K * fb));
+    // single precision: the recompute also keeps each kick's potential, so
+    // the reverse sweep needs one Poisson solve per kick instead of two
+    if (!P->dbl) QJ_TRY(dev_alloc(P, &P->adj_V, (size_t)(K + 1) * P->ncell * sizeof(float)));
     P->adj_cap = K;
   }
   const int nseg = (nsteps + K - 1) / K;
@@ -530,12 +537,16 @@ int adjoint_sweep(qj_plan *P, const void *ckpt, void *g, int nsteps, int K, doub
     const int m = std::min(K, nsteps - seg * K);
     const void *c0 = (const char *)ckpt + (size_t)seg * fb;
     QJ_CK(cudaMemcpyAsync(P->adj_psi, c0, fb, cudaMemcpyDeviceToDevice, st));
-    QJ_TRY(kdk_chunk(P, P->adj_psi, m, dt, si, vext, st, P->adj_states));
+    QJ_TRY(kdk_chunk(P, P->adj_psi, m, dt, si, vext, st, P->adj_states, (float *)P->adj_V));
     for (int j = m; j >= 0; --j) {
       const void *pre = j == 0 ? c0 : (const char *)P->adj_states + (size_t)(j - 1) * fb;
       const double coef = half * ((j == 0 || j == m) ? 1.0 : 2.0);
-      QJ_TRY(plain_potential(P, pre, nullptr, nullptr, P->V, si, vext, st));
-      QJ_TRY(launch_adj_mu(P->dbl, g, pre, P->V, coef, mu, P->ncell, st));
+      const void *Vj = P->V;
+      if (P->dbl)
+        QJ_TRY(plain_potential(P, pre, nullptr, nullptr, P->V, si, vext, st));
+      else
+        Vj = (const float *)P->adj_V + (size_t)j * P->ncell;
+      QJ_TRY(launch_adj_mu(P->dbl, g, pre, Vj, coef, mu, P->ncell, st));
       // W = (L + b) mu: the Poisson operator without the rho_bar shift
       QJ_TRY(launch_build_rho(P->dbl, nullptr, nullptr, nullptr, mu, 4.0 * M_PI * P->ph.G, 0.0,
                               nullptr, P->c0, P->ncell, st));
@@ -544,7 +555,7 @@ int adjoint_sweep(qj_plan *P, const void *ckpt, void *g, int nsteps, int K, doub
       QJ_TRY(fft3d(P, P->c0, +1, st));
       QJ_TRY(launch_real_part(P->dbl, P->c0, 1.0, si ? mu : nullptr, P->ph.b_coeff, nullptr, W,
                               P->ncell, st));
-      QJ_TRY(launch_adj_update(P->dbl, g, pre, P->V, W, coef, P->ncell, st));
+      QJ_TRY(launch_adj_update(P->dbl, g, pre, Vj, W, coef, P->ncell, st));
       if (j > 0) {  // adjoint of drift j - 1
         QJ_TRY(fft3d(P, g, -1, st));
         QJ_TRY(launch_drift_mul(P->dbl, g, ktabs(P), -dt, P->ph.m_per_hbar, P->ncell, st));

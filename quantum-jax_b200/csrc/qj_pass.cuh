@@ -46,7 +46,9 @@ struct FusedArgs {
   float2 *S1;
   float2 *S2;
   const float2 *tw;    // stage twiddle table of this axis' length (stage_tw_off)
-  const float2 *prop;  // drift propagator of this axis, already scaled by 1/n
+  const float2 *prop;  // drift propagator of this axis minus one (see prop_apply)
+  float prop_scale;    // 1/n of this axis
+  float *v_out;        // KICK: optional copy of the kick potential V (adjoint)
   const float *k[3];   // k value per index, per axis (Nyquist negative)
   const float *kt[3];  // k with the Nyquist entry set to 0 (odd derivatives)
   // stars filed by the pencil of their lower CIC corner (this pass' axis)
@@ -335,6 +337,14 @@ __device__ __forceinline__ void sincos_reduced(double theta, float &sn, float &c
   cs = q == 0 ? c : (q == 1 ? -s : (q == 2 ? -c : s));
 }
 
+// Drift propagator applied in the form (z + z d) * scale with
+// d = exp(i th) - 1 and scale = 1/n.
+__device__ __forceinline__ float2 prop_apply(float2 z, float2 d, float scale) {
+  const float re = fmaf(z.x, d.x, fmaf(-z.y, d.y, z.x));
+  const float im = fmaf(z.x, d.y, fmaf(z.y, d.x, z.y));
+  return float2{re * scale, im * scale};
+}
+
 // exp(-i theta) * z
 __device__ __forceinline__ float2 phase_rotate(float2 z, double theta) {
   float s, c;
@@ -552,10 +562,14 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CO
     }
 #pragma unroll
     for (int e = 0; e < E; ++e) ps[e] = phase_rotate(ps[e], a.kick_coef * (double)V[e]);
+    if (a.v_out) {
+#pragma unroll
+      for (int e = 0; e < E; ++e) a.v_out[gb + e * gs] = V[e];
+    }
     if (a.do_drift) {
       fft_pencil<N, -1, true>(ps, t, smv, tw);
 #pragma unroll
-      for (int e = 0; e < E; ++e) ps[e] = cmul(ps[e], __ldg(&a.prop[t + P * e]));
+      for (int e = 0; e < E; ++e) ps[e] = prop_apply(ps[e], __ldg(&a.prop[t + P * e]), a.prop_scale);
       fft_pencil<N, +1, true>(ps, t, smv, tw);
     }
     store_pencil<E>(ps, a.psi, base, st, t, P);
@@ -587,7 +601,7 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CO
     load_pencil<E>(v, a.psi, base, st, t, P);
     fft_pencil<N, -1, true>(v, t, smv, tw);
 #pragma unroll
-    for (int e = 0; e < E; ++e) v[e] = cmul(v[e], __ldg(&a.prop[t + P * e]));
+    for (int e = 0; e < E; ++e) v[e] = prop_apply(v[e], __ldg(&a.prop[t + P * e]), a.prop_scale);
     fft_pencil<N, +1, true>(v, t, smv, tw);
     store_pencil<E>(v, a.psi, base, st, t, P);
     if constexpr (MODE == M_DRIFT_DENSITY) {
