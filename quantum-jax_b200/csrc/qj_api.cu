@@ -76,9 +76,9 @@ int cuda_fail(cudaError_t e, const char *what, const char *file, int line) {
   return e == cudaErrorMemoryAllocation ? QJ_ERR_ALLOC : QJ_ERR_CUDA;
 }
 
-// Drift propagator of each axis, float64 phase, rounded once:
-// prop_a[i] = exp(-1j * dt_kin * k_a[i]^2 / (2 m_per_hbar)) / n_a
-// (the separable factor of quantum-stars.py:308, with the 1/n_a of ifftn).
+// Drift propagator of each axis minus one, float64 phase, rounded once:
+// prop_a[i] = exp(-1j * dt_kin * k_a[i]^2 / (2 m_per_hbar)) - 1
+// (the separable factor of quantum-stars.py:308).
 __global__ void k_prop_tables(float2 *p0, float2 *p1, float2 *p2, const double *k0,
                               const double *k1, const double *k2, int n0, int n1, int n2,
                               double dtk, double mph) {
@@ -88,9 +88,9 @@ __global__ void k_prop_tables(float2 *p0, float2 *p1, float2 *p2, const double *
   const int N[3] = {n0, n1, n2};
   for (int a = 0; a < 3; ++a) {
     if (i < N[a]) {
-      // stored as d = exp(i th) - 1 = (-2 sin^2(th/2), sin th): the pass applies
-      // psi + psi d, so the unit part is exact and small phases keep full
-      // relative precision (the 1/n of ifftn is applied separately)
+      // stored as d = exp(i th) - 1 = (-2 sin^2(th/2), sin th): the pass adds
+      // IFFT(d FFT(psi)) to psi, so small phases keep full relative precision
+      // (the 1/n of ifftn is applied after the transform)
       const double th = -dtk * K[a][i] * K[a][i] / (2.0 * mph);
       const double sh = sin(0.5 * th);
       P[a][i] = float2{(float)(-2.0 * sh * sh), (float)sin(th)};
@@ -247,7 +247,6 @@ FusedArgs fused_args(const qj_plan *P, int axis) {
   a.S2 = P->S2;
   a.tw = P->tws[axis];
   a.prop = P->prop[axis];
-  a.prop_scale = 1.0f / (float)P->n[axis];
   for (int d = 0; d < 3; ++d) {
     a.k[d] = P->kf[d];
     a.kt[d] = P->ktf[d];

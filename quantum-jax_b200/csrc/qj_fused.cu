@@ -60,7 +60,7 @@ int pass_blocks(int n_axis, int axis, int nx, int ny, int nz) {
 template <int N, bool CONTIG, int MODE>
 static int run_fused(const FusedArgs &a, cudaStream_t st) {
   using SH = PassShape<N, CONTIG>;
-  const size_t smem = SH::template smem_bytes<float2>() + stage_tw_size<N>() * sizeof(float2);
+  const size_t smem = fused_smem_bytes<N, CONTIG, MODE>();
   static std::once_flag once;
   static cudaError_t attr_err = cudaSuccess;
   std::call_once(once, [&] {
@@ -69,7 +69,7 @@ static int run_fused(const FusedArgs &a, cudaStream_t st) {
   });
   QJ_CK(attr_err);
   // L2 prefetch distance: the CTAs resident at once (occupancy x SMs) times
-  // QJ_L2_PREFETCH_WAVES (default 1; 0 disables).
+  // QJ_L2_PREFETCH_WAVES (default 0 = off).
   static int ahead = -1;
   if (ahead < 0) {
     int dev = 0, sms = 0, per_sm = 0;

@@ -46,8 +46,7 @@ struct FusedArgs {
   float2 *S1;
   float2 *S2;
   const float2 *tw;    // stage twiddle table of this axis' length (stage_tw_off)
-  const float2 *prop;  // drift propagator of this axis minus one (see prop_apply)
-  float prop_scale;    // 1/n of this axis
+  const float2 *prop;  // drift propagator of this axis minus one (see drift_pencil)
   float *v_out;        // KICK: optional copy of the kick potential V (adjoint)
   const float *k[3];   // k value per index, per axis (Nyquist negative)
   const float *kt[3];  // k with the Nyquist entry set to 0 (odd derivatives)
@@ -337,12 +336,56 @@ __device__ __forceinline__ void sincos_reduced(double theta, float &sn, float &c
   cs = q == 0 ? c : (q == 1 ? -s : (q == 2 ? -c : s));
 }
 
-// Drift propagator applied in the form (z + z d) * scale with
-// d = exp(i th) - 1 and scale = 1/n.
-__device__ __forceinline__ float2 prop_apply(float2 z, float2 d, float scale) {
-  const float re = fmaf(z.x, d.x, fmaf(-z.y, d.y, z.x));
-  const float im = fmaf(z.x, d.y, fmaf(z.y, d.x, z.y));
-  return float2{re * scale, im * scale};
+__device__ __forceinline__ float2 cmulf(float2 z, float2 d) {
+  return float2{fmaf(z.x, d.x, -(z.y * d.y)), fmaf(z.x, d.y, z.y * d.x)};
+}
+
+// s + w / n (the 1/n of the inverse transform): exact scaling for powers of
+// two, a correctly rounded division otherwise, so no bias builds up over steps.
+template <int N>
+__device__ __forceinline__ float2 add_scaled(float2 s, float2 w) {
+  if constexpr ((N & (N - 1)) == 0) {
+    constexpr float r = 1.0f / N;
+    return float2{fmaf(w.x, r, s.x), fmaf(w.y, r, s.y)};
+  } else {
+    return float2{s.x + __fdiv_rn(w.x, (float)N), s.y + __fdiv_rn(w.y, (float)N)};
+  }
+}
+
+// Kinetic drift of one pencil along its axis, psi <- IFFT(prop FFT(psi)),
+// evaluated in increment form
+//   psi <- psi + IFFT(d FFT(psi - c)),  d = prop - 1,  c = the pencil's first element.
+// d(k=0) = 0 removes c exactly.  The float32 rounding of the two transforms
+// then scales with |d (psi - c)| instead of |psi|: for the slowly turning
+// low-k modes, whose per-step rounding would otherwise repeat step after step
+// and add up linearly, it is smaller by the phase d.  The pre-transform values
+// wait in the thread's own slots of `save` (no barrier needed).
+template <int N, int E, int P, int THREADS, class SMV>
+__device__ __forceinline__ void drift_pencil(float2 (&v)[E], float2 c, const float2 *__restrict__ prop,
+                                             int t, SMV &smv, const float2 *tw, float2 *save) {
+  const int tid = threadIdx.x;
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    save[e * THREADS + tid] = v[e];
+    v[e] = float2{v[e].x - c.x, v[e].y - c.y};
+  }
+  fft_pencil<N, -1, true>(v, t, smv, tw);
+#pragma unroll
+  for (int e = 0; e < E; ++e) v[e] = cmulf(v[e], __ldg(&prop[t + P * e]));
+  fft_pencil<N, +1, true>(v, t, smv, tw);
+#pragma unroll
+  for (int e = 0; e < E; ++e) v[e] = add_scaled<N>(save[e * THREADS + tid], v[e]);
+}
+
+// Dynamic shared memory of a fused pass: the exchange rows, the stage twiddle
+// table and, for the drift passes, THREADS x E save slots.
+template <int N, bool CONTIG, int MODE>
+__host__ __device__ constexpr size_t fused_smem_bytes() {
+  using SH = PassShape<N, CONTIG>;
+  return SH::template smem_bytes<float2>() + stage_tw_size<N>() * sizeof(float2) +
+         ((MODE == M_KICK || MODE == M_DRIFT || MODE == M_DRIFT_DENSITY)
+              ? (size_t)SH::THREADS * SH::E * sizeof(float2)
+              : 0);
 }
 
 // exp(-i theta) * z
@@ -420,6 +463,7 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CO
   for (int i = tid; i < stage_tw_size<N>(); i += THREADS) tw_s[i] = a.tw[i];
   __syncthreads();
   const float2 *tw = tw_s;
+  float2 *save = tw_s + stage_tw_size<N>();  // drift passes: per-thread slots
 
   if constexpr (MODE == M_DENSITY) {
     float2 v[E];
@@ -567,10 +611,9 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CO
       for (int e = 0; e < E; ++e) a.v_out[gb + e * gs] = V[e];
     }
     if (a.do_drift) {
-      fft_pencil<N, -1, true>(ps, t, smv, tw);
-#pragma unroll
-      for (int e = 0; e < E; ++e) ps[e] = prop_apply(ps[e], __ldg(&a.prop[t + P * e]), a.prop_scale);
-      fft_pencil<N, +1, true>(ps, t, smv, tw);
+      // read before any thread of this pencil stores (the FFT's barriers order it)
+      const float2 c0 = a.psi[base];
+      drift_pencil<N, E, P, THREADS>(ps, c0, a.prop, t, smv, tw, save);
     }
     store_pencil<E>(ps, a.psi, base, st, t, P);
 #pragma unroll
@@ -599,10 +642,9 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CO
   } else if constexpr (MODE == M_DRIFT || MODE == M_DRIFT_DENSITY) {
     float2 v[E];
     load_pencil<E>(v, a.psi, base, st, t, P);
-    fft_pencil<N, -1, true>(v, t, smv, tw);
-#pragma unroll
-    for (int e = 0; e < E; ++e) v[e] = prop_apply(v[e], __ldg(&a.prop[t + P * e]), a.prop_scale);
-    fft_pencil<N, +1, true>(v, t, smv, tw);
+    // read before any thread of this pencil stores (the FFT's barriers order it)
+    const float2 c0 = a.psi[base];
+    drift_pencil<N, E, P, THREADS>(v, c0, a.prop, t, smv, tw, save);
     store_pencil<E>(v, a.psi, base, st, t, P);
     if constexpr (MODE == M_DRIFT_DENSITY) {
       double s = build_density<N, E>(v, a, pp, t, P);
