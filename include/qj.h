@@ -207,6 +207,12 @@ int qj_ensemble_step(qj_ensemble *ens, void *const *psi, void *const *pos,
 /* Bytes of device workspace the plan holds. */
 int64_t qj_plan_workspace_bytes(const qj_plan *plan);
 
+/* qj_plan_status: waits for the device, then returns QJ_ERR_TIMEOUT (and
+ * clears the flag) if a fused pass of this plan gave up a bounded wait for
+ * one of its tile copies since the last call, else QJ_OK.  No reference
+ * counterpart: the reference's XLA kernels have no device-side waits. */
+int qj_plan_status(qj_plan *plan);
+
 /* Instrumentation (no reference counterpart; used by the benchmark).
  * qj_launch_count: kernels libqj has launched in this process.
  * qj_profile_enable(1) clears and starts per-pass CUDA-event timing;

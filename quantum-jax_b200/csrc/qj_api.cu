@@ -143,6 +143,7 @@ struct qj_plan {
   cudaStream_t side = nullptr;
   cudaEvent_t ev_kick = nullptr, ev_parts = nullptr;
   void *amax = nullptr, *dts = nullptr;  // real type scalars
+  unsigned *err = nullptr;  // set by a fused pass whose bounded tile wait gave up
   void *tmp_scalar = nullptr;
   void *tmp_diag = nullptr;
   void *gas_out[4] = {nullptr, nullptr, nullptr, nullptr};  // hydro output scratch
@@ -256,6 +257,7 @@ FusedArgs fused_args(const qj_plan *P, int axis) {
   a.rho_bar = P->ph.rho_bar;
   a.inv_ncell = 1.0 / (double)P->ncell;
   a.amax_bits = (unsigned *)P->amax;
+  a.err = P->err;
   a.nbox = P->nbox;
   a.box_cells = P->ncell;
   a.box_stars = P->cur_stars;
@@ -903,6 +905,9 @@ int qj_plan_create_batched(qj_plan **plan, const qj_grid *grid, const qj_phys *p
   if ((rc = dev_alloc(P, &P->amax, 8 * (size_t)nbox))) return fail(rc);
   if ((rc = dev_alloc(P, &P->dts, 8 * (size_t)nbox))) return fail(rc);
   if ((rc = dev_alloc(P, &P->tmp_scalar, 8))) return fail(rc);
+  if ((rc = dev_alloc_t(P, &P->err, 4))) return fail(rc);
+  if (cudaMemset(P->err, 0, 4 * sizeof(unsigned)) != cudaSuccess)
+    return fail(cuda_fail(cudaGetLastError(), "plan init", __FILE__, __LINE__));
   cudaError_t e = cudaDeviceSynchronize();
   if (e != cudaSuccess) return fail(cuda_fail(e, "plan init", __FILE__, __LINE__));
   *plan = P;
@@ -933,6 +938,20 @@ int qj_plan_set_phys(qj_plan *P, const qj_phys *phys) {
 }
 
 int64_t qj_plan_workspace_bytes(const qj_plan *P) { return P ? P->ws_bytes : 0; }
+
+int qj_plan_status(qj_plan *P) {
+  if (!P) {
+    set_error("qj_plan_status: bad argument");
+    return QJ_ERR_ARG;
+  }
+  QJ_CK(cudaDeviceSynchronize());
+  unsigned w = 0;
+  QJ_CK(cudaMemcpy(&w, P->err, sizeof(w), cudaMemcpyDeviceToHost));
+  if (w == 0) return QJ_OK;
+  QJ_CK(cudaMemset(P->err, 0, sizeof(unsigned)));
+  set_error("a fused pass gave up waiting for a tile copy (bounded wait); its results are invalid");
+  return QJ_ERR_TIMEOUT;
+}
 
 int64_t qj_launch_count(void) { return (int64_t)g_launches.load(); }
 

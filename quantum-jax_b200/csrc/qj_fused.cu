@@ -1,9 +1,16 @@
 // Instantiations and launchers of the fused single-precision pencil passes.
+#include <algorithm>
 #include <cmath>
+#include <cstdint>
+#include <cstring>
 #include <cstdlib>
 #include <mutex>
 #include <vector>
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include "../../include/qj.h"
 #include "qj_internal.h"
 
 namespace qj {
@@ -47,43 +54,120 @@ std::vector<float2> stage_twiddles(int n) {
   return {};
 }
 
+// Tiles (pencil groups of one CTA) of a pass along `axis` of length n_axis.
 int pass_blocks(int n_axis, int axis, int nx, int ny, int nz) {
   if (axis == 2) {
-    const int E = (n_axis == 32 || n_axis == 64) ? 8 : (n_axis == 96 ? 12 : 16);
-    const int P = n_axis / E;
-    const int TP = P >= 256 ? 1 : 256 / P;
-    return (nx * ny) / TP;
+    int tp = 1;
+    switch (n_axis) {
+      case 16: tp = PassShape<16, true>::TP; break;
+      case 32: tp = PassShape<32, true>::TP; break;
+      case 64: tp = PassShape<64, true>::TP; break;
+      case 96: tp = PassShape<96, true>::TP; break;
+      case 128: tp = PassShape<128, true>::TP; break;
+      case 256: tp = PassShape<256, true>::TP; break;
+      case 512: tp = PassShape<512, true>::TP; break;
+    }
+    return (nx * ny) / tp;
   }
   return (axis == 0 ? ny : nx) * (nz / 16);
+}
+
+// CTA slots a persistent pass leaves free for concurrent work on other
+// streams, such as the star update and bucket sort that run beside the y
+// drift pass (QJ_PERSIST_RESERVE, default 2).
+static int reserve_ctas() {
+  static int r = -1;
+  if (r < 0) {
+    const char *env = getenv("QJ_PERSIST_RESERVE");
+    r = env ? std::max(0, atoi(env)) : 2;
+  }
+  return r;
+}
+
+// cuTensorMapEncodeTiled from the driver, looked up once.
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
+// Tensor maps of a strided pass' streamed fields (see TileMaps).
+template <int N, int MODE>
+static int strided_maps(const FusedArgs &a, TileMaps &maps) {
+  auto enc = tensor_map_encoder();
+  if (!enc) {
+    set_error("cuTensorMapEncodeTiled is not available from the driver");
+    return QJ_ERR_CUDA;
+  }
+  const int nbox = a.nbox > 1 ? a.nbox : 1;
+  const cuuint64_t dims[4] = {(cuuint64_t)a.nz, (cuuint64_t)a.ny, (cuuint64_t)a.nx, (cuuint64_t)nbox};
+  const cuuint64_t strides[3] = {(cuuint64_t)a.nz * 8, (cuuint64_t)a.ny * a.nz * 8,
+                                 (cuuint64_t)a.box_cells * 8};
+  const cuuint32_t rows = (cuuint32_t)std::min(N, 256);
+  const cuuint32_t box[4] = {16, a.axis == 0 ? 1u : rows, a.axis == 0 ? rows : 1u, 1};
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  for (int f = 0; f < stream_count<MODE>(); ++f) {
+    const CUresult r = enc(&maps.m[f], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4,
+                           const_cast<float2 *>(stream_field<MODE>(a, f)), dims, strides, box, estr,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+      set_error("cuTensorMapEncodeTiled failed (%d) for a %dx%dx%d pass along axis %d", (int)r, a.nx,
+                a.ny, a.nz, a.axis);
+      return QJ_ERR_CUDA;
+    }
+  }
+  return 0;
 }
 
 template <int N, bool CONTIG, int MODE>
 static int run_fused(const FusedArgs &a, cudaStream_t st) {
   using SH = PassShape<N, CONTIG>;
   const size_t smem = fused_smem_bytes<N, CONTIG, MODE>();
+  // persistent grid: the CTAs resident at once (occupancy x SMs), shared
+  // between the boxes of a batched launch
   static std::once_flag once;
   static cudaError_t attr_err = cudaSuccess;
+  static int resident = 0;
   std::call_once(once, [&] {
     attr_err = cudaFuncSetAttribute(k_fused<N, CONTIG, MODE>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int dev = 0, sms = 0, per_sm = 0;
+    if (attr_err == cudaSuccess) attr_err = cudaGetDevice(&dev);
+    if (attr_err == cudaSuccess)
+      attr_err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (attr_err == cudaSuccess)
+      attr_err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fused<N, CONTIG, MODE>,
+                                                               SH::THREADS, smem);
+    resident = std::max(1, per_sm) * std::max(1, sms);
   });
   QJ_CK(attr_err);
-  // L2 prefetch distance: the CTAs resident at once (occupancy x SMs) times
-  // QJ_L2_PREFETCH_WAVES (default 0 = off).
-  static int ahead = -1;
-  if (ahead < 0) {
-    int dev = 0, sms = 0, per_sm = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fused<N, CONTIG, MODE>, SH::THREADS, smem);
-    const char *env = getenv("QJ_L2_PREFETCH_WAVES");
-    const int waves = env ? atoi(env) : 0;
-    ahead = waves > 0 ? waves * sms * (per_sm > 0 ? per_sm : 1) : 0;
-  }
+  // the bulk tile copies need 16-byte aligned fields
+  const void *fields[4] = {a.psi, a.R, a.S1, a.S2};
+  for (const void *f : fields)
+    if ((reinterpret_cast<uintptr_t>(f) & 15) != 0) {
+      set_error("fields of the fused passes must be 16-byte aligned");
+      return QJ_ERR_ARG;
+    }
   FusedArgs b = a;
-  b.ahead = ahead;
-  const dim3 grid(grid_of<N, CONTIG>(a), a.nbox > 1 ? a.nbox : 1);
-  k_fused<N, CONTIG, MODE><<<grid, SH::THREADS, smem, st>>>(b);
+  b.ntiles = grid_of<N, CONTIG>(a);
+  TileMaps maps;
+  std::memset(&maps, 0, sizeof(maps));
+  if (!CONTIG && stream_count<MODE>() > 0) {
+    const int rc = strided_maps<N, MODE>(b, maps);
+    if (rc) return rc;
+  }
+  const int nbox = a.nbox > 1 ? a.nbox : 1;
+  const int gx = std::max(1, std::min(b.ntiles, (resident - reserve_ctas()) / nbox));
+  const dim3 grid(gx, nbox);
+  k_fused<N, CONTIG, MODE><<<grid, SH::THREADS, smem, st>>>(b, maps);
   QJ_CK_LAUNCH();
   return 0;
 }

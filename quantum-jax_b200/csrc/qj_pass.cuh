@@ -20,6 +20,8 @@
 //   DRIFT_DENSITY  DRIFT along r, then DENSITY along r
 #pragma once
 
+#include <cuda.h>
+
 #include "qj_fft.cuh"
 
 namespace qj {
@@ -76,9 +78,10 @@ struct FusedArgs {
   const float *grho;
   float *gv[3];
   float gas_dt;
-  // L2 prefetch distance in CTAs (0 = off): each CTA prefetches the input
-  // tile of CTA blockIdx.x + ahead, one resident wave later
-  int ahead;
+  // tiles of this pass per box (the persistent CTAs stride over them)
+  int ntiles;
+  // set to nonzero when a pass gave up waiting for a tile copy
+  unsigned *err;
   // batched boxes (blockIdx.y = box): per-box strides of the fields (cells),
   // stars, bucket starts, partial sums; a_max is per box
   int nbox;  // launch grid.y (0 or 1 = one box)
@@ -117,18 +120,18 @@ struct PencilPos {
 };
 
 template <bool CONTIG>
-__device__ __forceinline__ PencilPos pencil_pos(const FusedArgs &a, int p, int TP) {
+__device__ __forceinline__ PencilPos pencil_pos(const FusedArgs &a, int tile, int p, int TP) {
   PencilPos pp;
   if (CONTIG) {  // axis 2: rows x * ny + y
-    const int row = blockIdx.x * TP + p;
+    const int row = tile * TP + p;
     pp.pid = row;
     pp.base = (long long)row * a.nz;
     pp.c[0] = row / a.ny;
     pp.c[1] = row % a.ny;
     pp.c[2] = 0;
   } else {
-    const int o = blockIdx.x / a.ztiles;
-    const int z = (blockIdx.x % a.ztiles) * 16 + p;
+    const int o = tile / a.ztiles;
+    const int z = (tile % a.ztiles) * 16 + p;
     pp.base = (long long)o * a.outer_stride + z;
     pp.c[2] = z;
     if (a.axis == 0) {  // o = y
@@ -361,7 +364,7 @@ __device__ __forceinline__ float2 add_scaled(float2 s, float2 w) {
 // and add up linearly, it is smaller by the phase d.  The pre-transform values
 // wait in the thread's own slots of `save` (no barrier needed).
 template <int N, int E, int P, int THREADS, class SMV>
-__device__ __forceinline__ void drift_pencil(float2 (&v)[E], float2 c, const float2 *__restrict__ prop,
+__device__ __forceinline__ void drift_pencil(float2 (&v)[E], float2 c, const float2 *prop,
                                              int t, SMV &smv, const float2 *tw, float2 *save) {
   const int tid = threadIdx.x;
 #pragma unroll
@@ -371,21 +374,10 @@ __device__ __forceinline__ void drift_pencil(float2 (&v)[E], float2 c, const flo
   }
   fft_pencil<N, -1, true>(v, t, smv, tw);
 #pragma unroll
-  for (int e = 0; e < E; ++e) v[e] = cmulf(v[e], __ldg(&prop[t + P * e]));
+  for (int e = 0; e < E; ++e) v[e] = cmulf(v[e], prop[t + P * e]);
   fft_pencil<N, +1, true>(v, t, smv, tw);
 #pragma unroll
   for (int e = 0; e < E; ++e) v[e] = add_scaled<N>(save[e * THREADS + tid], v[e]);
-}
-
-// Dynamic shared memory of a fused pass: the exchange rows, the stage twiddle
-// table and, for the drift passes, THREADS x E save slots.
-template <int N, bool CONTIG, int MODE>
-__host__ __device__ constexpr size_t fused_smem_bytes() {
-  using SH = PassShape<N, CONTIG>;
-  return SH::template smem_bytes<float2>() + stage_tw_size<N>() * sizeof(float2) +
-         ((MODE == M_KICK || MODE == M_DRIFT || MODE == M_DRIFT_DENSITY)
-              ? (size_t)SH::THREADS * SH::E * sizeof(float2)
-              : 0);
 }
 
 // exp(-i theta) * z
@@ -395,51 +387,222 @@ __device__ __forceinline__ float2 phase_rotate(float2 z, double theta) {
   return float2{z.x * c + z.y * s, z.y * c - z.x * s};
 }
 
-// Bring the tile of CTA `blk` of field f into L2 (cp.async.bulk.prefetch.L2:
-// no registers, no shared memory, no completion to wait for).  Strided tiles
-// are N rows of 16 complex64 (128 B); contiguous tiles are TP rows of N.
-template <int N, bool CONTIG>
-__device__ __forceinline__ void prefetch_tile(const float2 *f, const FusedArgs &a, int blk) {
+// ---------------------------------------------------------------------------
+// Streaming tiles through shared memory.
+//
+// The CTAs of a pass are persistent (tile = blockIdx.x + k gridDim.x).  A
+// pass reads its input fields tile by tile through one landing buffer: while
+// the CTA transforms one field of one tile, bulk copies (cp.async.bulk into
+// this CTA's own shared memory, completion counted in bytes on an mbarrier)
+// bring in the next one, i.e. the next field of the same tile or the first
+// field of the CTA's next tile.  HBM reads thus overlap the in-register
+// transforms instead of alternating with them.
+
+// Landing buffer of one tile.  Contiguous tiles (z pencils) land as one row
+// per pencil, padded by P elements when P < 16 so that the lanes of the
+// different pencils in a warp read different banks; strided tiles land as N rows of the 16
+// pencils' elements (128 B each), the dense box of a tensor-map copy.  Every
+// copy is a multiple of 16 bytes and starts on a 16-byte boundary.
+template <int N, bool CONTIG> struct Landing {
   using SH = PassShape<N, CONTIG>;
-  const int tid = threadIdx.x;
-  if (CONTIG) {
-    if (tid < SH::TP) {
-      const float2 *row = f + (long long)(blk * SH::TP + tid) * a.nz;
-      asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(row), "r"(N * 8) : "memory");
+  static constexpr int PAD = CONTIG ? (SH::P >= 16 ? 0 : (SH::P >= 2 ? SH::P : 2)) : 0;
+  static constexpr int ROWS = CONTIG ? SH::TP : N;   // bulk copies per tile
+  static constexpr int ROW_ELEMS = CONTIG ? N : 16;  // complex64 per copy
+  static constexpr int ROW_STRIDE = CONTIG ? N + PAD : 16;
+  static constexpr size_t BYTES = (size_t)ROWS * ROW_STRIDE * sizeof(float2);
+  static constexpr unsigned TX = (unsigned)ROWS * ROW_ELEMS * (unsigned)sizeof(float2);
+  static_assert((ROW_STRIDE * sizeof(float2)) % 16 == 0, "landing rows must stay 16-byte aligned");
+  static_assert(TX < (1u << 20), "tile larger than an mbarrier transaction count");
+  __device__ static __forceinline__ int idx(int p, int i) {
+    return CONTIG ? p * ROW_STRIDE + i : i * 16 + p;
+  }
+};
+
+// Dynamic shared memory of a fused pass: the exchange rows, the stage twiddle
+// table, the pass axis' own tables, THREADS x E per-thread save slots (drift
+// and Poisson passes) and the landing buffer.
+template <int N, bool CONTIG, int MODE> struct FusedSmem {
+  using SH = PassShape<N, CONTIG>;
+  static constexpr bool DRIFTS = MODE == M_KICK || MODE == M_DRIFT || MODE == M_DRIFT_DENSITY;
+  static constexpr bool LANDS = MODE != M_DEPOSIT;
+  static constexpr bool SAVES = DRIFTS || MODE == M_POISSON;
+  static constexpr size_t a16(size_t x) { return (x + 15) & ~(size_t)15; }
+  // per-axis tables: the drift propagator (N complex) or k and k~ (2 N floats)
+  static constexpr size_t TAB_BYTES = DRIFTS ? N * sizeof(float2) : (MODE == M_POISSON ? 2 * N * sizeof(float) : 0);
+  static constexpr size_t TW = a16(SH::template smem_bytes<float2>());
+  static constexpr size_t TAB = a16(TW + (size_t)stage_tw_size<N>() * sizeof(float2));
+  static constexpr size_t SAVE = a16(TAB + TAB_BYTES);
+  static constexpr size_t LAND =
+      a16(SAVE + (SAVES ? (size_t)SH::THREADS * SH::E * sizeof(float2) : 0));
+  // + slack to round the landing buffer up to a 128-byte boundary (tensor copies)
+  static constexpr size_t TOTAL = LAND + (LANDS ? Landing<N, CONTIG>::BYTES + 128 : 0);
+};
+template <int N, bool CONTIG, int MODE>
+__host__ __device__ constexpr size_t fused_smem_bytes() {
+  return FusedSmem<N, CONTIG, MODE>::TOTAL;
+}
+
+// The input fields a pass streams, in order of use.
+template <int MODE> __host__ __device__ constexpr int stream_count() {
+  return MODE == M_KICK ? 3 : (MODE == M_IFFT2 ? 2 : (MODE == M_DEPOSIT ? 0 : 1));
+}
+template <int MODE>
+__host__ __device__ __forceinline__ const float2 *stream_field(const FusedArgs &a, int f) {
+  if constexpr (MODE == M_KICK) return f == 0 ? a.S2 : (f == 1 ? a.S1 : a.psi);
+  if constexpr (MODE == M_IFFT2) return f == 0 ? a.S1 : a.S2;
+  if constexpr (MODE == M_FFT_FWD || MODE == M_POISSON) return a.R;
+  return a.psi;
+}
+
+// Strided passes: one tiled tensor map per streamed field, over the
+// (z, y, x, box) array of complex64 (8-byte elements), whose box is 16 z by
+// up to 256 rows along the pass axis.  One copy instruction then brings a
+// whole tile (two for n = 512).
+struct TileMaps {
+  CUtensorMap m[3];
+};
+
+__device__ __forceinline__ unsigned smem_addr(const void *p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// Bounded wait for phase `parity` of the landing barrier: gives up after 2 s
+// (or 2^24 polls) and returns false, so a copy that never completes cannot
+// hang the GPU.
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long *bar, unsigned parity) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  for (unsigned i = 0; i < (1u << 24); ++i) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if (global_ns() - t0 > 2000000000ull) break;
+  }
+  return false;
+}
+
+template <bool CONTIG>
+__device__ __forceinline__ long long tile_origin(const FusedArgs &a, int tile, int TP) {
+  if (CONTIG) return (long long)tile * TP * a.nz;
+  return (long long)(tile / a.ztiles) * a.outer_stride + (long long)(tile % a.ztiles) * 16;
+}
+
+// Start the copies of streamed field f's tile into the landing buffer (warp
+// 0 only).  Contiguous tiles: one bulk copy per pencil row.  Strided tiles:
+// the field's tensor map, coordinates (z0, y, x, box) with the pass axis
+// starting at row h.
+template <int N, bool CONTIG, int MODE>
+__device__ __forceinline__ void issue_tile(const FusedArgs &a, const TileMaps &maps, int f, int tile,
+                                           float2 *land, unsigned long long *bar) {
+  using L = Landing<N, CONTIG>;
+  constexpr int T = PassShape<N, CONTIG>::THREADS;
+  constexpr unsigned MASK = T >= 32 ? 0xffffffffu : ((1u << T) - 1u);
+  const int lane = threadIdx.x & 31;
+  if (lane == 0) {
+    // order the buffer's earlier generic-proxy reads before the async writes
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect_tx(bar, L::TX);
+  }
+  if constexpr (CONTIG) {
+    __syncwarp(MASK);
+    const float2 *fld = stream_field<MODE>(a, f);
+    const long long o = tile_origin<CONTIG>(a, tile, PassShape<N, CONTIG>::TP);
+    for (int r = lane; r < L::ROWS; r += 32) {
+      const float2 *src = fld + o + (long long)r * a.nz;
+      asm volatile(
+          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+              smem_addr(land + r * L::ROW_STRIDE)),
+          "l"(src), "r"((unsigned)(L::ROW_ELEMS * sizeof(float2))), "r"(smem_addr(bar))
+          : "memory");
     }
   } else {
-    for (int i = tid; i < N; i += SH::THREADS) {
-      const int o = blk / a.ztiles;
-      const float2 *row = f + (long long)o * a.outer_stride + (blk % a.ztiles) * 16 + (long long)i * a.stride;
-      asm volatile("cp.async.bulk.prefetch.L2.global [%0], 128;" ::"l"(row) : "memory");
+    if (lane == 0) {
+      const int z0 = (tile % a.ztiles) * 16, o = tile / a.ztiles, box = blockIdx.y;
+      const unsigned long long map = reinterpret_cast<unsigned long long>(&maps.m[f]);
+#pragma unroll
+      for (int h = 0; h < N; h += 256) {
+        const int cy = a.axis == 0 ? o : h, cx = a.axis == 0 ? h : o;
+        asm volatile(
+            "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+            " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(smem_addr(land + h * 16)),
+            "l"(map), "r"(z0), "r"(cy), "r"(cx), "r"(box), "r"(smem_addr(bar))
+            : "memory");
+      }
     }
   }
 }
 
+// Take the current field's tile from the landing buffer: wait for it, copy
+// this thread's elements (and element 0 of its pencil, c0), release the
+// buffer to the next copy and start that copy.  Returns false on every
+// thread of the CTA if the wait gave up (the error word is set).
+template <int N, bool CONTIG, int MODE, int E>
+__device__ __forceinline__ bool take_tile(float2 (&v)[E], float2 &c0, const FusedArgs &a,
+                                          const TileMaps &maps, float2 *land,
+                                          unsigned long long *bar, unsigned &parity, int &f, int tile,
+                                          int p, int t) {
+  using L = Landing<N, CONTIG>;
+  constexpr int P = N / E, NF = stream_count<MODE>();
+  bool ok = mbar_wait_bounded(bar, parity);
+  if (ok) {
+#pragma unroll
+    for (int e = 0; e < E; ++e) v[e] = land[L::idx(p, t + P * e)];
+    c0 = land[L::idx(p, 0)];
+  }
+  ok = __syncthreads_and(ok);
+  parity ^= 1u;
+  if (!ok) {
+    if (threadIdx.x == 0 && a.err) atomicOr(a.err, 1u);
+    return false;
+  }
+  int nf = f + 1, nt = tile;
+  if (nf == NF) {
+    nf = 0;
+    nt = tile + gridDim.x;
+  }
+  f = nf;
+  if (nt < a.ntiles && threadIdx.x < 32) issue_tile<N, CONTIG, MODE>(a, maps, nf, nt, land, bar);
+  return true;
+}
+
 template <int N, bool CONTIG, int MODE>
 __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CONTIG>::MINB)
-    k_fused(FusedArgs a) {
+    k_fused(FusedArgs a, const __grid_constant__ TileMaps maps) {
   select_box(a);
-  if (a.ahead > 0 && (int)blockIdx.x + a.ahead < (int)gridDim.x) {
-    const int nb = blockIdx.x + a.ahead;
-    if constexpr (MODE == M_DENSITY || MODE == M_DRIFT || MODE == M_DRIFT_DENSITY) {
-      prefetch_tile<N, CONTIG>(a.psi, a, nb);
-    } else if constexpr (MODE == M_FFT_FWD || MODE == M_POISSON) {
-      prefetch_tile<N, CONTIG>(a.R, a, nb);
-    } else if constexpr (MODE == M_IFFT2) {
-      prefetch_tile<N, CONTIG>(a.S1, a, nb);
-      prefetch_tile<N, CONTIG>(a.S2, a, nb);
-    } else if constexpr (MODE == M_KICK) {
-      prefetch_tile<N, CONTIG>(a.S1, a, nb);
-      prefetch_tile<N, CONTIG>(a.S2, a, nb);
-      prefetch_tile<N, CONTIG>(a.psi, a, nb);
-    }
-  }
   using SH = PassShape<N, CONTIG>;
+  using LAY = FusedSmem<N, CONTIG, MODE>;
   constexpr int E = SH::E, P = SH::P, TP = SH::TP, THREADS = SH::THREADS;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   float2 *sm = reinterpret_cast<float2 *>(smem_raw);
+  float2 *tw_s = reinterpret_cast<float2 *>(smem_raw + LAY::TW);
+  float2 *save = reinterpret_cast<float2 *>(smem_raw + LAY::SAVE);  // per-thread slots
+  float2 *tab2 = reinterpret_cast<float2 *>(smem_raw + LAY::TAB);  // drift propagator
+  float *tabk = reinterpret_cast<float *>(smem_raw + LAY::TAB);    // Poisson: k, then k~
+  float2 *land = reinterpret_cast<float2 *>(
+      smem_raw + ((LAY::LAND + smem_addr(smem_raw) + 127) & ~(size_t)127) - smem_addr(smem_raw));
   __shared__ double red[(THREADS + 31) / 32 + 1];
+  __shared__ __align__(8) unsigned long long lbar;
 
   const int tid = threadIdx.x;
   int p, t;
@@ -450,8 +613,6 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CO
     p = tid % TP;
     t = tid / TP;
   }
-  const PencilPos pp = pencil_pos<CONTIG>(a, p, TP);
-  const long long base = pp.base, st = a.stride;
   using SMV = typename std::conditional<CONTIG, SmemContig<float2>, SmemStrided<float2, TP>>::type;
   SMV smv;
   if constexpr (CONTIG)
@@ -459,134 +620,199 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CO
   else
     smv.base = sm + p;
   // the stage twiddle table of this axis, staged after the exchange rows
-  float2 *tw_s = sm + SH::template smem_bytes<float2>() / sizeof(float2);
   for (int i = tid; i < stage_tw_size<N>(); i += THREADS) tw_s[i] = a.tw[i];
+  if constexpr (LAY::DRIFTS) {
+    for (int i = tid; i < N; i += THREADS) tab2[i] = a.prop[i];
+  } else if constexpr (MODE == M_POISSON) {
+    for (int i = tid; i < N; i += THREADS) {
+      tabk[i] = a.k[a.axis][i];
+      tabk[N + i] = a.kt[a.axis][i];
+    }
+  }
+  if (tid == 0) mbar_init(&lbar, 1);
   __syncthreads();
   const float2 *tw = tw_s;
-  float2 *save = tw_s + stage_tw_size<N>();  // drift passes: per-thread slots
+  unsigned parity = 0;
+  int fld = 0;
+  if constexpr (LAY::LANDS)
+    if ((int)blockIdx.x < a.ntiles && tid < 32)
+      issue_tile<N, CONTIG, MODE>(a, maps, 0, blockIdx.x, land, &lbar);
 
-  if constexpr (MODE == M_DENSITY) {
-    float2 v[E];
-    load_pencil<E>(v, a.psi, base, st, t, P);
-    double s = build_density<N, E>(v, a, pp, t, P);
-    s = block_sum<THREADS>(s, red);
-    if (tid == 0) a.part[blockIdx.x] = s;
-    fft_pencil<N, -1, true>(v, t, smv, tw);
-    store_pencil<E>(v, a.R, base, st, t, P);
-  } else if constexpr (MODE == M_FFT_FWD) {
-    float2 v[E];
-    load_pencil<E>(v, a.R, base, st, t, P);
-    fft_pencil<N, -1, true>(v, t, smv, tw);
-    store_pencil<E>(v, a.R, base, st, t, P);
-  } else if constexpr (MODE == M_POISSON) {
-    float2 v[E];
-    load_pencil<E>(v, a.R, base, st, t, P);
-    // Mean density in float64 for the k = 0 mode (pencil 0 of CTA 0 only).
-    double mean = 0.0;
-    if (blockIdx.x == 0) {
-      double s = 0.0;
-      for (int i = tid; i < a.n_part; i += THREADS) s += a.part_in[i];
-      mean = block_sum<THREADS>(s, red) * a.inv_ncell;
-    }
-    fft_pencil<N, -1, true>(v, t, smv, tw);
-    const int ax = a.axis;            // r: 0 or 2
-    const int aq = 2 - ax;            // the other non-y axis
-    const float kq2 = a.k[aq][pp.c[aq]] * a.k[aq][pp.c[aq]];
-    const float ky = a.k[1][pp.c[1]];
-    const float kperp2 = kq2 + ky * ky;
-    const float ktq = a.kt[aq][pp.c[aq]], kty = a.kt[1][pp.c[1]];
-    const float g0 = (float)(-a.fourpiG * a.inv_ncell);
-    float2 w[E];
-#pragma unroll
-    for (int e = 0; e < E; ++e) {
-      const int i = t + P * e;
-      const float kr = a.k[ax][i];
-      const float k2 = kperp2 + kr * kr;
-      float2 vh;
-      if (k2 == 0.0f) {
-        // V^(0) = -4 pi G (sum rho - ncell rho_bar) / 1, scaled by 1/ncell
-        vh = float2{(float)(-a.fourpiG * (mean - a.rho_bar)), 0.0f};
-      } else {
-        const float g = g0 / k2;
-        vh = float2{v[e].x * g, v[e].y * g};
+  for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
+    const PencilPos pp = pencil_pos<CONTIG>(a, tile, p, TP);
+    const long long base = pp.base, st = a.stride;
+    float2 c0;
+#define QJ_TAKE(v) \
+  if (!take_tile<N, CONTIG, MODE, E>(v, c0, a, maps, land, &lbar, parity, fld, tile, p, t)) return
+
+    if constexpr (MODE == M_DENSITY) {
+      float2 v[E];
+      QJ_TAKE(v);
+      double s = build_density<N, E>(v, a, pp, t, P);
+      s = block_sum<THREADS>(s, red);
+      if (tid == 0) a.part[tile] = s;
+      fft_pencil<N, -1, true>(v, t, smv, tw);
+      store_pencil<E>(v, a.R, base, st, t, P);
+    } else if constexpr (MODE == M_FFT_FWD) {
+      float2 v[E];
+      QJ_TAKE(v);
+      fft_pencil<N, -1, true>(v, t, smv, tw);
+      store_pencil<E>(v, a.R, base, st, t, P);
+    } else if constexpr (MODE == M_POISSON) {
+      float2 v[E];
+      QJ_TAKE(v);
+      // Mean density in float64 for the k = 0 mode (tile 0 only).
+      double mean = 0.0;
+      if (tile == 0) {
+        double s = 0.0;
+        for (int i = tid; i < a.n_part; i += THREADS) s += a.part_in[i];
+        mean = block_sum<THREADS>(s, red) * a.inv_ncell;
       }
-      const float f1 = 1.0f + a.kt[ax][i];
-      v[e] = float2{vh.x * f1, vh.y * f1};
-      // (kty - i ktq) * vh
-      w[e] = float2{kty * vh.x + ktq * vh.y, kty * vh.y - ktq * vh.x};
-    }
-    fft_pencil<N, +1, true>(v, t, smv, tw);
-    store_pencil<E>(v, a.S1, base, st, t, P);
-    fft_pencil<N, +1, true>(w, t, smv, tw);
-    store_pencil<E>(w, a.S2, base, st, t, P);
-  } else if constexpr (MODE == M_IFFT2) {
-    float2 v[E];
-    load_pencil<E>(v, a.S1, base, st, t, P);
-    fft_pencil<N, +1, true>(v, t, smv, tw);
-    store_pencil<E>(v, a.S1, base, st, t, P);
-    load_pencil<E>(v, a.S2, base, st, t, P);
-    fft_pencil<N, +1, true>(v, t, smv, tw);
-    store_pencil<E>(v, a.S2, base, st, t, P);
-  } else if constexpr (MODE == M_KICK) {
-    const int aq = a.axis;  // the kick axis; ar = 2 - aq is the Poisson axis
-    const unsigned gb = (unsigned)base + (unsigned)t * (unsigned)st, gs = (unsigned)P * (unsigned)st;
-    float am = 0.0f;
-    float V[E];
-    {
-      // phase 1: S1 -> V + i a_r
-      float2 v1[E];
-      load_pencil<E>(v1, a.S1, base, st, t, P);
-      fft_pencil<N, +1, true>(v1, t, smv, tw);
+      fft_pencil<N, -1, true>(v, t, smv, tw);
+      const int ax = a.axis;  // r: 0 or 2
+      const int aq = 2 - ax;  // the other non-y axis
+      const float kq2 = a.k[aq][pp.c[aq]] * a.k[aq][pp.c[aq]];
+      const float ky = a.k[1][pp.c[1]];
+      const float kperp2 = kq2 + ky * ky;
+      const float ktq = a.kt[aq][pp.c[aq]], kty = a.kt[1][pp.c[1]];
+      const float g0 = (float)(-a.fourpiG * a.inv_ncell);
 #pragma unroll
       for (int e = 0; e < E; ++e) {
-        V[e] = v1[e].x;
-        am = fmaxf(am, fabsf(v1[e].y));
+        const int i = t + P * e;
+        const float kr = tabk[i];
+        const float k2 = kperp2 + kr * kr;
+        float2 vh;
+        if (k2 == 0.0f) {
+          // V^(0) = -4 pi G (sum rho - ncell rho_bar) / 1, scaled by 1/ncell
+          vh = float2{(float)(-a.fourpiG * (mean - a.rho_bar)), 0.0f};
+        } else {
+          const float g = g0 / k2;
+          vh = float2{v[e].x * g, v[e].y * g};
+        }
+        const float f1 = 1.0f + tabk[N + i];
+        v[e] = float2{vh.x * f1, vh.y * f1};
+        // (kty - i ktq) * vh waits in the thread's save slots
+        save[e * THREADS + tid] = float2{kty * vh.x + ktq * vh.y, kty * vh.y - ktq * vh.x};
       }
-      if (a.has_stars)
-        for_star_corners<N, false>(a, star_ranges(a, pp), t, P,
-                                   [&](unsigned s, int cbits, int m, float, float, float, float) {
-                                     const float ar_ = reg_get<E>(v1, m / P).y;
-                                     a.A[3 * (8 * s + c_corner_of_bits_dev(cbits)) + (aq == 0 ? 2 : 0)] = ar_;
-                                   });
-      if (a.gv[0]) {  // gas half kick, quantum-gas-bh.py:255-266
-        float *g = a.gv[aq == 0 ? 2 : 0];
+      fft_pencil<N, +1, true>(v, t, smv, tw);
+      store_pencil<E>(v, a.S1, base, st, t, P);
 #pragma unroll
-        for (int e = 0; e < E; ++e) g[gb + e * gs] = g[gb + e * gs] + v1[e].y * a.gas_dt;
-      }
-    }
-    {
-      // phase 2: S2 -> a_q + i a_y
-      float2 v2[E];
-      load_pencil<E>(v2, a.S2, base, st, t, P);
-      fft_pencil<N, +1, true>(v2, t, smv, tw);
+      for (int e = 0; e < E; ++e) v[e] = save[e * THREADS + tid];
+      fft_pencil<N, +1, true>(v, t, smv, tw);
+      store_pencil<E>(v, a.S2, base, st, t, P);
+    } else if constexpr (MODE == M_IFFT2) {
+      float2 v[E];
+      QJ_TAKE(v);
+      fft_pencil<N, +1, true>(v, t, smv, tw);
+      store_pencil<E>(v, a.S1, base, st, t, P);
+      QJ_TAKE(v);
+      fft_pencil<N, +1, true>(v, t, smv, tw);
+      store_pencil<E>(v, a.S2, base, st, t, P);
+    } else if constexpr (MODE == M_KICK) {
+      const int aq = a.axis;  // the kick axis; ar = 2 - aq is the Poisson axis
+      const unsigned gb = (unsigned)base + (unsigned)t * (unsigned)st, gs = (unsigned)P * (unsigned)st;
+      float am = 0.0f;
+      float V[E];
+      {
+        // phase 1: S2 -> a_q + i a_y
+        float2 v2[E];
+        QJ_TAKE(v2);
+        fft_pencil<N, +1, true>(v2, t, smv, tw);
 #pragma unroll
-      for (int e = 0; e < E; ++e) am = fmaxf(am, fmaxf(fabsf(v2[e].x), fabsf(v2[e].y)));
-      if (a.has_stars)
-        for_star_corners<N, false>(a, star_ranges(a, pp), t, P,
-                                   [&](unsigned s, int cbits, int m, float, float, float, float) {
-                                     const float2 w = reg_get<E>(v2, m / P);
-                                     float *dst = a.A + 3 * (8 * s + c_corner_of_bits_dev(cbits));
-                                     dst[aq] = w.x;
-                                     dst[1] = w.y;
-                                   });
-      if (a.gv[0]) {
-        float *gq = a.gv[aq], *gy = a.gv[1];
+        for (int e = 0; e < E; ++e) am = fmaxf(am, fmaxf(fabsf(v2[e].x), fabsf(v2[e].y)));
+        if (a.has_stars) {
+          // the corner lookups index the thread's save slots (free until the drift)
 #pragma unroll
-        for (int e = 0; e < E; ++e) {
-          gq[gb + e * gs] = gq[gb + e * gs] + v2[e].x * a.gas_dt;
-          gy[gb + e * gs] = gy[gb + e * gs] + v2[e].y * a.gas_dt;
+          for (int e = 0; e < E; ++e) save[e * THREADS + tid] = v2[e];
+          for_star_corners<N, false>(a, star_ranges(a, pp), t, P,
+                                     [&](unsigned s, int cbits, int m, float, float, float, float) {
+                                       const float2 w = save[(m / P) * THREADS + tid];
+                                       float *dst = a.A + 3 * (8 * s + c_corner_of_bits_dev(cbits));
+                                       dst[aq] = w.x;
+                                       dst[1] = w.y;
+                                     });
+        }
+        if (a.gv[0]) {
+          float *gq = a.gv[aq], *gy = a.gv[1];
+#pragma unroll
+          for (int e = 0; e < E; ++e) {
+            gq[gb + e * gs] = gq[gb + e * gs] + v2[e].x * a.gas_dt;
+            gy[gb + e * gs] = gy[gb + e * gs] + v2[e].y * a.gas_dt;
+          }
         }
       }
-    }
-    // phase 3: psi <- exp(-i c V) psi with V = Poisson + b rho + V_ext, then
-    // the drift along this axis
-    float2 ps[E];
-    load_pencil<E>(ps, a.psi, base, st, t, P);
-    if (a.b_coeff != 0.0f) {
-      // rho = |psi|^2 + rho_stars, the argument of get_potential (quantum-stars.py:193)
-      float rs[E];
+      {
+        // phase 2: S1 -> V + i a_r (V right before the kick that uses it)
+        float2 v1[E];
+        QJ_TAKE(v1);
+        fft_pencil<N, +1, true>(v1, t, smv, tw);
 #pragma unroll
-      for (int e = 0; e < E; ++e) rs[e] = 0.0f;
+        for (int e = 0; e < E; ++e) {
+          V[e] = v1[e].x;
+          am = fmaxf(am, fabsf(v1[e].y));
+        }
+        if (a.has_stars) {
+#pragma unroll
+          for (int e = 0; e < E; ++e) save[e * THREADS + tid].x = v1[e].y;
+          for_star_corners<N, false>(a, star_ranges(a, pp), t, P,
+                                     [&](unsigned s, int cbits, int m, float, float, float, float) {
+                                       a.A[3 * (8 * s + c_corner_of_bits_dev(cbits)) + (aq == 0 ? 2 : 0)] =
+                                           save[(m / P) * THREADS + tid].x;
+                                     });
+        }
+        if (a.gv[0]) {  // gas half kick, quantum-gas-bh.py:255-266
+          float *g = a.gv[aq == 0 ? 2 : 0];
+#pragma unroll
+          for (int e = 0; e < E; ++e) g[gb + e * gs] = g[gb + e * gs] + v1[e].y * a.gas_dt;
+        }
+      }
+      // phase 3: psi <- exp(-i c V) psi with V = Poisson + b rho + V_ext, then
+      // the drift along this axis
+      float2 ps[E];
+      QJ_TAKE(ps);
+      if (a.b_coeff != 0.0f) {
+        // rho = |psi|^2 + rho_stars, the argument of get_potential (quantum-stars.py:193);
+        // the star density of a cell is summed from zero in star order in the
+        // thread's save slots
+        float *rs = reinterpret_cast<float *>(save);
+#pragma unroll
+        for (int e = 0; e < E; ++e) rs[2 * (e * THREADS + tid)] = 0.0f;
+        if (a.has_stars)
+          for_star_corners<N, true>(a, star_ranges(a, pp), t, P,
+                                    [&](unsigned, int, int m, float wx, float wy, float wz, float fac) {
+                                      const float val = fmul_rn(fmul_rn(fmul_rn(wx, wy), wz), fac);
+                                      float &r = rs[2 * ((m / P) * THREADS + tid)];
+                                      r = fadd_rn(r, val);
+                                    });
+#pragma unroll
+        for (int e = 0; e < E; ++e)
+          V[e] = V[e] + a.b_coeff * (ps[e].x * ps[e].x + ps[e].y * ps[e].y + rs[2 * (e * THREADS + tid)]);
+      }
+      if (a.v_ext) {
+#pragma unroll
+        for (int e = 0; e < E; ++e) V[e] = V[e] + a.v_ext[gb + e * gs];
+      }
+#pragma unroll
+      for (int e = 0; e < E; ++e) ps[e] = phase_rotate(ps[e], a.kick_coef * (double)V[e]);
+      if (a.v_out) {
+#pragma unroll
+        for (int e = 0; e < E; ++e) a.v_out[gb + e * gs] = V[e];
+      }
+      if (a.do_drift) drift_pencil<N, E, P, THREADS>(ps, c0, a.prop, t, smv, tw, save);
+      store_pencil<E>(ps, a.psi, base, st, t, P);
+      if constexpr (THREADS >= 32) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) am = fmaxf(am, __shfl_xor_sync(0xffffffffu, am, o));
+        if ((tid & 31) == 0) atomic_max_nonneg(a.amax_bits, am);
+      } else {
+        atomic_max_nonneg(a.amax_bits, am);
+      }
+    } else if constexpr (MODE == M_DEPOSIT) {
+      // bin_stars (quantum-stars.py:212-247): every cell sums its star
+      // contributions from zero in star order
+      float acc[E];
+#pragma unroll
+      for (int e = 0; e < E; ++e) acc[e] = 0.0f;
       if (a.has_stars)
         for_star_corners<N, true>(a, star_ranges(a, pp), t, P,
                                   [&](unsigned, int, int m, float wx, float wy, float wz, float fac) {
@@ -594,65 +820,28 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CO
                                     const int e = m / P;
 #pragma unroll
                                     for (int qq = 0; qq < E; ++qq)
-                                      if (qq == e) rs[qq] = fadd_rn(rs[qq], val);
+                                      if (qq == e) acc[qq] = fadd_rn(acc[qq], val);
                                   });
+      const unsigned gb = (unsigned)base + (unsigned)t * (unsigned)st, gs = (unsigned)P * (unsigned)st;
 #pragma unroll
-      for (int e = 0; e < E; ++e)
-        V[e] = V[e] + a.b_coeff * (ps[e].x * ps[e].x + ps[e].y * ps[e].y + rs[e]);
+      for (int e = 0; e < E; ++e) a.rho_out[gb + e * gs] = acc[e];
+      (void)smv;
+      (void)tw;
+      (void)c0;
+    } else if constexpr (MODE == M_DRIFT || MODE == M_DRIFT_DENSITY) {
+      float2 v[E];
+      QJ_TAKE(v);
+      drift_pencil<N, E, P, THREADS>(v, c0, a.prop, t, smv, tw, save);
+      store_pencil<E>(v, a.psi, base, st, t, P);
+      if constexpr (MODE == M_DRIFT_DENSITY) {
+        double s = build_density<N, E>(v, a, pp, t, P);
+        s = block_sum<THREADS>(s, red);
+        if (tid == 0) a.part[tile] = s;
+        fft_pencil<N, -1, true>(v, t, smv, tw);
+        store_pencil<E>(v, a.R, base, st, t, P);
+      }
     }
-    if (a.v_ext) {
-#pragma unroll
-      for (int e = 0; e < E; ++e) V[e] = V[e] + a.v_ext[gb + e * gs];
-    }
-#pragma unroll
-    for (int e = 0; e < E; ++e) ps[e] = phase_rotate(ps[e], a.kick_coef * (double)V[e]);
-    if (a.v_out) {
-#pragma unroll
-      for (int e = 0; e < E; ++e) a.v_out[gb + e * gs] = V[e];
-    }
-    if (a.do_drift) {
-      // read before any thread of this pencil stores (the FFT's barriers order it)
-      const float2 c0 = a.psi[base];
-      drift_pencil<N, E, P, THREADS>(ps, c0, a.prop, t, smv, tw, save);
-    }
-    store_pencil<E>(ps, a.psi, base, st, t, P);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) am = fmaxf(am, __shfl_xor_sync(0xffffffffu, am, o));
-    if ((tid & 31) == 0) atomic_max_nonneg(a.amax_bits, am);
-  } else if constexpr (MODE == M_DEPOSIT) {
-    // bin_stars (quantum-stars.py:212-247): every cell sums its star
-    // contributions from zero in star order
-    float acc[E];
-#pragma unroll
-    for (int e = 0; e < E; ++e) acc[e] = 0.0f;
-    if (a.has_stars)
-      for_star_corners<N, true>(a, star_ranges(a, pp), t, P,
-                                [&](unsigned, int, int m, float wx, float wy, float wz, float fac) {
-                                  const float val = fmul_rn(fmul_rn(fmul_rn(wx, wy), wz), fac);
-                                  const int e = m / P;
-#pragma unroll
-                                  for (int qq = 0; qq < E; ++qq)
-                                    if (qq == e) acc[qq] = fadd_rn(acc[qq], val);
-                                });
-    const unsigned gb = (unsigned)base + (unsigned)t * (unsigned)st, gs = (unsigned)P * (unsigned)st;
-#pragma unroll
-    for (int e = 0; e < E; ++e) a.rho_out[gb + e * gs] = acc[e];
-    (void)smv;
-    (void)tw;
-  } else if constexpr (MODE == M_DRIFT || MODE == M_DRIFT_DENSITY) {
-    float2 v[E];
-    load_pencil<E>(v, a.psi, base, st, t, P);
-    // read before any thread of this pencil stores (the FFT's barriers order it)
-    const float2 c0 = a.psi[base];
-    drift_pencil<N, E, P, THREADS>(v, c0, a.prop, t, smv, tw, save);
-    store_pencil<E>(v, a.psi, base, st, t, P);
-    if constexpr (MODE == M_DRIFT_DENSITY) {
-      double s = build_density<N, E>(v, a, pp, t, P);
-      s = block_sum<THREADS>(s, red);
-      if (tid == 0) a.part[blockIdx.x] = s;
-      fft_pencil<N, -1, true>(v, t, smv, tw);
-      store_pencil<E>(v, a.R, base, st, t, P);
-    }
+#undef QJ_TAKE
   }
 }
 
@@ -673,7 +862,7 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS) k_fft(FftArgs a
   using C = cplx<R>;
   using SH = PassShape<N, CONTIG>;
   constexpr int E = SH::E, P = SH::P, TP = SH::TP;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   C *sm = reinterpret_cast<C *>(smem_raw);
   const int tid = threadIdx.x;
   int p, t;

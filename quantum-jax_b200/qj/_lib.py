@@ -69,6 +69,7 @@ SIGNATURES = {
     "qj_get_potential_f32_noalloc": (c_int, [ctypes.POINTER(QjGrid), ctypes.POINTER(QjPhys),
                                              c_void_p, c_void_p, c_int, c_void_p]),
     "qj_plan_workspace_bytes": (c_int64, [c_void_p]),
+    "qj_plan_status": (c_int, [c_void_p]),
     "qj_launch_count": (c_int64, []),
     "qj_profile_enable": (c_int, [c_int]),
     "qj_profile_read": (c_int, [ctypes.POINTER(c_double), ctypes.POINTER(c_int64), c_int]),

@@ -119,6 +119,11 @@ class Plan:
     def workspace_bytes(self):
         return int(lib().qj_plan_workspace_bytes(self._h))
 
+    def status(self):
+        """Wait for the device; raise if a fused pass of this plan gave up a
+        bounded wait for a tile copy since the last call."""
+        check(lib().qj_plan_status(self._h))
+
     # ----- argument checks -----
     def _field(self, t, name, complex_=False):
         dt = self.cdtype if complex_ else self.rdtype

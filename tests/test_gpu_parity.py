@@ -122,7 +122,7 @@ def run_qj(g, p, psi, pos, vel, dt, nsteps, precision, chunks=1, si=False, v_ext
     vx = cuda(v_ext, rt) if v_ext is not None else None
     for c in range(chunks):
         plan.kdk_step(ps, po, ve, diag, dt, nsteps // chunks, p.m_s, si, vx)
-    torch.cuda.synchronize()
+    plan.status()  # no fused pass gave up a bounded tile wait
     out = (ps.cpu().numpy(), po.cpu().numpy() if po is not None else pos,
            ve.cpu().numpy() if ve is not None else vel, diag.cpu().numpy())
     plan.close()
