@@ -61,6 +61,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--no-gas", action="store_true")
+    ap.add_argument("--gas-n", type=int, default=128)
+    ap.add_argument("--gas-steps", type=int, default=500)
     ap.add_argument("--ens-steps", type=int, default=100)
     ap.add_argument("--ens-chunk", type=int, default=10)
     ap.add_argument("--adj-n", type=int, default=128)
@@ -155,6 +158,84 @@ def make_ic(n, n_s):
 
     psi, pos, vel, g, p = O.stars_ic(n, n_s, seed=0)
     return psi, pos, vel, g, p, O.default_dt(g, p)
+
+
+def gas_bh_leg(a, dev, stream, barrier):
+    """Gas + black-hole step at gas_n^3: psi = sqrt(1 + 0.1 delta), isothermal gas
+    rho = 0.2 (1 + 0.05 delta'), v = 0, c_s = 1; one black hole at the box centre
+    with 1 % of the box mass, Bondi sink radius 2 cells; dt = min(dx^2/6,
+    0.3 dx / (c_s + |v|max)).  The speed of light keeps the reference's c / c_s
+    (299792.458 / 20).  Fused float32 against the plain float64 path after the
+    same steps; the total mass counts psi, gas and the black hole."""
+    import numpy as np
+    import torch
+
+    import qj
+    from oracle import oracle as O
+
+    n, steps = a.gas_n, a.gas_steps
+    dx = 1.0 / n
+    rho_dm = 1.0 + 0.1 * O.delta_field(n, 0)
+    rho_g = 0.2 * (1.0 + 0.05 * O.delta_field(n, 1))
+    vol = dx ** 3
+    m_bh0 = 0.01 * (rho_dm.sum() + rho_g.sum()) * vol
+    dt = min(dx * dx / 6.0, 0.3 * dx / (1.0 + 0.0))
+    phys = qj.Phys(m_per_hbar=1.0, G=1.0 / (4.0 * np.pi), rho_bar=float(rho_dm.mean()), cs=1.0,
+                   c_light=299792.458 / 20.0)
+    out, ms = {}, {}
+    for prec, name in ((qj.FUSED_F32, "fused"), (qj.PLAIN_F64, "plain")):
+        ct = torch.complex64 if prec == qj.FUSED_F32 else torch.complex128
+        rt = torch.float32 if prec == qj.FUSED_F32 else torch.float64
+        plan = qj.Plan(qj.Grid(n, n, n), phys, prec, 1)
+
+        def state():
+            return [torch.as_tensor(np.sqrt(rho_dm), dtype=ct, device=dev).contiguous(),
+                    torch.as_tensor(rho_g, dtype=rt, device=dev).contiguous(),
+                    torch.zeros((n, n, n), dtype=rt, device=dev),
+                    torch.zeros((n, n, n), dtype=rt, device=dev),
+                    torch.zeros((n, n, n), dtype=rt, device=dev),
+                    torch.tensor([m_bh0], dtype=rt, device=dev),
+                    torch.tensor([[0.5, 0.5, 0.5]], dtype=rt, device=dev),
+                    torch.zeros((1, 3), dtype=rt, device=dev)]
+
+        w = state()
+        plan.kdk_gas_bh(*w, dt, 3, 0.0, bondi_r_acc_mult=2.0)  # warm-up
+        st = state()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier()
+        e0.record(stream)
+        plan.kdk_gas_bh(*st, dt, steps, 0.0, bondi_r_acc_mult=2.0)
+        e1.record(stream)
+        barrier()
+        ms[name] = e0.elapsed_time(e1)
+        plan.status()
+        out[name] = [x.to(torch.complex128 if x.is_complex() else torch.float64) for x in st]
+        plan.close()
+        del w, st
+
+    def rel(x, y):
+        return float(torch.linalg.vector_norm(x - y) / torch.linalg.vector_norm(y))
+
+    f, p = out["fused"], out["plain"]
+    mass0 = (rho_dm.sum() + rho_g.sum()) * vol + m_bh0
+
+    def mass(s):
+        return float(((s[0].abs() ** 2).sum() + s[1].sum()) * vol + s[5].sum())
+
+    cells = n ** 3
+    return {"workload": f"gas + black hole {n}^3 (psi complex64, gas rho + 3 velocities "
+                        f"float32), Bondi sink radius 2 cells", "steps": steps, "dt": dt,
+            "fused_cell_steps_per_s": cells * steps / (ms["fused"] * 1e-3),
+            "plain_f64_cell_steps_per_s": cells * steps / (ms["plain"] * 1e-3),
+            "fused_over_plain": ms["plain"] / ms["fused"],
+            "psi_rel_l2_vs_f64": rel(f[0], p[0]),
+            "rho_dm_rel_l2_vs_f64": rel(f[0].abs() ** 2, p[0].abs() ** 2),
+            "gas_rho_rel_l2_vs_f64": rel(f[1], p[1]),
+            "gas_v_rel_l2_vs_f64": rel(torch.stack(f[2:5]), torch.stack(p[2:5])),
+            "m_bh_rel_vs_f64": float(abs(f[5] - p[5]).max() / abs(p[5]).max()),
+            "mass_drift_fused": mass(f) / mass0 - 1.0,
+            "mass_drift_f64": mass(p) / mass0 - 1.0,
+            "l2_resident": "yes (fields of 8-16 MiB): not HBM-bound"}
 
 
 def cpu_baseline(n, n_s, steps=2):
@@ -511,6 +592,11 @@ def main():
         for pl in plans + singles:
             pl.close()
 
+    # ---------------- gas + black hole, 128^3 (quantum-gas-bh.py:537-578) ------
+    gas_bh = None
+    if not a.no_gas:
+        gas_bh = gas_bh_leg(a, dev, stream, barrier)
+
     cb = None
     if rank == 0 and world == 1 and not a.no_cpu:
         cb = cpu_baseline(n, n_s, 2)
@@ -535,7 +621,7 @@ def main():
                              "f64_path": "plain float64 GPU path (matches the oracle to 1e-11)"},
                 "roofline": roofline, "step_roofline": step_roof, "passes": per_pass,
                 "gpu_launches": launches, "clocks": clk, "e2e": e2e, "cpu_baseline": cb,
-                "adjoint": adjoint, "ensemble": ensemble}
+                "adjoint": adjoint, "ensemble": ensemble, "gas_bh": gas_bh}
         print(json.dumps(line), flush=True)
     fused.close()
     if dist is not None:
