@@ -146,7 +146,7 @@ struct qj_plan {
   unsigned *err = nullptr;  // set by a fused pass whose bounded tile wait gave up
   void *tmp_scalar = nullptr;
   void *tmp_diag = nullptr;
-  void *gas_out[4] = {nullptr, nullptr, nullptr, nullptr};  // hydro output scratch
+  void *gas_prim = nullptr;  // hydro: 16 values per cell (limited gradients, predicted primitives)
   // adjoint: recomputed chunk states
   void *adj_psi = nullptr, *adj_states = nullptr, *adj_V = nullptr;
   int adj_cap = 0;
@@ -584,20 +584,14 @@ struct GasArgs {
 };
 
 int ensure_gas_ws(qj_plan *P) {
-  for (int i = 0; i < 4; ++i)
-    if (!P->gas_out[i]) QJ_TRY(dev_alloc(P, &P->gas_out[i], P->ncell * P->rsz));
+  if (!P->gas_prim) QJ_TRY(dev_alloc(P, &P->gas_prim, 16 * P->ncell * P->rsz));
   return 0;
 }
 
 int gas_hydro(qj_plan *P, const GasArgs &g, cudaStream_t st) {
   const double dx = P->g.Lx / P->n[0];
-  QJ_TRY(launch_hydro(P->dbl, g.rho, g.v[0], g.v[1], g.v[2], P->gas_out[0], P->gas_out[1],
-                      P->gas_out[2], P->gas_out[3], P->n[0], dx, g.dt, P->ph.cs,
-                      (g.bondi > 0 && g.n_bh > 0) ? 1 : 0, st));
-  void *dst[4] = {g.rho, g.v[0], g.v[1], g.v[2]};
-  for (int i = 0; i < 4; ++i)
-    QJ_CK(cudaMemcpyAsync(dst[i], P->gas_out[i], P->ncell * P->rsz, cudaMemcpyDeviceToDevice, st));
-  return 0;
+  return launch_hydro(P->dbl, g.rho, g.v[0], g.v[1], g.v[2], P->gas_prim, P->n[0], dx, g.dt,
+                      P->ph.cs, (g.bondi > 0 && g.n_bh > 0) ? 1 : 0, st);
 }
 
 int fused_gas_step(qj_plan *P, const GasArgs &g, cudaStream_t st) {

@@ -251,8 +251,10 @@ template <int N, bool CONTIG> struct PassShape {
   static constexpr int P = N / E;
   static constexpr int TP = CONTIG ? (P >= 256 ? 1 : 256 / P) : 16;
   static constexpr int THREADS = TP * P;
-  // resident CTAs per SM requested from the register allocator
-  static constexpr int MINB = THREADS <= 256 ? 2 : 1;
+  // resident CTAs per SM requested from the register allocator: enough for
+  // a budget of 128 registers per thread (2 x 256, 4 x 128, ... threads)
+  static constexpr int MINB0 = 65536 / (THREADS * 128);
+  static constexpr int MINB = MINB0 < 1 ? 1 : (MINB0 > 16 ? 16 : MINB0);
   static constexpr int ROW = N + N / 16;  // padded contiguous row
   template <typename C> static constexpr size_t smem_bytes() {
     return CONTIG ? (size_t)TP * ROW * sizeof(C) : (size_t)TP * N * sizeof(C);

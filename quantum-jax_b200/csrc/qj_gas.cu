@@ -1,14 +1,13 @@
 // Isothermal gas and black-hole kernels (quantum-gas-bh.py, quantum-bh.py,
 // quantum-fluid-accretion-test.py), templated on the real type.
 //
-// k_hydro is one MUSCL-Hancock update of solve_hydro (quantum-gas-bh.py:269-337)
-// per cell.  The reference computes whole-grid arrays (gradients, limited
-// gradients, predicted primitives, face states, fluxes) with jnp.roll; here a
-// thread evaluates, for its cell and its six face neighbours, the limited
-// gradients and predicted primitives from the raw fields (read through L1),
-// then the fluxes through its six faces and the flux-form update, in the same
-// floating-point order as the reference.  The grid is cubic with spacing dx,
-// as in the reference.
+// One MUSCL-Hancock update of solve_hydro (quantum-gas-bh.py:269-337) is two
+// kernels, like the reference's whole-grid arrays: k_hydro_prim stores every
+// cell's limited gradients and half-step primitives (16 values per cell,
+// structure of arrays); k_hydro_update reads its cell's and its six face
+// neighbours' records, forms the fluxes through its six faces and applies the
+// flux-form update in place, in the same floating-point order as the
+// reference.  The grid is cubic with spacing dx, as in the reference.
 #include <cmath>
 
 #include "../../include/qj.h"
@@ -23,13 +22,14 @@ template <typename R> struct Prim {
   R g[4][3];   // limited gradients of rho, vx, vy, vz along x, y, z
 };
 
+// Periodic index of a cell at most one cell outside [0, n) on each axis.
 struct Idx3 {
   int n;
+  __device__ __forceinline__ static int wrap1(int x, int n) {
+    return x < 0 ? x + n : (x >= n ? x - n : x);
+  }
   __device__ __forceinline__ long long at(int x, int y, int z) const {
-    x = (x % n + n) % n;
-    y = (y % n + n) % n;
-    z = (z % n + n) % n;
-    return ((long long)x * n + y) * n + z;
+    return ((long long)wrap1(x, n) * n + wrap1(y, n)) * n + wrap1(z, n);
   }
 };
 
@@ -120,18 +120,47 @@ __device__ void face_flux(const Prim<R> &L, const Prim<R> &Rt, int d, R dx, R cs
   }
 }
 
+// Record of one cell: P[k * ncell + i], k = f[0..3] then g[v][d] at 4 + 3 v + d.
 template <typename R>
-__global__ void __launch_bounds__(128)
-    k_hydro(const R *rho, const R *vx, const R *vy, const R *vz, R *orho, R *ovx, R *ovy, R *ovz,
-            int n, R dx, R dt, R cs, R vol, R fac, int clamp_rho) {
+__global__ void __launch_bounds__(256)
+    k_hydro_prim(const R *rho, const R *vx, const R *vy, const R *vz, R *P, int n, R dx, R dt, R cs) {
   const long long ncell = (long long)n * n * n;
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i >= ncell) return;
   const int z = (int)(i % n), y = (int)((i / n) % n), x = (int)(i / ((long long)n * n));
   const R *const F[4] = {rho, vx, vy, vz};
+  const Prim<R> C = cell_prim(F, Idx3{n}, x, y, z, dx, dt, cs);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) P[k * ncell + i] = C.f[k];
+#pragma unroll
+  for (int v = 0; v < 4; ++v)
+#pragma unroll
+    for (int d = 0; d < 3; ++d) P[(4 + 3 * v + d) * ncell + i] = C.g[v][d];
+}
+
+// the primitives and the axis-d gradients of cell j (what face_flux uses)
+template <typename R>
+__device__ __forceinline__ void load_face_prim(const R *P, long long ncell, long long j, int d,
+                                               Prim<R> &q) {
+#pragma unroll
+  for (int k = 0; k < 4; ++k) q.f[k] = P[k * ncell + j];
+#pragma unroll
+  for (int v = 0; v < 4; ++v) q.g[v][d] = P[(4 + 3 * v + d) * ncell + j];
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256)
+    k_hydro_update(R *rho, R *vx, R *vy, R *vz, const R *P, int n, R dx, R cs, R vol, R fac,
+                   int clamp_rho) {
+  const long long ncell = (long long)n * n * n;
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= ncell) return;
+  const int z = (int)(i % n), y = (int)((i / n) % n), x = (int)(i / ((long long)n * n));
   const Idx3 I{n};
-  const Prim<R> C = cell_prim(F, I, x, y, z, dx, dt, cs);
-  // conserved (:170-176)
+  Prim<R> C;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) load_face_prim(P, ncell, i, d, C);
+  // conserved (:170-176); this thread's cell only, so the update is in place
   R U[4];
   U[0] = rho[i] * vol;
   U[1] = rho[i] * vx[i] * vol;
@@ -139,15 +168,19 @@ __global__ void __launch_bounds__(128)
   U[3] = rho[i] * vz[i] * vol;
   // apply_fluxes (:212-223): per axis, F += -fac * flux(+face); F += fac * flux(-face)
   R up[3][4], dn[3][4];
+#pragma unroll
   for (int d = 0; d < 3; ++d) {
     const int ex = d == 0, ey = d == 1, ez = d == 2;
-    const Prim<R> Pp = cell_prim(F, I, x + ex, y + ey, z + ez, dx, dt, cs);
-    const Prim<R> Pm = cell_prim(F, I, x - ex, y - ey, z - ez, dx, dt, cs);
+    Prim<R> Pp, Pm;
+    load_face_prim(P, ncell, I.at(x + ex, y + ey, z + ez), d, Pp);
+    load_face_prim(P, ncell, I.at(x - ex, y - ey, z - ez), d, Pm);
     face_flux(C, Pp, d, dx, cs, up[d]);
     face_flux(Pm, C, d, dx, cs, dn[d]);
   }
+#pragma unroll
   for (int v = 0; v < 4; ++v) {
     R u = U[v];
+#pragma unroll
     for (int d = 0; d < 3; ++d) {
       u = u + -fac * up[d][v];
       u = u + fac * dn[d][v];
@@ -157,10 +190,10 @@ __global__ void __launch_bounds__(128)
   // get_primitive (:179-185)
   R r = U[0] / vol;
   if (clamp_rho) r = fmax((R)0, r);
-  orho[i] = r;
-  ovx[i] = U[1] / U[0];
-  ovy[i] = U[2] / U[0];
-  ovz[i] = U[3] / U[0];
+  rho[i] = r;
+  vx[i] = U[1] / U[0];
+  vy[i] = U[2] / U[0];
+  vz[i] = U[3] / U[0];
 }
 
 // do_accretion (quantum-gas-bh.py:497-530; quantum-bh.py:306-339 with sigma)
@@ -269,22 +302,29 @@ __global__ void __launch_bounds__(256)
 
 }  // namespace
 
-int launch_hydro(bool dbl, const void *rho, const void *vx, const void *vy, const void *vz,
-                 void *orho, void *ovx, void *ovy, void *ovz, int n, double dx, double dt,
-                 double cs, int clamp_rho, cudaStream_t st) {
+int launch_hydro(bool dbl, void *rho, void *vx, void *vy, void *vz, void *prim, int n, double dx,
+                 double dt, double cs, int clamp_rho, cudaStream_t st) {
   const long long ncell = (long long)n * n * n;
-  const int T = 128;
+  const int T = 256;
   const int B = (int)((ncell + T - 1) / T);
   const double vol = dx * dx * dx, fac = dt * dx * dx;
-  if (dbl)
-    k_hydro<double><<<B, T, 0, st>>>((const double *)rho, (const double *)vx, (const double *)vy,
-                                     (const double *)vz, (double *)orho, (double *)ovx,
-                                     (double *)ovy, (double *)ovz, n, dx, dt, cs, vol, fac, clamp_rho);
-  else
-    k_hydro<float><<<B, T, 0, st>>>((const float *)rho, (const float *)vx, (const float *)vy,
-                                    (const float *)vz, (float *)orho, (float *)ovx, (float *)ovy,
-                                    (float *)ovz, n, (float)dx, (float)dt, (float)cs, (float)vol,
-                                    (float)fac, clamp_rho);
+  if (dbl) {
+    k_hydro_prim<double><<<B, T, 0, st>>>((const double *)rho, (const double *)vx,
+                                          (const double *)vy, (const double *)vz, (double *)prim,
+                                          n, dx, dt, cs);
+    QJ_CK_LAUNCH();
+    k_hydro_update<double><<<B, T, 0, st>>>((double *)rho, (double *)vx, (double *)vy,
+                                            (double *)vz, (const double *)prim, n, dx, cs, vol,
+                                            fac, clamp_rho);
+  } else {
+    k_hydro_prim<float><<<B, T, 0, st>>>((const float *)rho, (const float *)vx, (const float *)vy,
+                                         (const float *)vz, (float *)prim, n, (float)dx,
+                                         (float)dt, (float)cs);
+    QJ_CK_LAUNCH();
+    k_hydro_update<float><<<B, T, 0, st>>>((float *)rho, (float *)vx, (float *)vy, (float *)vz,
+                                           (const float *)prim, n, (float)dx, (float)cs,
+                                           (float)vol, (float)fac, clamp_rho);
+  }
   QJ_CK_LAUNCH();
   return 0;
 }

@@ -145,9 +145,8 @@ int launch_adj_update(bool dbl, void *g, const void *psi, const void *V, const v
                       long long ncell, cudaStream_t st);
 
 // ----- gas and black hole (qj_gas.cu) -----
-int launch_hydro(bool dbl, const void *rho, const void *vx, const void *vy, const void *vz,
-                 void *orho, void *ovx, void *ovy, void *ovz, int n, double dx, double dt,
-                 double cs, int clamp_rho, cudaStream_t st);
+int launch_hydro(bool dbl, void *rho, void *vx, void *vy, void *vz, void *prim, int n, double dx,
+                 double dt, double cs, int clamp_rho, cudaStream_t st);
 int launch_accrete(bool dbl, void *psi, const void *pos, const void *vel, void *m_bh, int n,
                    double dx, double sigma_v, double G, double m_per_hbar, double c_light,
                    double dt, cudaStream_t st);
