@@ -144,6 +144,7 @@ struct qj_plan {
   cudaEvent_t ev_kick = nullptr, ev_parts = nullptr;
   void *amax = nullptr, *dts = nullptr;  // real type scalars
   unsigned *err = nullptr;  // set by a fused pass whose bounded tile wait gave up
+  double *phi = nullptr;    // fused: per-box phase of the uniform potential (float64)
   void *tmp_scalar = nullptr;
   void *tmp_diag = nullptr;
   void *gas_prim = nullptr;  // hydro: 16 values per cell (limited gradients, predicted primitives)
@@ -322,6 +323,11 @@ int fused_kdk(qj_plan *P, float2 *psi, float *pos, float *vel, int n_s, double m
   P->cur_stars = n_s;
   auto half = [&](int n) { return sc ? sc->kick_half[n] : P->ph.m_per_hbar * dt / 2.0; };
   auto drift_dt = [&](int n) { return sc ? sc->drift[n] : dt; };
+  auto kick_coef = [&](int k, bool last) { return (k > 0 ? half(k - 1) : 0.0) + (last ? 0.0 : half(k)); };
+  // the uniform potential's phase is carried in float64 (FusedArgs::phi), except
+  // on the adjoint's recompute path, whose saved potentials include it
+  const bool use_phi = save == nullptr && vsave == nullptr;
+  if (use_phi) QJ_CK(cudaMemsetAsync(P->phi, 0, (size_t)nb * sizeof(double), st));
   QJ_TRY(launch_diag_load(false, diag, P->amax, st, nb));
   if (parts) QJ_TRY(launch_set_scalar(false, P->dts, INFINITY, st, nb));
   int q = 2;
@@ -349,6 +355,10 @@ int fused_kdk(qj_plan *P, float2 *psi, float *pos, float *vel, int n_s, double m
       FusedArgs a = fused_args(P, r);
       a.part_in = P->part;
       a.n_part = pass_blocks(P->n[q], q, P->n[0], P->n[1], P->n[2]);
+      if (use_phi) {
+        a.phi = P->phi;
+        a.phi_coef = kick_coef(k, last);
+      }
       QJ_TRY(launch_fused(M_POISSON, P->n[r], a, st));
     }
     {
@@ -359,7 +369,11 @@ int fused_kdk(qj_plan *P, float2 *psi, float *pos, float *vel, int n_s, double m
       FusedArgs a = fused_args(P, q);
       a.psi = psi;
       // kick k = second half kick of step k-1 and first half kick of step k
-      a.kick_coef = (k > 0 ? half(k - 1) : 0.0) + (last ? 0.0 : half(k));
+      a.kick_coef = kick_coef(k, last);
+      if (use_phi) {
+        a.phi = P->phi;
+        a.phi_final = last ? 1 : 0;
+      }
       a.b_coeff = si ? (float)P->ph.b_coeff : 0.0f;
       a.v_ext = vext;
       a.do_drift = last ? 0 : 1;
@@ -594,11 +608,14 @@ int gas_hydro(qj_plan *P, const GasArgs &g, cudaStream_t st) {
                       P->ph.cs, (g.bondi > 0 && g.n_bh > 0) ? 1 : 0, st);
 }
 
-int fused_gas_step(qj_plan *P, const GasArgs &g, cudaStream_t st) {
+// first / last: the call's first and last step (the uniform potential's phase
+// is carried in float64 over the call, see FusedArgs::phi).
+int fused_gas_step(qj_plan *P, const GasArgs &g, cudaStream_t st, bool first, bool last) {
   const bool bh = g.n_bh > 0, gas = g.rho != nullptr;
   const double dx = P->g.Lx / P->n[0];
   const double half = P->ph.m_per_hbar * g.dt / 2.0;
   QJ_TRY(ensure_prop(P, g.dt, st));
+  if (first) QJ_CK(cudaMemsetAsync(P->phi, 0, sizeof(double), st));
   auto stars = [&](FusedArgs &a) {
     if (bh) set_stars(a, P);
     if (gas) {
@@ -611,6 +628,8 @@ int fused_gas_step(qj_plan *P, const GasArgs &g, cudaStream_t st) {
     a = fused_args(P, r);
     a.part_in = P->part;
     a.n_part = pass_blocks(P->n[q], q, P->n[0], P->n[1], P->n[2]);
+    a.phi = P->phi;
+    a.phi_coef = half;
     QJ_TRY(launch_fused(M_POISSON, P->n[r], a, st));
     a = fused_args(P, 1);
     return launch_fused(M_IFFT2, P->n[1], a, st);
@@ -620,6 +639,8 @@ int fused_gas_step(qj_plan *P, const GasArgs &g, cudaStream_t st) {
     a.psi = (float2 *)g.psi;
     a.kick_coef = half;
     a.do_drift = drift;
+    a.phi = P->phi;
+    a.phi_final = (last && !drift) ? 1 : 0;  // the call's last half kick
     if (bh) set_stars(a, P);
     if (gas) {
       for (int d = 0; d < 3; ++d) a.gv[d] = (float *)g.v[d];
@@ -900,6 +921,7 @@ int qj_plan_create_batched(qj_plan **plan, const qj_grid *grid, const qj_phys *p
   if ((rc = dev_alloc(P, &P->dts, 8 * (size_t)nbox))) return fail(rc);
   if ((rc = dev_alloc(P, &P->tmp_scalar, 8))) return fail(rc);
   if ((rc = dev_alloc_t(P, &P->err, 4))) return fail(rc);
+  if ((rc = dev_alloc_t(P, &P->phi, (size_t)nbox))) return fail(rc);
   if (cudaMemset(P->err, 0, 4 * sizeof(unsigned)) != cudaSuccess)
     return fail(cuda_fail(cudaGetLastError(), "plan init", __FILE__, __LINE__));
   cudaError_t e = cudaDeviceSynchronize();
@@ -1122,7 +1144,7 @@ int qj_kdk_gas_bh_step(qj_plan *P, void *psi, void *rho, void *vx, void *vy, voi
   g.dm_accretion = dm_accretion;
   g.bondi = bondi_r_acc_mult;
   for (int s = 0; s < nsteps; ++s)
-    QJ_TRY(P->dbl ? plain_gas_step(P, g, st) : fused_gas_step(P, g, st));
+    QJ_TRY(P->dbl ? plain_gas_step(P, g, st) : fused_gas_step(P, g, st, s == 0, s == nsteps - 1));
   if (t_io) *t_io += nsteps * dt;
   return QJ_OK;
 }

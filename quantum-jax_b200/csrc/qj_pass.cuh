@@ -74,6 +74,14 @@ struct FusedArgs {
   const float *v_ext;
   unsigned *amax_bits;
   int do_drift;
+  // Uniform part of the potential (the k = 0 offset -4 pi G (mean rho - rho_bar)),
+  // kept out of the float32 kicks: POISSON adds phi_coef * V0 to *phi (float64,
+  // per box) instead of putting V0 into V; the call's last KICK (phi_final)
+  // adds *phi to its phase.  A uniform V only turns the global phase, which
+  // float32 cannot follow in sub-ulp steps (it biases |psi|).
+  double *phi;
+  double phi_coef;
+  int phi_final;
   // isothermal gas
   const float *grho;
   float *gv[3];
@@ -103,6 +111,7 @@ __device__ __forceinline__ void select_box(FusedArgs &a) {
   if (a.part) a.part += (long long)b * a.box_part;
   if (a.part_in) a.part_in += (long long)b * a.box_part;
   if (a.amax_bits) a.amax_bits += b;
+  if (a.phi) a.phi += b;
   const long long s = (long long)b * a.box_stars;
   if (a.sidx) a.sidx += s;
   if (a.sw0) a.sw0 += s;
@@ -684,7 +693,13 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CO
         float2 vh;
         if (k2 == 0.0f) {
           // V^(0) = -4 pi G (sum rho - ncell rho_bar) / 1, scaled by 1/ncell
-          vh = float2{(float)(-a.fourpiG * (mean - a.rho_bar)), 0.0f};
+          const double v0 = -a.fourpiG * (mean - a.rho_bar);
+          if (a.phi) {
+            *a.phi += a.phi_coef * v0;  // the one k = 0 element of the grid
+            vh = float2{0.0f, 0.0f};
+          } else {
+            vh = float2{(float)v0, 0.0f};
+          }
         } else {
           const float g = g0 / k2;
           vh = float2{v[e].x * g, v[e].y * g};
@@ -792,8 +807,9 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CO
 #pragma unroll
         for (int e = 0; e < E; ++e) V[e] = V[e] + a.v_ext[gb + e * gs];
       }
+      const double phi = (a.phi_final && a.phi) ? *a.phi : 0.0;
 #pragma unroll
-      for (int e = 0; e < E; ++e) ps[e] = phase_rotate(ps[e], a.kick_coef * (double)V[e]);
+      for (int e = 0; e < E; ++e) ps[e] = phase_rotate(ps[e], a.kick_coef * (double)V[e] + phi);
       if (a.v_out) {
 #pragma unroll
         for (int e = 0; e < E; ++e) a.v_out[gb + e * gs] = V[e];
