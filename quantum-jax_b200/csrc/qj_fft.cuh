@@ -167,13 +167,20 @@ template <typename C> struct SmemContig {
   __device__ __forceinline__ static void sync() { __syncwarp(); }
 };
 
-// Stage twiddle tables: for stage s > 0 (Ns = product of earlier radices,
-// radix r), entry (q - 1) * Ns + jm holds w_N^(jm q N / (Ns r)); the stages
-// are concatenated.  Threads of one stage read consecutive jm, so the table is
-// bank-conflict free when staged in shared memory.
+// Stage twiddle tables (read from shared memory by the fused passes): for
+// stage s > 0 (Ns = product of earlier radices, radix r), row jm < Ns holds
+// w_N^(jm q N / (Ns r)) for q = 1..r-1, padded to tw_row(s) entries; the
+// stages are concatenated.  A thread reads its row two twiddles at a time
+// (16-byte loads); the row length is 2 mod 4 entries, so eight consecutive
+// rows start on eight different bank quads (conflict-free 16-byte loads).
+template <int N> __host__ __device__ constexpr int tw_row(int s) {
+  int L = FftPlan<N>::radix(s) - 1;
+  while (L % 4 != 2) ++L;
+  return L;
+}
 template <int N> __host__ __device__ constexpr int stage_tw_off(int s) {
   int off = 0;
-  for (int i = 1; i < s; ++i) off += stage_ns<N>(i) * (FftPlan<N>::radix(i) - 1);
+  for (int i = 1; i < s; ++i) off += stage_ns<N>(i) * tw_row<N>(i);
   return off;
 }
 template <int N> __host__ __device__ constexpr int stage_tw_size() {
@@ -206,14 +213,23 @@ template <int N, int DIR, int S, typename C, class SM, bool TWS> struct FftStage
       for (int q = 0; q < r; ++q) a[q] = v[u + q * B];
       if constexpr (Ns > 1) {
         const int jm = j % Ns;
+        if constexpr (TWS) {
+          // two twiddles per 16-byte load from the thread's row
+          const float4 *row =
+              reinterpret_cast<const float4 *>(tw + stage_tw_off<N>(S) + jm * tw_row<N>(S));
 #pragma unroll
-        for (int q = 1; q < r; ++q) {
-          C w;
-          if constexpr (TWS)
-            w = tw[stage_tw_off<N>(S) + (q - 1) * Ns + jm];
-          else
-            w = __ldg(&tw[jm * q * (N / (Ns * r))]);
-          a[q] = DIR < 0 ? cmul(a[q], w) : cmulc(a[q], w);
+          for (int h = 0; 2 * h + 1 < r; ++h) {
+            const float4 w2 = row[h];
+            a[2 * h + 1] = DIR < 0 ? cmul(a[2 * h + 1], C{w2.x, w2.y}) : cmulc(a[2 * h + 1], C{w2.x, w2.y});
+            if (2 * h + 2 < r)
+              a[2 * h + 2] = DIR < 0 ? cmul(a[2 * h + 2], C{w2.z, w2.w}) : cmulc(a[2 * h + 2], C{w2.z, w2.w});
+          }
+        } else {
+#pragma unroll
+          for (int q = 1; q < r; ++q) {
+            const C w = __ldg(&tw[jm * q * (N / (Ns * r))]);
+            a[q] = DIR < 0 ? cmul(a[q], w) : cmulc(a[q], w);
+          }
         }
       }
       Dft<r, DIR, C>::run(a);

@@ -35,7 +35,7 @@ template <int N> static std::vector<float2> stage_table() {
       for (int jm = 0; jm < ns; ++jm) {
         const long long m = (long long)jm * q * (N / (ns * r));
         const long double th = -2.0L * 3.14159265358979323846264338327950288L * m / N;
-        t[stage_tw_off<N>(s) + (q - 1) * ns + jm] = float2{(float)cosl(th), (float)sinl(th)};
+        t[stage_tw_off<N>(s) + jm * tw_row<N>(s) + (q - 1)] = float2{(float)cosl(th), (float)sinl(th)};
       }
   }
   return t;
