@@ -382,11 +382,56 @@ def gen_bh(ref_dir):
     np.savez_compressed(os.path.join(HERE, "bh_res1.npz"), **out)
 
 
+def run_ic_block(mod):
+    """Execute the initial-condition block of the script's own main() (the
+    lines from "# Initial Conditions" up to "# Construct initial simulation
+    state") in the module's namespace; returns that namespace."""
+    import inspect
+    import textwrap
+
+    lines = textwrap.dedent(inspect.getsource(mod.main)).splitlines()[1:]
+    i0 = next(i for i, ln in enumerate(lines) if "# Initial Conditions" in ln)
+    i1 = next(i for i, ln in enumerate(lines) if "# Construct initial simulation state" in ln)
+    ns = dict(vars(mod))
+    exec(textwrap.dedent("\n".join(lines[i0:i1])), ns)
+    return ns
+
+
+def gen_ics(ref_dir):
+    """Initial conditions of quantum-stars (Gaussian blobs, seeded stars),
+    quantum-fluid (sorted random phases), quantum-bh (random phases and the
+    soliton), from the scripts' own main() code."""
+    out = {}
+    ref = load_reference(ref_dir, "quantum-stars.py", ["--res", "1"])
+    ns = run_ic_block(ref)
+    summarize("stars.psi", plain(ns["psi"]), out)
+    out["stars.pos"] = plain(ns["pos"]).copy()
+    out["stars.vel"] = plain(ns["vel"]).copy()
+    ref = load_reference(ref_dir, "quantum-fluid.py", ["--res", "1"])
+    ns = run_ic_block(ref)
+    summarize("fluid.psi", plain(ns["psi"]), out)
+    out["fluid.const"] = np.array([ref.nx, ref.Lx, ref.sigma, ref.m_per_hbar, ref.frac_dm,
+                                   ref.rho_bar, ref.rho_gas])
+    ref = load_reference(ref_dir, "quantum-bh.py", ["--res", "1"])
+    ns = run_ic_block(ref)
+    summarize("bh.psi", plain(ns["psi"]), out)
+    out["bh.const"] = np.array([ref.nx, ref.Lx, ref.sigma, ref.m_per_hbar, ref.rho_bar])
+    ref = load_reference(ref_dir, "quantum-bh.py", ["--res", "1", "--soliton"])
+    ns = run_ic_block(ref)
+    summarize("soliton.psi", plain(ns["psi"]), out)
+    out["soliton.const"] = np.array([ref.nx, ref.Lx, ref.m_22, ref.r_soliton])
+    np.savez_compressed(os.path.join(HERE, "ic_res1.npz"), **out)
+
+
 def main():
     ap = _argparse.ArgumentParser()
     ap.add_argument("ref_dir", nargs="?", default="/root/reference")
+    ap.add_argument("--only", default=None, help="generate one case, e.g. gen_ics")
     a = ap.parse_args()
-    for fn in (gen_stars, gen_gasbh, gen_tidal, gen_cosmo, gen_bondi, gen_bh):
+    fns = (gen_stars, gen_gasbh, gen_tidal, gen_cosmo, gen_bondi, gen_bh, gen_ics)
+    for fn in fns:
+        if a.only and fn.__name__ != a.only:
+            continue
         print(fn.__name__, flush=True)
         fn(a.ref_dir)
 
