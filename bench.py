@@ -62,6 +62,9 @@ def parse():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-gas", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--tune-dir", default=os.path.join(os.environ.get("TMPDIR", "/tmp"), "qj_tune"),
+                    help="where the autotuner's JSON cache lives")
     ap.add_argument("--gas-n", type=int, default=128)
     ap.add_argument("--gas-steps", type=int, default=500)
     ap.add_argument("--ens-steps", type=int, default=100)
@@ -337,6 +340,12 @@ def main():
     # ---------------- fused float32: device-timed ----------------
     fused = qj.Plan(grid, phys, qj.FUSED_F32, n_s)
     ps, po, ve, diag = fresh(qj.FUSED_F32)
+    # launch tuning (CTAs per SM per pass, reserved slots): timed on a copy of
+    # the state before the warm-up; results do not depend on it
+    tuning = fused.tuning
+    if not a.no_autotune:
+        tuning = fused.autotune(ps, po, ve, p.m_s, dt, probe_steps=10,
+                                cache_file=os.path.join(a.tune_dir, "tuning.json"))
     fused.kdk_step(ps, po, ve, diag, dt, a.warmup, p.m_s)
     barrier()
     clocks = Clocks(local)
@@ -532,6 +541,15 @@ def main():
             singles.append(qj.Plan(qj.Grid(n_e, n_e, n_e),
                                    qj.Phys(m_per_hbar=1.0, G=p_e.G, rho_bar=p_e.rho_bar),
                                    qj.FUSED_F32, 256))
+        if not a.no_autotune:
+            # each batched plan, and each single-box plan of the one-by-one
+            # comparison, on its own state (the first box for the latter)
+            for pl, sg, stt in zip(plans, singles, state):
+                pl.autotune(stt[0], stt[1], stt[2], stt[5], stt[4], probe_steps=5,
+                            cache_file=os.path.join(a.tune_dir, "tuning.json"))
+                sg.autotune(stt[0][0].contiguous(), stt[1][0].contiguous(),
+                            stt[2][0].contiguous(), stt[5], stt[4], probe_steps=5,
+                            cache_file=os.path.join(a.tune_dir, "tuning.json"))
         ens = qj.Ensemble(plans)
         init = [[t.clone() if isinstance(t, torch.Tensor) else t for t in s] for s in state]
 
@@ -582,6 +600,7 @@ def main():
                                      torch.linalg.vector_norm(ps64))
             pl64.close()
         ensemble = {"boxes": "16x64^3 + 8x96^3 + 8x128^3, 256 stars each",
+                    "tuning": {f"{n_e}^3": pl.tuning for (n_e, _), pl in zip(groups, plans)},
                     "cells": cells, "steps": ens_steps, "graph_chunk": a.ens_chunk,
                     "ensemble_cell_steps_per_s": cells * ens_steps / (ens_ms * 1e-3),
                     "one_by_one_cell_steps_per_s": cells * ens_steps / (seq_ms * 1e-3),
@@ -620,6 +639,7 @@ def main():
                              "pos_rel_l2_vs_f64": pos_err,
                              "f64_path": "plain float64 GPU path (matches the oracle to 1e-11)"},
                 "roofline": roofline, "step_roofline": step_roof, "passes": per_pass,
+                "tuning": tuning,
                 "gpu_launches": launches, "clocks": clk, "e2e": e2e, "cpu_baseline": cb,
                 "adjoint": adjoint, "ensemble": ensemble, "gas_bh": gas_bh}
         print(json.dumps(line), flush=True)

@@ -207,6 +207,23 @@ int qj_ensemble_step(qj_ensemble *ens, void *const *psi, void *const *pos,
 /* Bytes of device workspace the plan holds. */
 int64_t qj_plan_workspace_bytes(const qj_plan *plan);
 
+/* Launch tuning of a plan: QJ_TUNE_N integers.
+ *   [0..7]  CTAs per SM of the persistent fused passes, by pass (0 density,
+ *           1 forward FFT y, 2 Poisson, 3 inverse FFT y, 4 kick, 5 drift y,
+ *           6 drift + density, 7 deposit); 0 = the occupancy maximum.
+ *   [8]     CTA slots the passes leave free for the star stream; -1 = 2.
+ *   [9]     threads per block of the hydro kernels; 0 = 256.
+ * Tuning changes launch shapes only: results are bit-identical for every
+ * setting.  qj_autotune_kdk times qj_kdk_step on a copy of the given state
+ * (probe_steps steps per trial; psi/pos/vel are not modified) and keeps the
+ * fastest setting of [0..8] in the plan.  No reference counterpart (XLA picks
+ * its own launch shapes). */
+#define QJ_TUNE_N 10
+int qj_plan_get_tuning(const qj_plan *plan, int32_t *tune, int n);
+int qj_plan_set_tuning(qj_plan *plan, const int32_t *tune, int n);
+int qj_autotune_kdk(qj_plan *plan, const void *psi, const void *pos, const void *vel, int n_s,
+                    double m_s, double dt, int probe_steps, void *stream);
+
 /* qj_plan_status: waits for the device, then returns QJ_ERR_TIMEOUT (and
  * clears the flag) if a fused pass of this plan gave up a bounded wait for
  * one of its tile copies since the last call, else QJ_OK.  No reference

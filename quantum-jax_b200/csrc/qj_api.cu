@@ -145,6 +145,7 @@ struct qj_plan {
   void *amax = nullptr, *dts = nullptr;  // real type scalars
   unsigned *err = nullptr;  // set by a fused pass whose bounded tile wait gave up
   double *phi = nullptr;    // fused: per-box phase of the uniform potential (float64)
+  int tune[QJ_TUNE_N] = {0, 0, 0, 0, 0, 0, 0, 0, -1, 0};  // launch tuning (include/qj.h)
   void *tmp_scalar = nullptr;
   void *tmp_diag = nullptr;
   void *gas_prim = nullptr;  // hydro: 16 values per cell (limited gradients, predicted primitives)
@@ -259,6 +260,7 @@ FusedArgs fused_args(const qj_plan *P, int axis) {
   a.inv_ncell = 1.0 / (double)P->ncell;
   a.amax_bits = (unsigned *)P->amax;
   a.err = P->err;
+  a.tune = P->tune;
   a.nbox = P->nbox;
   a.box_cells = P->ncell;
   a.box_stars = P->cur_stars;
@@ -605,7 +607,8 @@ int ensure_gas_ws(qj_plan *P) {
 int gas_hydro(qj_plan *P, const GasArgs &g, cudaStream_t st) {
   const double dx = P->g.Lx / P->n[0];
   return launch_hydro(P->dbl, g.rho, g.v[0], g.v[1], g.v[2], P->gas_prim, P->n[0], dx, g.dt,
-                      P->ph.cs, (g.bondi > 0 && g.n_bh > 0) ? 1 : 0, st);
+                      P->ph.cs, (g.bondi > 0 && g.n_bh > 0) ? 1 : 0, st,
+                      P->tune[9] > 0 ? P->tune[9] : 256);
 }
 
 // first / last: the call's first and last step (the uniform potential's phase
@@ -954,6 +957,144 @@ int qj_plan_set_phys(qj_plan *P, const qj_phys *phys) {
 }
 
 int64_t qj_plan_workspace_bytes(const qj_plan *P) { return P ? P->ws_bytes : 0; }
+
+int qj_plan_get_tuning(const qj_plan *P, int32_t *tune, int n) {
+  if (!P || !tune || n < QJ_TUNE_N) {
+    set_error("qj_plan_get_tuning: bad argument (n must be >= %d)", QJ_TUNE_N);
+    return QJ_ERR_ARG;
+  }
+  for (int i = 0; i < QJ_TUNE_N; ++i) tune[i] = P->tune[i];
+  return QJ_OK;
+}
+
+int qj_plan_set_tuning(qj_plan *P, const int32_t *tune, int n) {
+  if (!P || !tune || n < QJ_TUNE_N) {
+    set_error("qj_plan_set_tuning: bad argument (n must be >= %d)", QJ_TUNE_N);
+    return QJ_ERR_ARG;
+  }
+  for (int i = 0; i < 8; ++i)
+    if (tune[i] < 0 || tune[i] > 32) {
+      set_error("qj_plan_set_tuning: CTAs per SM of pass %d must be 0..32", i);
+      return QJ_ERR_ARG;
+    }
+  if (tune[8] < -1 || tune[8] > 64 || !(tune[9] == 0 || tune[9] == 64 || tune[9] == 128 ||
+                                         tune[9] == 256)) {
+    set_error("qj_plan_set_tuning: reserve must be -1..64, hydro block 0/64/128/256");
+    return QJ_ERR_ARG;
+  }
+  for (int i = 0; i < QJ_TUNE_N; ++i) P->tune[i] = tune[i];
+  return QJ_OK;
+}
+
+// Coordinate search over the launch tuning of the fused step: per pass, the
+// CTAs per SM (1 .. occupancy maximum); then the reserved CTA slots.  Each
+// trial runs probe_steps steps of qj_kdk_step on a scratch copy of the state
+// (the caller's arrays are only read) and takes the faster of two timings.
+int qj_autotune_kdk(qj_plan *P, const void *psi, const void *pos, const void *vel, int n_s,
+                    double m_s, double dt, int probe_steps, void *stream) {
+  if (!P || !psi || n_s < 0 || (n_s > 0 && (!pos || !vel)) || probe_steps < 1 ||
+      !(dt > 0) || n_s > P->max_particles) {
+    set_error("qj_autotune_kdk: bad argument");
+    return QJ_ERR_ARG;
+  }
+  if (P->dbl) return QJ_OK;  // the plain path has no persistent passes to tune
+  cudaStream_t st = (cudaStream_t)stream;
+  const int nb = P->nbox;
+  const size_t psi_b = (size_t)nb * P->ncell * sizeof(float2);
+  const size_t par_b = (size_t)nb * n_s * 3 * sizeof(float);
+  void *s_psi = nullptr, *s_pos = nullptr, *s_vel = nullptr, *s_diag = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int rc = QJ_OK;
+  auto cleanup = [&] {
+    cudaFree(s_psi);
+    cudaFree(s_pos);
+    cudaFree(s_vel);
+    cudaFree(s_diag);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+  };
+  cudaError_t e = cudaMalloc(&s_psi, psi_b);
+  if (e == cudaSuccess && n_s > 0) e = cudaMalloc(&s_pos, par_b);
+  if (e == cudaSuccess && n_s > 0) e = cudaMalloc(&s_vel, par_b);
+  if (e == cudaSuccess) e = cudaMalloc(&s_diag, (size_t)nb * 3 * sizeof(double));
+  if (e == cudaSuccess) e = cudaEventCreate(&e0);
+  if (e == cudaSuccess) e = cudaEventCreate(&e1);
+  if (e != cudaSuccess) {
+    cleanup();
+    return cuda_fail(e, "autotune scratch", __FILE__, __LINE__);
+  }
+  std::vector<double> diag0((size_t)nb * 3);
+  for (int b = 0; b < nb; ++b) {
+    diag0[3 * b] = 0.0;
+    diag0[3 * b + 1] = 0.0;
+    diag0[3 * b + 2] = dt;
+  }
+  auto trial = [&](float &ms) -> int {
+    float best = 1e30f;
+    for (int rep = 0; rep < 2; ++rep) {
+      QJ_CK(cudaMemcpyAsync(s_psi, psi, psi_b, cudaMemcpyDeviceToDevice, st));
+      if (n_s > 0) {
+        QJ_CK(cudaMemcpyAsync(s_pos, pos, par_b, cudaMemcpyDeviceToDevice, st));
+        QJ_CK(cudaMemcpyAsync(s_vel, vel, par_b, cudaMemcpyDeviceToDevice, st));
+      }
+      QJ_CK(cudaMemcpyAsync(s_diag, diag0.data(), diag0.size() * sizeof(double),
+                            cudaMemcpyHostToDevice, st));
+      QJ_CK(cudaEventRecord(e0, st));
+      QJ_TRY(fused_kdk(P, (float2 *)s_psi, (float *)s_pos, (float *)s_vel, n_s, m_s, dt,
+                       probe_steps, 0, nullptr, (double *)s_diag, st));
+      QJ_CK(cudaEventRecord(e1, st));
+      QJ_CK(cudaEventSynchronize(e1));
+      float t = 0.f;
+      QJ_CK(cudaEventElapsedTime(&t, e0, e1));
+      best = std::min(best, t);
+    }
+    ms = best;
+    return 0;
+  };
+  const int saved[QJ_TUNE_N] = {P->tune[0], P->tune[1], P->tune[2], P->tune[3], P->tune[4],
+                                P->tune[5], P->tune[6], P->tune[7], P->tune[8], P->tune[9]};
+  float best_ms = 0.f;
+  if ((rc = trial(best_ms)) == 0 && (rc = trial(best_ms)) == 0) {  // warm-up, then baseline
+    const int modes[] = {M_FFT_FWD, M_POISSON, M_IFFT2, M_KICK, M_DRIFT, M_DRIFT_DENSITY};
+    for (int m : modes) {
+      // occupancy of the pass over both orientations it runs in
+      int kmax = 0;
+      for (int ax = 0; ax < 3; ++ax) kmax = std::max(kmax, fused_max_ctas_per_sm(m, P->n[ax], ax == 2));
+      const int cur = P->tune[m];
+      int best_k = cur;
+      for (int k = 1; k <= kmax && rc == 0; ++k) {
+        if (k == cur || (cur == 0 && k == kmax)) continue;
+        P->tune[m] = k;
+        float t = 0.f;
+        if ((rc = trial(t)) == 0 && t < 0.99f * best_ms) {
+          best_ms = t;
+          best_k = k;
+        }
+      }
+      P->tune[m] = best_k;
+    }
+    const int cur_r = P->tune[8];
+    int best_r = cur_r;
+    for (int r : {0, 2, 4, 8}) {
+      if (rc) break;
+      if (r == (cur_r < 0 ? 2 : cur_r)) continue;
+      P->tune[8] = r;
+      float t = 0.f;
+      if ((rc = trial(t)) == 0 && t < 0.99f * best_ms) {
+        best_ms = t;
+        best_r = r;
+      }
+    }
+    P->tune[8] = best_r;
+  }
+  if (rc)
+    for (int i = 0; i < QJ_TUNE_N; ++i) P->tune[i] = saved[i];
+  const cudaError_t se = cudaStreamSynchronize(st);
+  cleanup();
+  if (rc) return rc;
+  QJ_CK(se);
+  return QJ_OK;
+}
 
 int qj_plan_status(qj_plan *P) {
   if (!P) {

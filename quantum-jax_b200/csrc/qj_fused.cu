@@ -127,28 +127,43 @@ static int strided_maps(const FusedArgs &a, TileMaps &maps) {
   return 0;
 }
 
+// Resident CTAs per SM of a pass (occupancy) and the SM count, queried once.
+template <int N, bool CONTIG, int MODE>
+static cudaError_t fused_occupancy(int &per_sm, int &sms) {
+  using SH = PassShape<N, CONTIG>;
+  static std::once_flag once;
+  static cudaError_t err = cudaSuccess;
+  static int c_per_sm = 1, c_sms = 1;
+  std::call_once(once, [&] {
+    const size_t smem = fused_smem_bytes<N, CONTIG, MODE>();
+    err = cudaFuncSetAttribute(k_fused<N, CONTIG, MODE>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int dev = 0, n_sm = 0, p = 0;
+    if (err == cudaSuccess) err = cudaGetDevice(&dev);
+    if (err == cudaSuccess) err = cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+    if (err == cudaSuccess)
+      err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&p, k_fused<N, CONTIG, MODE>, SH::THREADS,
+                                                          smem);
+    c_per_sm = std::max(1, p);
+    c_sms = std::max(1, n_sm);
+  });
+  per_sm = c_per_sm;
+  sms = c_sms;
+  return err;
+}
+
 template <int N, bool CONTIG, int MODE>
 static int run_fused(const FusedArgs &a, cudaStream_t st) {
   using SH = PassShape<N, CONTIG>;
   const size_t smem = fused_smem_bytes<N, CONTIG, MODE>();
   // persistent grid: the CTAs resident at once (occupancy x SMs), shared
   // between the boxes of a batched launch
-  static std::once_flag once;
-  static cudaError_t attr_err = cudaSuccess;
-  static int resident = 0;
-  std::call_once(once, [&] {
-    attr_err = cudaFuncSetAttribute(k_fused<N, CONTIG, MODE>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    int dev = 0, sms = 0, per_sm = 0;
-    if (attr_err == cudaSuccess) attr_err = cudaGetDevice(&dev);
-    if (attr_err == cudaSuccess)
-      attr_err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (attr_err == cudaSuccess)
-      attr_err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fused<N, CONTIG, MODE>,
-                                                               SH::THREADS, smem);
-    resident = std::max(1, per_sm) * std::max(1, sms);
-  });
-  QJ_CK(attr_err);
+  int per_sm = 0, sms = 0;
+  const cudaError_t occ = fused_occupancy<N, CONTIG, MODE>(per_sm, sms);
+  QJ_CK(occ);
+  const int want = a.tune ? a.tune[MODE] : 0;
+  const int resident = (want > 0 ? std::min(want, per_sm) : per_sm) * sms;
+  const int reserve = (a.tune && a.tune[8] >= 0) ? a.tune[8] : reserve_ctas();
   // the bulk tile copies need 16-byte aligned fields
   const void *fields[4] = {a.psi, a.R, a.S1, a.S2};
   for (const void *f : fields)
@@ -165,7 +180,7 @@ static int run_fused(const FusedArgs &a, cudaStream_t st) {
     if (rc) return rc;
   }
   const int nbox = a.nbox > 1 ? a.nbox : 1;
-  const int gx = std::max(1, std::min(b.ntiles, (resident - reserve_ctas()) / nbox));
+  const int gx = std::max(1, std::min(b.ntiles, (resident - reserve) / nbox));
   const dim3 grid(gx, nbox);
   k_fused<N, CONTIG, MODE><<<grid, SH::THREADS, smem, st>>>(b, maps);
   QJ_CK_LAUNCH();
@@ -232,6 +247,46 @@ static int launch_fused_impl(int mode, int n, const FusedArgs &a, cudaStream_t s
   }
   set_error("internal: bad pass mode %d", mode);
   return 1;
+}
+
+template <int MODE> static int occupancy_of(int n, bool contig) {
+  int per_sm = 0, sms = 0;
+  cudaError_t e = cudaSuccess;
+  constexpr bool ONLY_Y = (MODE == M_FFT_FWD || MODE == M_IFFT2 || MODE == M_DRIFT);
+  constexpr bool ONLY_Z = (MODE == M_DEPOSIT);
+#define QJ_OCC(NN)                                                                          \
+  case NN:                                                                                  \
+    if constexpr (ONLY_Y) e = fused_occupancy<NN, false, MODE>(per_sm, sms);                \
+    else if constexpr (ONLY_Z) e = fused_occupancy<NN, true, MODE>(per_sm, sms);            \
+    else e = contig ? fused_occupancy<NN, true, MODE>(per_sm, sms)                          \
+                    : fused_occupancy<NN, false, MODE>(per_sm, sms);                        \
+    break;
+  switch (n) {
+    QJ_OCC(16)
+    QJ_OCC(32)
+    QJ_OCC(64)
+    QJ_OCC(96)
+    QJ_OCC(128)
+    QJ_OCC(256)
+    QJ_OCC(512)
+    default: return 0;
+  }
+#undef QJ_OCC
+  return e == cudaSuccess ? per_sm : 0;
+}
+
+int fused_max_ctas_per_sm(int mode, int n, bool contig) {
+  switch (mode) {
+    case M_DENSITY: return occupancy_of<M_DENSITY>(n, contig);
+    case M_FFT_FWD: return occupancy_of<M_FFT_FWD>(n, contig);
+    case M_POISSON: return occupancy_of<M_POISSON>(n, contig);
+    case M_IFFT2: return occupancy_of<M_IFFT2>(n, contig);
+    case M_KICK: return occupancy_of<M_KICK>(n, contig);
+    case M_DRIFT: return occupancy_of<M_DRIFT>(n, contig);
+    case M_DRIFT_DENSITY: return occupancy_of<M_DRIFT_DENSITY>(n, contig);
+    case M_DEPOSIT: return occupancy_of<M_DEPOSIT>(n, contig);
+  }
+  return 0;
 }
 
 int launch_fused(int mode, int n, const FusedArgs &a, cudaStream_t st) {

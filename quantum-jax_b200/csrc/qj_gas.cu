@@ -303,9 +303,9 @@ __global__ void __launch_bounds__(256)
 }  // namespace
 
 int launch_hydro(bool dbl, void *rho, void *vx, void *vy, void *vz, void *prim, int n, double dx,
-                 double dt, double cs, int clamp_rho, cudaStream_t st) {
+                 double dt, double cs, int clamp_rho, cudaStream_t st, int block) {
   const long long ncell = (long long)n * n * n;
-  const int T = 256;
+  const int T = (block == 64 || block == 128 || block == 256) ? block : 256;
   const int B = (int)((ncell + T - 1) / T);
   const double vol = dx * dx * dx, fac = dt * dx * dx;
   if (dbl) {

@@ -145,8 +145,11 @@ int launch_adj_update(bool dbl, void *g, const void *psi, const void *V, const v
                       long long ncell, cudaStream_t st);
 
 // ----- gas and black hole (qj_gas.cu) -----
+// CTAs of a fused pass that fit one SM (occupancy), 0 if unknown.
+int fused_max_ctas_per_sm(int mode, int n, bool contig);
+
 int launch_hydro(bool dbl, void *rho, void *vx, void *vy, void *vz, void *prim, int n, double dx,
-                 double dt, double cs, int clamp_rho, cudaStream_t st);
+                 double dt, double cs, int clamp_rho, cudaStream_t st, int block = 256);
 int launch_accrete(bool dbl, void *psi, const void *pos, const void *vel, void *m_bh, int n,
                    double dx, double sigma_v, double G, double m_per_hbar, double c_light,
                    double dt, cudaStream_t st);

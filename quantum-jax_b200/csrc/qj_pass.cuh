@@ -88,6 +88,8 @@ struct FusedArgs {
   float gas_dt;
   // tiles of this pass per box (the persistent CTAs stride over them)
   int ntiles;
+  // host side only: the plan's launch tuning (QJ_TUNE_* of include/qj.h)
+  const int *tune;
   // set to nonzero when a pass gave up waiting for a tile copy
   unsigned *err;
   // batched boxes (blockIdx.y = box): per-box strides of the fields (cells),

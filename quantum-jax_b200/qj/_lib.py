@@ -21,6 +21,7 @@ QJ_ERR_TIMEOUT = 4
 QJ_ERR_ALLOC = 5
 QJ_PLAIN_F64 = 0
 QJ_FUSED_F32 = 1
+QJ_TUNE_N = 10
 
 # Every symbol include/qj.h declares, with (restype, argtypes).
 c_void_p, c_int, c_double, c_int64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int64
@@ -70,6 +71,10 @@ SIGNATURES = {
                                              c_void_p, c_void_p, c_int, c_void_p]),
     "qj_plan_workspace_bytes": (c_int64, [c_void_p]),
     "qj_plan_status": (c_int, [c_void_p]),
+    "qj_plan_get_tuning": (c_int, [c_void_p, c_void_p, c_int]),
+    "qj_plan_set_tuning": (c_int, [c_void_p, c_void_p, c_int]),
+    "qj_autotune_kdk": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_double,
+                                c_double, c_int, c_void_p]),
     "qj_launch_count": (c_int64, []),
     "qj_profile_enable": (c_int, [c_int]),
     "qj_profile_read": (c_int, [ctypes.POINTER(c_double), ctypes.POINTER(c_int64), c_int]),

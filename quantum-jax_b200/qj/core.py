@@ -119,6 +119,61 @@ class Plan:
     def workspace_bytes(self):
         return int(lib().qj_plan_workspace_bytes(self._h))
 
+    # ----- launch tuning -----
+    @property
+    def tuning(self):
+        """The plan's launch tuning (QJ_TUNE_N ints, see include/qj.h)."""
+        buf = (ctypes.c_int32 * _lib.QJ_TUNE_N)()
+        check(lib().qj_plan_get_tuning(self._h, buf, _lib.QJ_TUNE_N))
+        return list(buf)
+
+    @tuning.setter
+    def tuning(self, values):
+        buf = (ctypes.c_int32 * _lib.QJ_TUNE_N)(*[int(v) for v in values])
+        check(lib().qj_plan_set_tuning(self._h, buf, _lib.QJ_TUNE_N))
+
+    def autotune(self, psi, pos, vel, m_s, dt, probe_steps=10, cache_file=None):
+        """Pick the fused passes' CTAs per SM and the reserved CTA slots by
+        timing qj_kdk_step on a copy of (psi, pos, vel); the arrays are only
+        read.  Results are cached in a JSON file (QJ_TUNING_CACHE, default
+        ~/.cache/qj/tuning.json) keyed by device, grid, boxes, stars and
+        precision; a cached entry is applied without timing.  Returns the
+        tuning list."""
+        import json
+        import os
+
+        n_s = 0 if pos is None else int(pos.shape[-2])
+        key = "|".join(str(x) for x in (
+            torch.cuda.get_device_name(psi.device), self.grid.nx, self.grid.ny, self.grid.nz,
+            self.nbox, n_s, self.precision))
+        path = cache_file or os.environ.get(
+            "QJ_TUNING_CACHE", os.path.join(os.path.expanduser("~"), ".cache", "qj", "tuning.json"))
+        cache = {}
+        if os.path.exists(path):
+            with open(path) as f:
+                cache = json.load(f)
+        if key in cache:
+            self.tuning = cache[key]
+            return self.tuning
+        ncell = self.grid.nx * self.grid.ny * self.grid.nz
+        if (not psi.is_cuda or psi.dtype != self.cdtype or not psi.is_contiguous()
+                or psi.numel() != self.nbox * ncell):
+            raise ValueError(f"psi must be a contiguous CUDA {self.cdtype} tensor of "
+                             f"{self.nbox} box(es) of {ncell} cells")
+        for t, name in ((pos, "pos"), (vel, "vel")):
+            if n_s and (not t.is_cuda or t.dtype != self.rdtype or not t.is_contiguous()
+                        or t.numel() != self.nbox * n_s * 3):
+                raise ValueError(f"{name} must be a contiguous CUDA {self.rdtype} tensor "
+                                 f"[nbox, n_s, 3] (or [n_s, 3] for one box)")
+        check(lib().qj_autotune_kdk(self._h, _ptr(psi), _ptr(pos) if n_s else None,
+                                    _ptr(vel) if n_s else None, n_s, float(m_s), float(dt),
+                                    int(probe_steps), _stream()))
+        cache[key] = self.tuning
+        os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
+        with open(path, "w") as f:
+            json.dump(cache, f, indent=1)
+        return cache[key]
+
     def status(self):
         """Wait for the device; raise if a fused pass of this plan gave up a
         bounded wait for a tile copy since the last call."""
