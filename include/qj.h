@@ -207,6 +207,24 @@ int qj_ensemble_step(qj_ensemble *ens, void *const *psi, void *const *pos,
 /* Bytes of device workspace the plan holds. */
 int64_t qj_plan_workspace_bytes(const qj_plan *plan);
 
+/* bh_bondi_step_ambient (quantum-fluid-accretion.py:440-510): fixed-grid sink
+ * of radius r_acc_mult dx around x_bh with the ambient density sampled in
+ * the shell [max(ann_lo r_acc, r_acc + dx/4), max(ann_hi r_acc, r_lo + dx/2)].
+ * rho (the plan's real type) is updated in place.  vx/vy/vz (may be NULL)
+ * add the BHL term with the black-hole velocity v_bh.  fmax <= 0: no cap
+ * beyond the sink's mass.  out (device, 7 doubles) = dMdt_target, rho_inf,
+ * rB, dM_cap, r_acc, M_avail, dM_uncl. */
+int qj_bondi_ambient(qj_plan *plan, void *rho, const void *vx, const void *vy, const void *vz,
+                     const double *x_bh, const double *v_bh, double M_bh, double dt,
+                     double r_acc_mult, double lam, double fmax, double ann_lo, double ann_hi,
+                     double *out, void *stream);
+
+/* Hydro CFL step, quantum-fluid-accretion.py:697-701 (constant sound speed
+ * cs, cs2_local :248-250): dt_out (device double) = min(dt, cfl dx /
+ * max(cs + |v|)). */
+int qj_hydro_cfl_dt(qj_plan *plan, const void *vx, const void *vy, const void *vz, double cs,
+                    double cfl, double dt, double *dt_out, void *stream);
+
 /* Launch tuning of a plan: QJ_TUNE_N integers.
  *   [0..7]  CTAs per SM of the persistent fused passes, by pass (0 density,
  *           1 forward FFT y, 2 Poisson, 3 inverse FFT y, 4 kick, 5 drift y,

@@ -549,6 +549,55 @@ def bondi_sink(rho, M_bh, x_bh, dx, Lx, cs, G, dt, r_acc_mult=4.0,
     return rho_new, M_bh + dM_cap, dMdt, rho_inf, r_B, dM_cap
 
 
+def bondi_sink_ambient(rho, M_bh, x_bh, dx, Lx, cs, G, dt, r_acc_mult=2.5,
+                       lam=LAMBDA_ISO, fmax=None, ann_lo=1.1, ann_hi=1.8,
+                       v=None, v_bh=(0.0, 0.0, 0.0)):
+    """Fixed-grid sink with the ambient density sampled in a shell just outside
+    r_acc, quantum-fluid-accretion.py:440-510.  v = (vx, vy, vz) gas
+    velocities enable the BHL denominator (cs^2 + v_rel^2)^1.5.
+    Returns (rho_new, dMdt_target, rho_inf, rB, dM_cap, r_acc, M_avail, dM_uncl)."""
+    nx = rho.shape[0]
+    xs = (np.arange(nx) + 0.5) * dx
+
+    def pdelta(x0):
+        d = np.abs(xs - x0)
+        return np.minimum(d, Lx - d)
+
+    dX, dY, dZ = np.meshgrid(pdelta(x_bh[0]), pdelta(x_bh[1]), pdelta(x_bh[2]), indexing="ij")
+    R = np.sqrt(dX * dX + dY * dY + dZ * dZ)
+    rB = G * M_bh / (cs * cs + 1e-30)
+    r_acc = r_acc_mult * dx
+    rK = min(0.5 * r_acc, max(0.5 * dx, rB))
+    mask = R <= r_acc
+    W = np.exp(-0.5 * (R / (rK + 1e-30)) ** 2) * mask
+    r_lo = max(ann_lo * r_acc, r_acc + 0.25 * dx)
+    r_hi = max(ann_hi * r_acc, r_lo + 0.5 * dx)
+    shell = (R >= r_lo) & (R <= r_hi)
+    n_sh = np.sum(shell) + 1e-30
+    rho_inf = np.sum(rho * shell) / n_sh
+    if v is not None:
+        v_inf = [np.sum(c * shell) / n_sh for c in v]
+        v_rel2 = sum((b - c) ** 2 for b, c in zip(v_bh, v_inf))
+        denom = (cs**2 + v_rel2) ** 1.5
+    else:
+        denom = cs**3
+    dMdt = 4.0 * np.pi * lam * (G * M_bh) ** 2 * rho_inf / (denom + 1e-30)
+    dM_uncl = dMdt * dt
+    WRho = W * rho
+    phi = WRho / (np.sum(WRho) + 1e-30)
+    M_avail = np.sum(rho * mask) * dx**3
+    dM_cap = min(dM_uncl, M_avail) if fmax is None else min(dM_uncl, fmax * M_avail)
+    rho_new = np.maximum(0.0, rho - (dM_cap / dx**3) * phi)
+    return rho_new, dMdt, rho_inf, rB, dM_cap, r_acc, M_avail, dM_uncl
+
+
+def hydro_cfl_dt(vx, vy, vz, cs, dx, cfl, dt):
+    """dt_eff = min(dt, cfl dx / max(c + |v|)), quantum-fluid-accretion.py:697-701
+    with the constant sound speed of cs2_local (:248-250)."""
+    cmax = np.max(cs + np.sqrt(vx * vx + vy * vy + vz * vz))
+    return min(dt, cfl * dx / (cmax + 1e-30))
+
+
 # ---------------------------------------------------------------------------
 # R16: the gas + black-hole step, quantum-gas-bh.py:537-578
 # ---------------------------------------------------------------------------

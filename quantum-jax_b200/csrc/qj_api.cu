@@ -145,6 +145,7 @@ struct qj_plan {
   void *amax = nullptr, *dts = nullptr;  // real type scalars
   unsigned *err = nullptr;  // set by a fused pass whose bounded tile wait gave up
   double *phi = nullptr;    // fused: per-box phase of the uniform potential (float64)
+  double *cfl_part = nullptr;  // per-block maxima of the CFL reduction
   int tune[QJ_TUNE_N] = {0, 0, 0, 0, 0, 0, 0, 0, -1, 0};  // launch tuning (include/qj.h)
   void *tmp_scalar = nullptr;
   void *tmp_diag = nullptr;
@@ -957,6 +958,39 @@ int qj_plan_set_phys(qj_plan *P, const qj_phys *phys) {
 }
 
 int64_t qj_plan_workspace_bytes(const qj_plan *P) { return P ? P->ws_bytes : 0; }
+
+int qj_bondi_ambient(qj_plan *P, void *rho, const void *vx, const void *vy, const void *vz,
+                     const double *x_bh, const double *v_bh, double M_bh, double dt,
+                     double r_acc_mult, double lam, double fmax, double ann_lo, double ann_hi,
+                     double *out, void *stream) {
+  if (!P || !rho || !x_bh || !out || (vx && (!vy || !vz || !v_bh)) || !(dt >= 0) ||
+      !(r_acc_mult > 0) || !(M_bh >= 0)) {
+    set_error("qj_bondi_ambient: bad argument");
+    return QJ_ERR_ARG;
+  }
+  QJ_ONE_BOX(P, "qj_bondi_ambient");
+  if (P->n[0] != P->n[1] || P->n[0] != P->n[2] || P->g.Lx != P->g.Ly || P->g.Lx != P->g.Lz) {
+    set_error("qj_bondi_ambient: needs a cubic grid and box");
+    return QJ_ERR_ARG;
+  }
+  const double zero[3] = {0.0, 0.0, 0.0};
+  return launch_bondi_ambient(P->dbl, rho, vx, vy, vz, P->n[0], P->g.Lx / P->n[0], P->g.Lx,
+                              x_bh, v_bh ? v_bh : zero, M_bh, P->ph.cs, P->ph.G, dt, r_acc_mult,
+                              lam, fmax, ann_lo, ann_hi, out, (cudaStream_t)stream);
+}
+
+int qj_hydro_cfl_dt(qj_plan *P, const void *vx, const void *vy, const void *vz, double cs,
+                    double cfl, double dt, double *dt_out, void *stream) {
+  if (!P || !vx || !vy || !vz || !dt_out || !(cfl > 0) || !(dt > 0)) {
+    set_error("qj_hydro_cfl_dt: bad argument");
+    return QJ_ERR_ARG;
+  }
+  QJ_ONE_BOX(P, "qj_hydro_cfl_dt");
+  const int nb = 592;
+  if (!P->cfl_part) QJ_TRY(dev_alloc_t(P, &P->cfl_part, (size_t)nb));
+  return launch_cfl_dt(P->dbl, vx, vy, vz, P->ncell, cs, P->g.Lx / P->n[0], cfl, dt,
+                       P->cfl_part, nb, dt_out, (cudaStream_t)stream);
+}
 
 int qj_plan_get_tuning(const qj_plan *P, int32_t *tune, int n) {
   if (!P || !tune || n < QJ_TUNE_N) {

@@ -8,6 +8,7 @@
 // neighbours' records, forms the fluxes through its six faces and applies the
 // flux-form update in place, in the same floating-point order as the
 // reference.  The grid is cubic with spacing dx, as in the reference.
+#include <algorithm>
 #include <cmath>
 
 #include "../../include/qj.h"
@@ -300,7 +301,174 @@ __global__ void __launch_bounds__(256)
   if (threadIdx.x == 0) m_bh[0] = (R)((double)M + dM_cap);
 }
 
+// Fixed-grid sink with the ambient density sampled in a shell outside r_acc
+// (bh_bondi_step_ambient, quantum-fluid-accretion.py:440-510), one CTA over
+// the (2K+1)^3 cells around the black hole; float64 sums in a fixed order.
+// out[7] = dMdt_target, rho_inf, rB, dM_cap, r_acc, M_avail, dM_uncl.
+template <typename R>
+__global__ void __launch_bounds__(256)
+    k_bondi_ambient(R *rho, const R *vx, const R *vy, const R *vz, int n, double dx, double L,
+                    double x0, double x1, double x2, double vb0, double vb1, double vb2,
+                    double M, double cs, double G, double dt, double r_acc_mult, double lam,
+                    double cap_frac, double ann_lo, double ann_hi, int K, double *out) {
+  __shared__ double red[8][256];
+  const double xb[3] = {x0, x1, x2};
+  const double rB = G * M / (cs * cs + 1e-30);
+  const double r_acc = r_acc_mult * dx;
+  const double rK = fmin(0.5 * r_acc, fmax(0.5 * dx, rB));
+  const double r_lo = fmax(ann_lo * r_acc, r_acc + 0.25 * dx);
+  const double r_hi = fmax(ann_hi * r_acc, r_lo + 0.5 * dx);
+  const bool bhl = vx != nullptr;
+  const int w = 2 * K + 1, tot = w * w * w;
+  int cidx[3];
+  for (int d = 0; d < 3; ++d) cidx[d] = (int)floor(xb[d] / dx);
+  // this thread's cells: index, distance R and kernel weight W (sink) / shell flag
+  auto cell = [&](int j, long long &c, double &Rd) {
+    const int o[3] = {j / (w * w) - K, (j / w) % w - K, j % w - K};
+    int ii[3];
+    double R2 = 0.0;
+    for (int d = 0; d < 3; ++d) {
+      ii[d] = ((cidx[d] + o[d]) % n + n) % n;
+      const double xs = ((double)ii[d] + 0.5) * dx;
+      const double dd = fabs(xs - xb[d]);
+      const double pd = fmin(dd, L - dd);
+      R2 += pd * pd;
+    }
+    Rd = sqrt(R2);
+    c = ((long long)ii[0] * n + ii[1]) * n + ii[2];
+  };
+  double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // sumWRho, M_sink, n_shell, rho_shell, v_shell[3]
+  for (int j = threadIdx.x; j < tot; j += blockDim.x) {
+    long long c;
+    double Rd;
+    cell(j, c, Rd);
+    const double r = (double)rho[c];
+    if (Rd <= r_acc) {
+      const double q = Rd / (rK + 1e-30);
+      acc[0] += exp(-0.5 * q * q) * r;
+      acc[1] += r;
+    }
+    if (Rd >= r_lo && Rd <= r_hi) {
+      acc[2] += 1.0;
+      acc[3] += r;
+      if (bhl) {
+        acc[4] += (double)vx[c];
+        acc[5] += (double)vy[c];
+        acc[6] += (double)vz[c];
+      }
+    }
+  }
+  for (int k = 0; k < 8; ++k) red[k][threadIdx.x] = acc[k];
+  __syncthreads();
+  for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+    if ((int)threadIdx.x < st)
+      for (int k = 0; k < 8; ++k) red[k][threadIdx.x] += red[k][threadIdx.x + st];
+    __syncthreads();
+  }
+  const double n_sh = red[2][0] + 1e-30;
+  const double rho_inf = red[3][0] / n_sh;
+  double denom = cs * cs * cs;
+  if (bhl) {
+    const double v_inf[3] = {red[4][0] / n_sh, red[5][0] / n_sh, red[6][0] / n_sh};
+    const double vb[3] = {vb0, vb1, vb2};
+    double v_rel2 = 0.0;
+    for (int d = 0; d < 3; ++d) v_rel2 += (vb[d] - v_inf[d]) * (vb[d] - v_inf[d]);
+    denom = pow(cs * cs + v_rel2, 1.5);
+  }
+  const double GM = G * M;
+  const double dMdt = 4.0 * 3.14159265358979323846 * lam * GM * GM * rho_inf / (denom + 1e-30);
+  const double dM_uncl = dMdt * dt;
+  const double sumWRho = red[0][0] + 1e-30;
+  const double vol = dx * dx * dx;
+  const double M_avail = red[1][0] * vol;
+  const double dM_cap = cap_frac > 0.0 ? fmin(dM_uncl, cap_frac * M_avail) : fmin(dM_uncl, M_avail);
+  __syncthreads();
+  for (int j = threadIdx.x; j < tot; j += blockDim.x) {
+    long long c;
+    double Rd;
+    cell(j, c, Rd);
+    if (Rd <= r_acc) {
+      const double q = Rd / (rK + 1e-30);
+      const double phi = exp(-0.5 * q * q) * (double)rho[c] / sumWRho;
+      rho[c] = (R)fmax(0.0, (double)rho[c] - (dM_cap / vol) * phi);
+    }
+  }
+  if (threadIdx.x == 0) {
+    out[0] = dMdt;
+    out[1] = rho_inf;
+    out[2] = rB;
+    out[3] = dM_cap;
+    out[4] = r_acc;
+    out[5] = M_avail;
+    out[6] = dM_uncl;
+  }
+}
+
+// max over cells of c + |v| (c constant), per-block partial maxima
+template <typename R>
+__global__ void k_cfl_partial(const R *vx, const R *vy, const R *vz, long long ncell, double c,
+                              double *part) {
+  __shared__ double red[256];
+  double m = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < ncell;
+       i += (long long)gridDim.x * blockDim.x) {
+    const double a = vx[i], b = vy[i], d = vz[i];
+    m = fmax(m, c + sqrt(a * a + b * b + d * d));
+  }
+  red[threadIdx.x] = m;
+  __syncthreads();
+  for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+    if ((int)threadIdx.x < st) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + st]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+__global__ void k_cfl_final(const double *part, int nb, double dx, double cfl, double dt,
+                            double *dt_out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double m = 0.0;
+  for (int b = 0; b < nb; ++b) m = fmax(m, part[b]);
+  *dt_out = fmin(dt, cfl * dx / (m + 1e-30));
+}
+
 }  // namespace
+
+int launch_bondi_ambient(bool dbl, void *rho, const void *vx, const void *vy, const void *vz,
+                         int n, double dx, double L, const double x_bh[3], const double v_bh[3],
+                         double M, double cs, double G, double dt, double r_acc_mult, double lam,
+                         double fmax, double ann_lo, double ann_hi, double *out, cudaStream_t st) {
+  const double r_acc = r_acc_mult * dx;
+  const double r_lo = std::max(ann_lo * r_acc, r_acc + 0.25 * dx);
+  const double r_hi = std::max(ann_hi * r_acc, r_lo + 0.5 * dx);
+  const int K = std::min((int)std::ceil(r_hi / dx) + 1, (n - 1) / 2);
+  if (dbl)
+    k_bondi_ambient<double><<<1, 256, 0, st>>>(
+        (double *)rho, (const double *)vx, (const double *)vy, (const double *)vz, n, dx, L,
+        x_bh[0], x_bh[1], x_bh[2], v_bh[0], v_bh[1], v_bh[2], M, cs, G, dt, r_acc_mult, lam, fmax,
+        ann_lo, ann_hi, K, out);
+  else
+    k_bondi_ambient<float><<<1, 256, 0, st>>>(
+        (float *)rho, (const float *)vx, (const float *)vy, (const float *)vz, n, dx, L, x_bh[0],
+        x_bh[1], x_bh[2], v_bh[0], v_bh[1], v_bh[2], M, cs, G, dt, r_acc_mult, lam, fmax, ann_lo,
+        ann_hi, K, out);
+  QJ_CK_LAUNCH();
+  return 0;
+}
+
+int launch_cfl_dt(bool dbl, const void *vx, const void *vy, const void *vz, long long ncell,
+                  double cs, double dx, double cfl, double dt, double *part, int nb, double *dt_out,
+                  cudaStream_t st) {
+  if (dbl)
+    k_cfl_partial<double><<<nb, 256, 0, st>>>((const double *)vx, (const double *)vy,
+                                              (const double *)vz, ncell, cs, part);
+  else
+    k_cfl_partial<float><<<nb, 256, 0, st>>>((const float *)vx, (const float *)vy,
+                                             (const float *)vz, ncell, cs, part);
+  QJ_CK_LAUNCH();
+  k_cfl_final<<<1, 32, 0, st>>>(part, nb, dx, cfl, dt, dt_out);
+  QJ_CK_LAUNCH();
+  return 0;
+}
 
 int launch_hydro(bool dbl, void *rho, void *vx, void *vy, void *vz, void *prim, int n, double dx,
                  double dt, double cs, int clamp_rho, cudaStream_t st, int block) {

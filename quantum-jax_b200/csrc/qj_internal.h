@@ -150,6 +150,13 @@ int fused_max_ctas_per_sm(int mode, int n, bool contig);
 
 int launch_hydro(bool dbl, void *rho, void *vx, void *vy, void *vz, void *prim, int n, double dx,
                  double dt, double cs, int clamp_rho, cudaStream_t st, int block = 256);
+int launch_bondi_ambient(bool dbl, void *rho, const void *vx, const void *vy, const void *vz,
+                         int n, double dx, double L, const double x_bh[3], const double v_bh[3],
+                         double M, double cs, double G, double dt, double r_acc_mult, double lam,
+                         double fmax, double ann_lo, double ann_hi, double *out, cudaStream_t st);
+int launch_cfl_dt(bool dbl, const void *vx, const void *vy, const void *vz, long long ncell,
+                  double cs, double dx, double cfl, double dt, double *part, int nb, double *dt_out,
+                  cudaStream_t st);
 int launch_accrete(bool dbl, void *psi, const void *pos, const void *vel, void *m_bh, int n,
                    double dx, double sigma_v, double G, double m_per_hbar, double c_light,
                    double dt, cudaStream_t st);

@@ -72,6 +72,11 @@ SIGNATURES = {
     "qj_plan_workspace_bytes": (c_int64, [c_void_p]),
     "qj_plan_status": (c_int, [c_void_p]),
     "qj_plan_get_tuning": (c_int, [c_void_p, c_void_p, c_int]),
+    "qj_bondi_ambient": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                 c_void_p, c_double, c_double, c_double, c_double, c_double,
+                                 c_double, c_double, c_void_p, c_void_p]),
+    "qj_hydro_cfl_dt": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_double, c_double,
+                                c_double, c_void_p, c_void_p]),
     "qj_plan_set_tuning": (c_int, [c_void_p, c_void_p, c_int]),
     "qj_autotune_kdk": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_double,
                                 c_double, c_int, c_void_p]),

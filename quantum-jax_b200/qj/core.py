@@ -269,6 +269,36 @@ class Plan:
             _stream()))
         return t_io.value
 
+    def bondi_ambient(self, rho, M_bh, x_bh, dt, v=None, v_bh=(0.0, 0.0, 0.0),
+                      r_acc_mult=2.5, lam=math.exp(1.5) / 4.0, fmax=None, ann_lo=1.1,
+                      ann_hi=1.8):
+        """bh_bondi_step_ambient (quantum-fluid-accretion.py:440-510): rho is
+        updated in place; returns (dMdt_target, rho_inf, rB, dM_cap, r_acc,
+        M_avail, dM_uncl).  v = (vx, vy, vz) adds the BHL term with v_bh."""
+        self._field(rho, "rho")
+        if v is not None:
+            for c, name in zip(v, ("vx", "vy", "vz")):
+                self._field(c, name)
+        out = torch.zeros(7, dtype=torch.float64, device=rho.device)
+        xb = (ctypes.c_double * 3)(*[float(c) for c in x_bh])
+        vb = (ctypes.c_double * 3)(*[float(c) for c in v_bh])
+        check(lib().qj_bondi_ambient(
+            self._h, _ptr(rho), _ptr(v[0]) if v is not None else None,
+            _ptr(v[1]) if v is not None else None, _ptr(v[2]) if v is not None else None,
+            xb, vb, float(M_bh), float(dt), float(r_acc_mult), float(lam),
+            float(fmax) if fmax is not None else 0.0, float(ann_lo), float(ann_hi), _ptr(out),
+            _stream()))
+        return tuple(float(x) for x in out.cpu())
+
+    def hydro_cfl_dt(self, vx, vy, vz, cs, cfl, dt):
+        """min(dt, cfl dx / max(cs + |v|)), quantum-fluid-accretion.py:697-701."""
+        for c, name in ((vx, "vx"), (vy, "vy"), (vz, "vz")):
+            self._field(c, name)
+        out = torch.zeros(1, dtype=torch.float64, device=vx.device)
+        check(lib().qj_hydro_cfl_dt(self._h, _ptr(vx), _ptr(vy), _ptr(vz), float(cs), float(cfl),
+                                    float(dt), _ptr(out), _stream()))
+        return float(out.cpu())
+
     def kdk_cosmo(self, psi, a, da, H0, omega_m, omega_l, nsteps=1):
         """nsteps x compute_step(psi, a) of quantum-cosmo.py:169-196, in place;
         returns the new scale factor a."""

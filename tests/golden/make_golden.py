@@ -114,6 +114,12 @@ class _Inert:
     def __call__(self, *a, **k):
         return _Inert()
 
+    def __getitem__(self, key):
+        return _Inert()
+
+    def __setitem__(self, key, value):
+        pass
+
 
 def _install_stubs():
     jnp = _proxy_module("jax.numpy", np)
@@ -143,7 +149,8 @@ def _install_stubs():
     for name in (
         "orbax", "orbax.checkpoint", "matplotlib", "matplotlib.pyplot",
         "matplotlib.animation", "matplotlib.patches", "h5py", "IPython",
-        "IPython.display",
+        "IPython.display", "imageio_ffmpeg", "imageio", "imageio.v2", "imageio.v3",
+        "cmasher", "matplotlib.patheffects",
     ):
         m = types.ModuleType(name)
         m.__getattr__ = lambda attr: _Inert()
@@ -359,6 +366,40 @@ def gen_bondi(ref_dir):
     np.savez_compressed(os.path.join(HERE, "bondi_res1.npz"), **out)
 
 
+def gen_bondi_ambient(ref_dir):
+    """bh_bondi_step_ambient (quantum-fluid-accretion.py:440-510), with and
+    without the BHL velocity term, and the hydro CFL step (:697-701) with the
+    script's own cs2_local and HYDRO_CFL."""
+    ref = load_reference(ref_dir, "quantum-fluid-accretion.py", [])
+    n, L, dx = ref.nx, ref.Lx, ref.dx
+    rho = ref.rho_gas * (1.0 + 0.05 * O.delta_field(n, 9))
+    rng = np.random.default_rng(10)
+    vx, vy, vz = (5.0 * rng.standard_normal((n, n, n)) for _ in range(3))
+    x_bh = np.array([0.5 * L, 0.52 * L, 0.47 * L])
+    v_bh = (12.0, -7.0, 3.0)
+    out = {}
+    out["const.grid"] = np.array([n, n, n, L, L, L])
+    out["const.cs"] = np.array(ref.cs_const)
+    out["const.G"] = np.array(ref.G)
+    out["const.dt"] = np.array(ref.dt)
+    out["const.r_acc_mult"] = np.array(ref.R_ACC_MULT)
+    out["const.ann"] = np.array([ref.ann_lo, ref.ann_hi])
+    out["input.rho_gas"] = np.array(ref.rho_gas)
+    for tag, M, bhl in (("m1e8", 1.0e8, False), ("m1e10_bhl", 1.0e10, True)):
+        kw = dict(vx=_as_at(vx), vy=_as_at(vy), vz=_as_at(vz), vxbh=v_bh[0], vybh=v_bh[1],
+                  vzbh=v_bh[2]) if bhl else {}
+        r = ref.bh_bondi_step_ambient(rho=_as_at(rho), M_bh_eff=M, x_bh=_as_at(x_bh), dx=dx,
+                                      Lx=L, cs_iso=ref.cs_const, G=ref.G, dt=ref.dt, **kw)
+        summarize(f"amb.{tag}.rho", plain(r[0]), out)
+        out[f"amb.{tag}.scalars"] = np.array([float(v) for v in r[1:]])
+    c_eff = np.sqrt(plain(ref.cs2_local(_as_at(rho))))
+    vmag = np.sqrt(vx * vx + vy * vy + vz * vz)
+    out["cfl.dt_eff"] = np.array(min(ref.dt, ref.HYDRO_CFL * dx / (np.max(c_eff + vmag) + 1e-30)))
+    out["cfl.dt_big"] = np.array(min(1.0, ref.HYDRO_CFL * dx / (np.max(c_eff + vmag) + 1e-30)))
+    out["const.hydro_cfl"] = np.array(ref.HYDRO_CFL)
+    np.savez_compressed(os.path.join(HERE, "bondi_ambient.npz"), **out)
+
+
 def gen_bh(ref_dir):
     ref = load_reference(ref_dir, "quantum-bh.py", ["--res", "1"])
     n, L = ref.nx, ref.Lx
@@ -428,7 +469,7 @@ def main():
     ap.add_argument("ref_dir", nargs="?", default="/root/reference")
     ap.add_argument("--only", default=None, help="generate one case, e.g. gen_ics")
     a = ap.parse_args()
-    fns = (gen_stars, gen_gasbh, gen_tidal, gen_cosmo, gen_bondi, gen_bh, gen_ics)
+    fns = (gen_stars, gen_gasbh, gen_tidal, gen_cosmo, gen_bondi, gen_bh, gen_ics, gen_bondi_ambient)
     for fn in fns:
         if a.only and fn.__name__ != a.only:
             continue

@@ -130,3 +130,49 @@ def test_hydro_uniform_state_is_fixed_point_and_mass_conserved():
     got, _ = run(qj.PLAIN_F64, g, p, [psi, rho2, v, -v, 0.5 * v, np.zeros(1), np.zeros((1, 3)),
                                       np.zeros((1, 3))], dt, 3, dm_acc=False)
     assert got[1].sum() == pytest.approx(rho2.sum(), rel=1e-13)
+
+
+def ambient_case(n=64, L=10.0, seed=9):
+    rho = 1.0e6 * (1.0 + 0.05 * O.delta_field(n, seed))
+    rng = np.random.default_rng(10)
+    v = tuple(5.0 * rng.standard_normal((n, n, n)) for _ in range(3))
+    return rho, v, np.array([0.5 * L, 0.52 * L, 0.47 * L]), (12.0, -7.0, 3.0)
+
+
+@pytest.mark.parametrize("dbl", [True, False])
+@pytest.mark.parametrize("M,bhl", [(1.0e8, False), (1.0e10, True)])
+def test_bondi_ambient_vs_oracle(dbl, M, bhl):
+    """bh_bondi_step_ambient (quantum-fluid-accretion.py:440-510) on the GPU
+    against the oracle (itself pinned to the reference's own function)."""
+    import qj
+
+    n, L, G, cs, dt = 64, 10.0, 4.30241002e-6, 60.0, 3.7e-5
+    rho, v, x_bh, v_bh = ambient_case(n, L)
+    ref = O.bondi_sink_ambient(rho, M, x_bh, L / n, L, cs, G, dt, v=v if bhl else None, v_bh=v_bh)
+    prec = qj.PLAIN_F64 if dbl else qj.FUSED_F32
+    rt = torch.float64 if dbl else torch.float32
+    plan = qj.Plan(qj.Grid(n, n, n, L, L, L), qj.Phys(G=G, cs=cs), prec, 1)
+    r = torch.as_tensor(rho, dtype=rt, device="cuda").contiguous()
+    vt = tuple(torch.as_tensor(c, dtype=rt, device="cuda").contiguous() for c in v)
+    out = plan.bondi_ambient(r, M, x_bh, dt, v=vt if bhl else None, v_bh=v_bh)
+    tol = 1e-12 if dbl else 1e-6
+    assert O.rel_l2(r.cpu().numpy(), ref[0]) < tol
+    np.testing.assert_allclose(out, np.array(ref[1:], dtype=float), rtol=1e-11 if dbl else 1e-5)
+    plan.close()
+
+
+@pytest.mark.parametrize("dbl", [True, False])
+def test_hydro_cfl_vs_oracle(dbl):
+    import qj
+
+    n, L = 32, 10.0
+    _, v, _, _ = ambient_case(n, L)
+    rt = torch.float64 if dbl else torch.float32
+    plan = qj.Plan(qj.Grid(n, n, n, L, L, L), qj.Phys(cs=60.0),
+                   qj.PLAIN_F64 if dbl else qj.FUSED_F32, 1)
+    vt = [torch.as_tensor(c, dtype=rt, device="cuda").contiguous() for c in v]
+    for dt in (3.7e-5, 1.0):
+        got = plan.hydro_cfl_dt(*vt, 60.0, 0.15, dt)
+        vv = [c.cpu().numpy().astype(np.float64) for c in vt]
+        assert got == pytest.approx(O.hydro_cfl_dt(*vv, 60.0, L / n, 0.15, dt), rel=1e-14)
+    plan.close()

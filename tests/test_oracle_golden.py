@@ -158,6 +158,37 @@ def test_bondi_golden():
         np.testing.assert_allclose(np.array(r[1:], dtype=float), f[f"bondi.{tag}.scalars"], rtol=RTOL)
 
 
+def ambient_inputs(f):
+    g = grid_from(f)
+    n = g.nx
+    rho = float(f["input.rho_gas"]) * (1.0 + 0.05 * O.delta_field(n, 9))
+    rng = np.random.default_rng(10)
+    v = tuple(5.0 * rng.standard_normal((n, n, n)) for _ in range(3))
+    return g, rho, v, np.array([0.5 * g.Lx, 0.52 * g.Lx, 0.47 * g.Lx]), (12.0, -7.0, 3.0)
+
+
+def test_bondi_ambient_golden():
+    f = load("bondi_ambient.npz")
+    g, rho, v, x_bh, v_bh = ambient_inputs(f)
+    lo, hi = (float(x) for x in f["const.ann"])
+    for tag, M, bhl in (("m1e8", 1.0e8, False), ("m1e10_bhl", 1.0e10, True)):
+        r = O.bondi_sink_ambient(rho, M, x_bh, g.dx, g.Lx, float(f["const.cs"]),
+                                 float(f["const.G"]), float(f["const.dt"]),
+                                 r_acc_mult=float(f["const.r_acc_mult"]), ann_lo=lo, ann_hi=hi,
+                                 v=v if bhl else None, v_bh=v_bh)
+        check(f, f"amb.{tag}.rho", r[0])
+        np.testing.assert_allclose(np.array(r[1:], dtype=float), f[f"amb.{tag}.scalars"], rtol=RTOL)
+
+
+def test_hydro_cfl_golden():
+    f = load("bondi_ambient.npz")
+    g, rho, v, _, _ = ambient_inputs(f)
+    cfl, cs = float(f["const.hydro_cfl"]), float(f["const.cs"])
+    assert O.hydro_cfl_dt(*v, cs, g.dx, cfl, float(f["const.dt"])) == pytest.approx(
+        float(f["cfl.dt_eff"]), rel=1e-14)
+    assert O.hydro_cfl_dt(*v, cs, g.dx, cfl, 1.0) == pytest.approx(float(f["cfl.dt_big"]), rel=1e-14)
+
+
 def test_bh_golden():
     f = load("bh_res1.npz")
     g = grid_from(f)
