@@ -599,6 +599,213 @@ def hydro_cfl_dt(vx, vy, vz, cs, dx, cfl, dt):
 
 
 # ---------------------------------------------------------------------------
+# quantum-fluid-accretion.py: the kick-drift-kick step with a moving, softened,
+# accreting black hole seeded at the dark-matter peak (:695-870)
+# ---------------------------------------------------------------------------
+
+
+@dataclasses.dataclass
+class FaccParams:
+    """The toggles and constants of quantum-fluid-accretion.py:41-100, 670-690."""
+
+    cs: float = 60.0
+    hydro_cfl: float = 0.15
+    bh_on: bool = True
+    bh_grav: bool = True
+    bh_move: bool = True
+    bh_accretion: bool = True
+    bh_init_m: float = 1.0e7
+    bh_inject_t: float = 13.0
+    ramp_on: bool = True
+    ramp_center: float = 13.0
+    ramp_w: float = 1.0
+    r_acc_mult: float = 2.5
+    lam: float = LAMBDA_ISO
+    fmax: float | None = None
+    ann_lo: float = 1.1
+    ann_hi: float = 1.8
+    k_cut_frac: float = 0.6
+    inject_smooth_on: bool = True
+    inject_smooth_kpc: float = 0.0
+    rho_gas: float = 1.0e6  # reported as rho_inf while the sink is inactive
+
+
+def facc_seed_mass(t, placed, q: FaccParams):
+    """seed_mass_from_time, :682-690."""
+    pl = 1.0 if placed > 0.5 else 0.0
+    if q.ramp_on:
+        s = 0.5 * (1.0 + math.tanh((t - q.ramp_center) / (q.ramp_w + 1e-30)))
+        s = s * (1.0 if t >= q.bh_inject_t else 0.0)
+    else:
+        s = 1.0 if t >= q.bh_inject_t else 0.0
+    return q.bh_init_m * s * pl
+
+
+def facc_potential(rho_src, rho_bg, g: Grid, G, k_sq):
+    """get_potential_bg, :182-185 -> (V_hat, V)."""
+    V_hat = -np.fft.fftn(4.0 * np.pi * G * (rho_src - rho_bg)) / (k_sq + (k_sq == 0))
+    return V_hat, np.real(np.fft.ifftn(V_hat))
+
+
+def facc_accel(V_hat, k):
+    """accel_from_Vhat, :187-191."""
+    kx, ky, kz = k[0], k[1], k[2]
+    return tuple(-np.real(np.fft.ifftn(1.0j * kd * V_hat)) for kd in (kx, ky, kz))
+
+
+def facc_cic(x_bh, dx, n):
+    """CIC cells and weights of a point, :388-417 / 419-437 (corner order of both)."""
+    xi = np.asarray(x_bh) / dx - 0.5
+    i0 = np.floor(xi).astype(int)
+    f = xi - i0
+    w = np.array([(1 - f[0]) * (1 - f[1]) * (1 - f[2]), f[0] * (1 - f[1]) * (1 - f[2]),
+                  (1 - f[0]) * f[1] * (1 - f[2]), (1 - f[0]) * (1 - f[1]) * f[2],
+                  f[0] * f[1] * (1 - f[2]), f[0] * (1 - f[1]) * f[2],
+                  (1 - f[0]) * f[1] * f[2], f[0] * f[1] * f[2]])
+    off = ((0, 0, 0), (1, 0, 0), (0, 1, 0), (0, 0, 1), (1, 1, 0), (1, 0, 1), (0, 1, 1), (1, 1, 1))
+    cells = [tuple(int((i0[d] + o[d]) % n) for d in range(3)) for o in off]
+    return cells, w
+
+
+def facc_bh_density(M, x_bh, dx, n):
+    rho = np.zeros((n, n, n))
+    cells, w = facc_cic(x_bh, dx, n)
+    for c, wk in zip(cells, w):
+        rho[c] += wk * M / dx**3
+    return rho
+
+
+def facc_sample(field, x_bh, dx, n):
+    cells, w = facc_cic(x_bh, dx, n)
+    return float(np.sum(w * np.array([field[c] for c in cells])))
+
+
+def facc_hydro(rho, vx, vy, vz, dt, dx, cs):
+    """solve_hydro of quantum-fluid-accretion.py:273-317 (limited pressure
+    gradient, constant c^2 from cs2_local, eps-guarded divisions)."""
+    vol = dx**3
+    eps = 1e-30
+    c2 = np.full_like(rho, cs * cs)
+    P = rho * c2
+    grads = [get_gradient(f, dx) for f in (rho, vx, vy, vz, P)]
+    lim = [slope_limiter(f, dx, *gd) for f, gd in zip((rho, vx, vy, vz, P), grads)]
+    (rdx, rdy, rdz), (uxx, uxy, uxz), (uyx, uyy, uyz), (uzx, uzy, uzz), (Px, Py, Pz) = lim
+    rho_p = rho - 0.5 * dt * (vx * rdx + rho * uxx + vy * rdy + rho * uyy + vz * rdz + rho * uzz)
+    vx_p = vx - 0.5 * dt * (vx * uxx + vy * uxy + vz * uxz + Px / (rho + eps))
+    vy_p = vy - 0.5 * dt * (vx * uyx + vy * uyy + vz * uyz + Py / (rho + eps))
+    vz_p = vz - 0.5 * dt * (vx * uzx + vy * uzy + vz * uzz + Pz / (rho + eps))
+    R_ = extrap_to_face(rho_p, rdx, rdy, rdz, dx)
+    X_ = extrap_to_face(vx_p, uxx, uxy, uxz, dx)
+    Y_ = extrap_to_face(vy_p, uyx, uyy, uyz, dx)
+    Z_ = extrap_to_face(vz_p, uzx, uzy, uzz, dx)
+
+    def flux(rL, uL, aL, bL, rR, uR, aR, bR, c2L, c2R):
+        rs = 0.5 * (rL + rR)
+        mu = 0.5 * (rL * uL + rR * uR)
+        ma = 0.5 * (rL * aL + rR * aR)
+        mb = 0.5 * (rL * bL + rR * bR)
+        Ps = rs * 0.5 * (c2L + c2R)
+        fM, fU = mu, mu**2 / (rs + eps) + Ps
+        fA, fB = mu * ma / (rs + eps), mu * mb / (rs + eps)
+        C = np.maximum(np.sqrt(c2L) + np.abs(uL), np.sqrt(c2R) + np.abs(uR))
+        return (fM - C * 0.5 * (rR - rL), fU - C * 0.5 * (rR * uR - rL * uL),
+                fA - C * 0.5 * (rR * aR - rL * aL), fB - C * 0.5 * (rR * bR - rL * bL))
+
+    c2R = [np.roll(c2, -1, axis=a) for a in range(3)]
+    FX = flux(R_[0], X_[0], Y_[0], Z_[0], R_[1], X_[1], Y_[1], Z_[1], c2, c2R[0])
+    FYr = flux(R_[2], Y_[2], Z_[2], X_[2], R_[3], Y_[3], Z_[3], X_[3], c2, c2R[1])
+    FZr = flux(R_[4], Z_[4], X_[4], Y_[4], R_[5], Z_[5], X_[5], Y_[5], c2, c2R[2])
+    FY = (FYr[0], FYr[3], FYr[1], FYr[2])  # (M, My, Mz, Mx) -> (M, Mx, My, Mz)
+    FZ = (FZr[0], FZr[2], FZr[3], FZr[1])  # (M, Mz, Mx, My) -> (M, Mx, My, Mz)
+    U = get_conserved(rho, vx, vy, vz, vol)
+    U = [apply_fluxes(U[i], FX[i], FY[i], FZ[i], dx, dt) for i in range(4)]
+    Mass = U[0]
+    return Mass / vol, U[1] / (Mass + eps), U[2] / (Mass + eps), U[3] / (Mass + eps)
+
+
+def facc_compute_step(psi, rho, vx, vy, vz, t, M_acc, x_bh, v_bh, placed, g: Grid, p: Phys,
+                      q: FaccParams, dt, k=None):
+    """compute_step of quantum-fluid-accretion.py:695-870, float64.  Returns
+    (psi, rho, vx, vy, vz, t, M_bh_eff_out, M_acc, x_bh, v_bh, placed, diag) with
+    diag = (dMdt, rho_inf, r_B, dMdt_real, cap_ratio, r_acc_eff)."""
+    k = k if k is not None else kgrid(g)
+    k_sq = k[3]
+    n, dx, L, G, mph, cs = g.nx, g.dx, g.Lx, p.G, p.m_per_hbar, q.cs
+    x_bh = np.array(x_bh, dtype=float)
+    v_bh = np.array(v_bh, dtype=float)
+    dt_eff = hydro_cfl_dt(vx, vy, vz, cs, dx, q.hydro_cfl, dt)
+    M_eff = facc_seed_mass(t, placed, q) + M_acc
+    r_soft = q.r_acc_mult * dx
+    rho_bg = np.mean(np.abs(psi) ** 2) + np.mean(rho)
+    k_cut = q.k_cut_frac * (np.pi / dx)
+    LP = np.exp(-((k_sq / (k_cut**2 + 1e-30)) ** 4))
+    active = 1.0 if placed > 0.5 else 0.0
+
+    def bh_kick(psi_, v_bh_):
+        Vh, _ = facc_potential(np.abs(psi_) ** 2 + rho, rho_bg, g, G, k_sq)
+        a = facc_accel(Vh * LP, k)
+        return v_bh_ + np.array([facc_sample(ad, x_bh, dx, n) for ad in a]) * (dt_eff / 2.0) * active
+
+    if q.bh_on and q.bh_move:
+        v_bh = bh_kick(psi, v_bh)
+    rho_src = np.abs(psi) ** 2 + rho
+
+    def soft_bh(M, r):
+        if not (q.bh_on and q.bh_grav):
+            return 0.0
+        hat = np.fft.fftn(facc_bh_density(M, x_bh, dx, n)) * np.exp(-0.5 * r * r * k_sq)
+        on = 1.0 if (placed > 0.5 and M > 0.0) else 0.0
+        return np.real(np.fft.ifftn(hat)) * on
+
+    Vh, V = facc_potential(rho_src + soft_bh(M_eff, r_soft), rho_bg, g, G, k_sq)
+    psi = np.exp(-1.0j * mph * dt_eff / 2.0 * V) * psi
+    ax, ay, az = facc_accel(Vh, k)
+    vx, vy, vz = vx + ax * (dt_eff / 2.0), vy + ay * (dt_eff / 2.0), vz + az * (dt_eff / 2.0)
+    psi = np.fft.ifftn(np.exp(dt_eff * (-1.0j * k_sq / mph / 2.0)) * np.fft.fftn(psi))
+    rho, vx, vy, vz = facc_hydro(rho, vx, vy, vz, dt_eff, dx, cs)
+    if q.bh_on and q.bh_move:
+        x_bh = np.mod(x_bh + dt_eff * v_bh * active, L)
+    active_acc = 1.0 if (placed > 0.5 and M_eff > 0.0) else 0.0
+    dMdt = dMdt_real = cap_ratio = r_B = 0.0
+    rho_inf = q.rho_gas
+    r_acc_eff = max(q.r_acc_mult * dx, 2.0 * (G * M_eff / (cs**2 + 1e-30)))
+    if q.bh_on and q.bh_accretion:
+        r = bondi_sink_ambient(rho, M_eff, x_bh, dx, L, cs, G, dt_eff, r_acc_mult=q.r_acc_mult,
+                               lam=q.lam, fmax=q.fmax, ann_lo=q.ann_lo, ann_hi=q.ann_hi,
+                               v=(vx, vy, vz), v_bh=tuple(v_bh))
+        rho_try, dMdt_try, rho_inf_try, r_B_try, dM_cap, r_acc_used, _, dM_uncl = r
+        rho = rho * (1.0 - active_acc) + rho_try * active_acc
+        dMdt = dMdt_try * active_acc
+        rho_inf = rho_inf_try * active_acc + (1.0 - active_acc) * q.rho_gas
+        r_B = r_B_try * active_acc
+        M_acc = M_acc + dM_cap * active_acc
+        dMdt_real = dM_cap / (dt_eff + 1e-30) if active_acc > 0.5 else 0.0
+        cap_ratio = dM_cap / (dM_uncl + 1e-30) if (dM_uncl > 0.0 and active_acc > 0.5) else 0.0
+        r_acc_eff = r_acc_used * active_acc + (1.0 - active_acc) * r_acc_eff
+    M_mid = facc_seed_mass(t, placed, q) + M_acc
+    Vh2, V2 = facc_potential(np.abs(psi) ** 2 + rho + soft_bh(M_mid, r_acc_eff), rho_bg, g, G,
+                             k_sq)
+    psi = np.exp(-1.0j * mph * dt_eff / 2.0 * V2) * psi
+    ax, ay, az = facc_accel(Vh2, k)
+    vx, vy, vz = vx + ax * (dt_eff / 2.0), vy + ay * (dt_eff / 2.0), vz + az * (dt_eff / 2.0)
+    if q.bh_on and q.bh_move:
+        v_bh = bh_kick(psi, v_bh)
+    t = t + dt_eff
+    if placed < 0.5 and t >= q.bh_inject_t:
+        rho3 = np.abs(psi) ** 2
+        if q.inject_smooth_on:
+            s2 = max(q.inject_smooth_kpc, 1.5 * dx) ** 2
+            rho3 = np.real(np.fft.ifftn(np.fft.fftn(rho3) * np.exp(-0.5 * s2 * k_sq)))
+        i0, j0, k0 = np.unravel_index(np.argmax(rho3), rho3.shape)
+        x_bh = np.array([(i0 + 0.5) * dx, (j0 + 0.5) * dx, (k0 + 0.5) * dx])
+        v_bh = np.zeros(3)
+        placed = 1.0
+    M_out = facc_seed_mass(t, placed, q) + M_acc
+    return (psi, rho, vx, vy, vz, t, M_out, M_acc, x_bh, v_bh, placed,
+            (dMdt, rho_inf, r_B, dMdt_real, cap_ratio, r_acc_eff))
+
+
+# ---------------------------------------------------------------------------
 # R16: the gas + black-hole step, quantum-gas-bh.py:537-578
 # ---------------------------------------------------------------------------
 

@@ -400,6 +400,59 @@ def gen_bondi_ambient(ref_dir):
     np.savez_compressed(os.path.join(HERE, "bondi_ambient.npz"), **out)
 
 
+def facc_params_of(ref):
+    """The step's toggles and constants as read from the loaded script."""
+    return np.array([ref.cs_const, ref.HYDRO_CFL, ref.BH_INIT_M, ref.BH_INJECT_T,
+                     ref.BH_RAMP_CENTER, ref.BH_RAMP_W, ref.R_ACC_MULT, ref.LAMBDA_ISO,
+                     ref.ann_lo, ref.ann_hi, ref.K_CUT_FRAC, ref.INJECT_SMOOTH_KPC, ref.rho_gas,
+                     float(ref.BH_ON), float(ref.BH_GRAV), float(ref.BH_MOVE),
+                     float(ref.BH_ACCRETION), float(ref.BH_RAMP_ON), float(ref.INJECT_SMOOTH_ON)])
+
+
+def facc_inputs(ref):
+    n = ref.nx
+    rho_dm = ref.rho_bar * ref.frac_dm * (1.0 + 0.1 * O.delta_field(n, 11))
+    psi = np.sqrt(rho_dm) * np.exp(1.0j * 0.3 * O.delta_field(n, 12))
+    rho = ref.rho_gas * (1.0 + 0.05 * O.delta_field(n, 13))
+    rng = np.random.default_rng(14)
+    v = [10.0 * rng.standard_normal((n, n, n)) for _ in range(3)]
+    return psi, rho, v
+
+
+def gen_facc(ref_dir):
+    """compute_step of quantum-fluid-accretion.py (:695-870), two steps from two
+    seeded states: one crossing the injection time (the black hole is placed
+    at the smoothed dark-matter peak), one with a placed, ramped, moving black
+    hole (softened gravity, low-pass force, ambient Bondi sink)."""
+    ref = load_reference(ref_dir, "quantum-fluid-accretion.py", [])
+    L = ref.Lx
+    psi0, rho0, v0 = facc_inputs(ref)
+    out = {"const.params": facc_params_of(ref), "const.grid": np.array([ref.nx, L, ref.dx]),
+           "const.G": np.array(ref.G), "const.m_per_hbar": np.array(ref.m_per_hbar),
+           "const.dt": np.array(ref.dt), "const.rho_bar": np.array(ref.rho_bar)}
+    cases = {
+        "inject": (ref.BH_INJECT_T - 0.5 * ref.dt, 0.0, [0.5 * L] * 3, [0.0, 0.0, 0.0], 0.0),
+        "massive": (ref.BH_RAMP_CENTER, 2.0e6, [0.43 * L, 0.55 * L, 0.61 * L], [20.0, -10.0, 5.0],
+                    1.0),
+    }
+    for tag, (t, M_acc, x_bh, v_bh, placed) in cases.items():
+        st = [_as_at(psi0), _as_at(rho0), _as_at(v0[0]), _as_at(v0[1]), _as_at(v0[2]), t, M_acc,
+              _as_at(np.array(x_bh)), v_bh[0], v_bh[1], v_bh[2], placed]
+        for step in (1, 2):
+            r = ref.compute_step(*st)
+            (psi, rho, vx, vy, vz, t, M_out, M_acc, x_b, vbx, vby, vbz, dMdt, rho_inf, r_B,
+             placed, dMdt_real, cap_ratio, r_acc_eff) = r[:19]
+            pre = f"{tag}.s{step}."
+            summarize(pre + "psi", plain(psi), out)
+            summarize(pre + "rho", plain(rho), out)
+            summarize(pre + "vx", plain(vx), out)
+            out[pre + "scalars"] = np.array([float(x) for x in (
+                t, M_out, M_acc, *plain(x_b), float(vbx), float(vby), float(vbz), float(placed),
+                dMdt, rho_inf, r_B, dMdt_real, cap_ratio, r_acc_eff)])
+            st = [psi, rho, vx, vy, vz, t, M_acc, x_b, vbx, vby, vbz, placed]
+    np.savez_compressed(os.path.join(HERE, "facc_steps.npz"), **out)
+
+
 def gen_bh(ref_dir):
     ref = load_reference(ref_dir, "quantum-bh.py", ["--res", "1"])
     n, L = ref.nx, ref.Lx
@@ -469,7 +522,7 @@ def main():
     ap.add_argument("ref_dir", nargs="?", default="/root/reference")
     ap.add_argument("--only", default=None, help="generate one case, e.g. gen_ics")
     a = ap.parse_args()
-    fns = (gen_stars, gen_gasbh, gen_tidal, gen_cosmo, gen_bondi, gen_bh, gen_ics, gen_bondi_ambient)
+    fns = (gen_stars, gen_gasbh, gen_tidal, gen_cosmo, gen_bondi, gen_bh, gen_ics, gen_bondi_ambient, gen_facc)
     for fn in fns:
         if a.only and fn.__name__ != a.only:
             continue

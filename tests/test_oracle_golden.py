@@ -203,3 +203,53 @@ def test_bh_golden():
                             float(f["const.dt"]), float(f["const.sigma"]))
     check(f, "do_accretion.psi", p2)
     np.testing.assert_allclose(m2, f["do_accretion.m_bh"], rtol=RTOL)
+
+
+def facc_setup(f):
+    prm = f["const.params"]
+    n, L, dx = int(f["const.grid"][0]), float(f["const.grid"][1]), float(f["const.grid"][2])
+    g = O.Grid(n, n, n, L, L, L)
+    p = O.Phys(m_per_hbar=float(f["const.m_per_hbar"]), G=float(f["const.G"]),
+               rho_bar=float(f["const.rho_bar"]))
+    q = O.FaccParams(cs=prm[0], hydro_cfl=prm[1], bh_init_m=prm[2], bh_inject_t=prm[3],
+                     ramp_center=prm[4], ramp_w=prm[5], r_acc_mult=prm[6], lam=prm[7],
+                     ann_lo=prm[8], ann_hi=prm[9], k_cut_frac=prm[10], inject_smooth_kpc=prm[11],
+                     rho_gas=prm[12], bh_on=bool(prm[13]), bh_grav=bool(prm[14]),
+                     bh_move=bool(prm[15]), bh_accretion=bool(prm[16]), ramp_on=bool(prm[17]),
+                     inject_smooth_on=bool(prm[18]))
+    return g, p, q
+
+
+def facc_inputs(n, rho_bar, rho_gas, frac_dm=0.9):
+    rho_dm = rho_bar * frac_dm * (1.0 + 0.1 * O.delta_field(n, 11))
+    psi = np.sqrt(rho_dm) * np.exp(1.0j * 0.3 * O.delta_field(n, 12))
+    rho = rho_gas * (1.0 + 0.05 * O.delta_field(n, 13))
+    rng = np.random.default_rng(14)
+    v = [10.0 * rng.standard_normal((n, n, n)) for _ in range(3)]
+    return psi, rho, v
+
+
+FACC_CASES = {"inject": ("bh_inject_t", 0.0, (0.5, 0.5, 0.5), (0.0, 0.0, 0.0), 0.0),
+              "massive": ("ramp_center", 2.0e6, (0.43, 0.55, 0.61), (20.0, -10.0, 5.0), 1.0)}
+
+
+@pytest.mark.parametrize("tag", ["inject", "massive"])
+def test_fluid_accretion_step_golden(tag):
+    f = load("facc_steps.npz")
+    g, p, q = facc_setup(f)
+    dt = float(f["const.dt"])
+    psi, rho, v = facc_inputs(g.nx, p.rho_bar, q.rho_gas)
+    t_key, M_acc, xf, v_bh, placed = FACC_CASES[tag]
+    t = getattr(q, t_key) - (0.5 * dt if tag == "inject" else 0.0)
+    x_bh = np.array(xf) * g.Lx
+    k = O.kgrid(g)
+    vx, vy, vz = v
+    for step in (1, 2):
+        psi, rho, vx, vy, vz, t, M_out, M_acc, x_bh, v_bh, placed, diag = O.facc_compute_step(
+            psi, rho, vx, vy, vz, t, M_acc, x_bh, v_bh, placed, g, p, q, dt, k)
+        pre = f"{tag}.s{step}."
+        check(f, pre + "psi", psi)
+        check(f, pre + "rho", rho)
+        check(f, pre + "vx", vx)
+        got = np.array([t, M_out, M_acc, *x_bh, *v_bh, placed, *diag])
+        np.testing.assert_allclose(got, f[pre + "scalars"], rtol=1e-9, atol=1e-12)
