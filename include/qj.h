@@ -219,6 +219,35 @@ int qj_bondi_ambient(qj_plan *plan, void *rho, const void *vx, const void *vy, c
                      double r_acc_mult, double lam, double fmax, double ann_lo, double ann_hi,
                      double *out, void *stream);
 
+/* compute_step of quantum-fluid-accretion.py (:695-870): kick-drift-kick
+ * with a black hole that is placed at the (smoothed) dark-matter peak at
+ * t >= bh_inject_t, grows by a tanh seed ramp plus ambient-shell Bondi
+ * accretion, moves under a low-pass-filtered force, and gravitates through a
+ * Gaussian-softened CIC density; hydro of that script (limited pressure
+ * gradient, local c^2 flux); dt_eff = min(dt, hydro CFL) per step.
+ * Plain float64 plans only (the reference runs with x64).  The black-hole
+ * state lives on the host (state), as the reference's control flow depends
+ * on it: each step synchronises the stream.  diag (host, may be NULL)
+ * receives the last step's diagnostics. */
+typedef struct {
+  double t, M_acc, x_bh[3], v_bh[3], placed;
+} qj_facc_state;
+typedef struct {
+  double cs, hydro_cfl;
+  int bh_on, bh_grav, bh_move, bh_accretion;
+  double bh_init_m, bh_inject_t;
+  int ramp_on;
+  double ramp_center, ramp_w, r_acc_mult, lam, fmax, ann_lo, ann_hi, k_cut_frac;
+  int inject_smooth_on;
+  double inject_smooth_kpc, rho_gas;
+} qj_facc_params;
+typedef struct {
+  double dMdt, rho_inf, r_B, dMdt_real, cap_ratio, r_acc_eff, M_bh_eff_out, dt_eff;
+} qj_facc_diag;
+int qj_fluid_accretion_step(qj_plan *plan, void *psi, void *rho, void *vx, void *vy, void *vz,
+                            qj_facc_state *state, const qj_facc_params *params, double dt,
+                            int nsteps, qj_facc_diag *diag, void *stream);
+
 /* Hydro CFL step, quantum-fluid-accretion.py:697-701 (constant sound speed
  * cs, cs2_local :248-250): dt_out (device double) = min(dt, cfl dx /
  * max(cs + |v|)). */

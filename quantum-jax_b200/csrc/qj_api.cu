@@ -146,6 +146,10 @@ struct qj_plan {
   unsigned *err = nullptr;  // set by a fused pass whose bounded tile wait gave up
   double *phi = nullptr;    // fused: per-box phase of the uniform potential (float64)
   double *cfl_part = nullptr;  // per-block maxima of the CFL reduction
+  // fluid-accretion step: softened black-hole density, small scalars, partials
+  void *facc_bh = nullptr;
+  double *facc_scal = nullptr, *facc_part = nullptr;
+  long long *facc_pi = nullptr;
   int tune[QJ_TUNE_N] = {0, 0, 0, 0, 0, 0, 0, 0, -1, 0};  // launch tuning (include/qj.h)
   void *tmp_scalar = nullptr;
   void *tmp_diag = nullptr;
@@ -990,6 +994,207 @@ int qj_hydro_cfl_dt(qj_plan *P, const void *vx, const void *vy, const void *vz, 
   if (!P->cfl_part) QJ_TRY(dev_alloc_t(P, &P->cfl_part, (size_t)nb));
   return launch_cfl_dt(P->dbl, vx, vy, vz, P->ncell, cs, P->g.Lx / P->n[0], cfl, dt,
                        P->cfl_part, nb, dt_out, (cudaStream_t)stream);
+}
+
+}  // extern "C"
+
+namespace {
+// seed_mass_from_time, quantum-fluid-accretion.py:682-690
+double facc_seed(double t, double placed, const qj_facc_params &q) {
+  const double pl = placed > 0.5 ? 1.0 : 0.0;
+  double s;
+  if (q.ramp_on)
+    s = 0.5 * (1.0 + std::tanh((t - q.ramp_center) / (q.ramp_w + 1e-30))) *
+        (t >= q.bh_inject_t ? 1.0 : 0.0);
+  else
+    s = t >= q.bh_inject_t ? 1.0 : 0.0;
+  return q.bh_init_m * s * pl;
+}
+
+// One compute_step of quantum-fluid-accretion.py:695-870 (plain path).
+int facc_step(qj_plan *P, void *psi, void *rho, void *v[3], qj_facc_state &S,
+              const qj_facc_params &q, double dt, qj_facc_diag &D, cudaStream_t st) {
+  const bool dbl = P->dbl;
+  const long long nc = P->ncell;
+  const int n = P->n[0];
+  const double dx = P->g.Lx / n, L = P->g.Lx, G = P->ph.G, mph = P->ph.m_per_hbar, cs = q.cs;
+  const double fourpiG = 4.0 * M_PI * G;
+  const int nb = 592;
+  double *sc = P->facc_scal;  // [0] dt_eff, [2..3] means, [4..6] sample, [8..14] Bondi, [15] argmax
+  auto host = [&](int i, int cnt, double *dst) -> int {
+    QJ_CK(cudaMemcpyAsync(dst, sc + i, cnt * sizeof(double), cudaMemcpyDeviceToHost, st));
+    QJ_CK(cudaStreamSynchronize(st));
+    return 0;
+  };
+  // hydro CFL cap (:697-701)
+  QJ_TRY(launch_cfl_dt(dbl, v[0], v[1], v[2], nc, cs, dx, q.hydro_cfl, dt, P->cfl_part, nb, sc, st));
+  double dt_eff = 0.0;
+  QJ_TRY(host(0, 1, &dt_eff));
+  const double M_eff = facc_seed(S.t, S.placed, q) + S.M_acc;
+  const double r_soft = q.r_acc_mult * dx;
+  QJ_TRY(launch_mean_dm_gas(dbl, psi, rho, nc, P->facc_part, nb, sc + 2, st));
+  double means[2];
+  QJ_TRY(host(2, 2, means));
+  const double rho_bg = means[0] + means[1];
+  const double k_cut = q.k_cut_frac * (M_PI / dx);
+  const double active = S.placed > 0.5 ? 1.0 : 0.0;
+  // V^ of |psi|^2 + rho (+ rho_bh) against rho_bg into c0 (get_potential_bg, :182-185)
+  auto vhat = [&](const void *rho_bh) -> int {
+    QJ_TRY(launch_build_rho(dbl, psi, rho, rho_bh, nullptr, fourpiG, rho_bg, nullptr, P->c0, nc, st));
+    QJ_TRY(fft3d(P, P->c0, -1, st));
+    return launch_poisson_div(dbl, P->c0, ktabs(P), nc, st);
+  };
+  // the three accelerations -Re ifftn(i k_d V^) of c0 into ax, ay, az (accel_from_Vhat)
+  auto accel = [&]() -> int {
+    void *ag[3] = {P->ax, P->ay, P->az};
+    for (int d = 0; d < 3; ++d) {
+      QJ_TRY(launch_mul_ik(dbl, P->c0, d, ktabs(P), P->c1, nc, st));
+      QJ_TRY(fft3d(P, P->c1, +1, st));
+      QJ_TRY(launch_real_part(dbl, P->c1, -1.0, nullptr, 0.0, nullptr, ag[d], nc, st));
+    }
+    return 0;
+  };
+  // black-hole half kick with the low-passed force of the DM + gas potential
+  auto bh_kick = [&]() -> int {
+    QJ_TRY(vhat(nullptr));
+    QJ_TRY(launch_kfilter(dbl, P->c0, ktabs(P), 0, k_cut * k_cut, nc, st));
+    QJ_TRY(accel());
+    QJ_TRY(launch_cic_sample3(dbl, P->ax, P->ay, P->az, n, S.x_bh, dx, sc + 4, st));
+    double a[3];
+    QJ_TRY(host(4, 3, a));
+    for (int d = 0; d < 3; ++d) S.v_bh[d] = S.v_bh[d] + a[d] * (dt_eff / 2.0) * active;
+    return 0;
+  };
+  // Gaussian-softened CIC density of the black hole into facc_bh (:729-736)
+  // (out = nullptr when the black hole does not gravitate this kick)
+  auto soft_bh = [&](double M, double r, const void *&out) -> int {
+    out = nullptr;
+    if (!(q.bh_on && q.bh_grav) || !(S.placed > 0.5 && M > 0.0)) return 0;
+    QJ_CK(cudaMemsetAsync(P->facc_bh, 0, nc * P->rsz, st));
+    QJ_TRY(launch_cic_point(dbl, P->facc_bh, n, S.x_bh, dx, M, st));
+    QJ_TRY(launch_build_rho(dbl, nullptr, nullptr, nullptr, P->facc_bh, 1.0, 0.0, nullptr, P->c1,
+                            nc, st));
+    QJ_TRY(fft3d(P, P->c1, -1, st));
+    QJ_TRY(launch_kfilter(dbl, P->c1, ktabs(P), 1, r * r, nc, st));
+    QJ_TRY(fft3d(P, P->c1, +1, st));
+    QJ_TRY(launch_real_part(dbl, P->c1, 1.0, nullptr, 0.0, nullptr, P->facc_bh, nc, st));
+    out = P->facc_bh;
+    return 0;
+  };
+  // kick: psi and gas with the potential of |psi|^2 + rho + rho_bh
+  auto kick = [&](const void *rho_bh) -> int {
+    QJ_TRY(vhat(rho_bh));
+    QJ_CK(cudaMemcpyAsync(P->c1, P->c0, nc * P->csz, cudaMemcpyDeviceToDevice, st));
+    QJ_TRY(fft3d(P, P->c1, +1, st));
+    QJ_TRY(launch_real_part(dbl, P->c1, 1.0, nullptr, 0.0, nullptr, P->V, nc, st));
+    QJ_TRY(launch_kick_plain(dbl, psi, P->V, mph * dt_eff / 2.0, nc, st));
+    QJ_TRY(accel());
+    return launch_gas_kick(dbl, v[0], v[1], v[2], P->ax, P->ay, P->az, dt_eff / 2.0, nc, st);
+  };
+  if (q.bh_on && q.bh_move) QJ_TRY(bh_kick());
+  {
+    const void *bh = nullptr;
+    QJ_TRY(soft_bh(M_eff, r_soft, bh));
+    QJ_TRY(kick(bh));
+  }
+  // drift (quantum + hydro)
+  QJ_TRY(fft3d(P, psi, -1, st));
+  QJ_TRY(launch_drift_mul(dbl, psi, ktabs(P), dt_eff, mph, nc, st));
+  QJ_TRY(fft3d(P, psi, +1, st));
+  QJ_TRY(launch_hydro(dbl, rho, v[0], v[1], v[2], P->gas_prim, n, dx, dt_eff, cs, 0, st,
+                      P->tune[9] > 0 ? P->tune[9] : 256, true));
+  if (q.bh_on && q.bh_move)
+    for (int d = 0; d < 3; ++d) {
+      const double x = S.x_bh[d] + dt_eff * S.v_bh[d] * active;
+      S.x_bh[d] = x - L * std::floor(x / L);
+    }
+  // ambient-shell Bondi accretion (:770-800)
+  const double active_acc = (S.placed > 0.5 && M_eff > 0.0) ? 1.0 : 0.0;
+  D.dMdt = D.dMdt_real = D.cap_ratio = D.r_B = 0.0;
+  D.rho_inf = q.rho_gas;
+  D.r_acc_eff = std::max(q.r_acc_mult * dx, 2.0 * (G * M_eff / (cs * cs + 1e-30)));
+  if (q.bh_on && q.bh_accretion && active_acc > 0.5) {
+    QJ_TRY(launch_bondi_ambient(dbl, rho, v[0], v[1], v[2], n, dx, L, S.x_bh, S.v_bh, M_eff, cs, G,
+                                dt_eff, q.r_acc_mult, q.lam, q.fmax, q.ann_lo, q.ann_hi, sc + 8, st));
+    double o[7];
+    QJ_TRY(host(8, 7, o));
+    D.dMdt = o[0];
+    D.rho_inf = o[1];
+    D.r_B = o[2];
+    S.M_acc = S.M_acc + o[3];
+    D.dMdt_real = o[3] / (dt_eff + 1e-30);
+    D.cap_ratio = o[6] > 0.0 ? o[3] / (o[6] + 1e-30) : 0.0;
+    D.r_acc_eff = o[4];
+  }
+  // second kick (:806-830)
+  {
+    const double M_mid = facc_seed(S.t, S.placed, q) + S.M_acc;
+    const void *bh = nullptr;
+    QJ_TRY(soft_bh(M_mid, D.r_acc_eff, bh));
+    QJ_TRY(kick(bh));
+  }
+  if (q.bh_on && q.bh_move) QJ_TRY(bh_kick());
+  S.t = S.t + dt_eff;
+  // black-hole site at the smoothed dark-matter peak, once (:836-860)
+  if (S.placed < 0.5 && S.t >= q.bh_inject_t) {
+    QJ_TRY(launch_build_rho(dbl, psi, nullptr, nullptr, nullptr, 1.0, 0.0, P->rho_tot, P->c1, nc, st));
+    if (q.inject_smooth_on) {
+      const double s = std::max(q.inject_smooth_kpc, 1.5 * dx);
+      QJ_TRY(fft3d(P, P->c1, -1, st));
+      QJ_TRY(launch_kfilter(dbl, P->c1, ktabs(P), 1, s * s, nc, st));
+      QJ_TRY(fft3d(P, P->c1, +1, st));
+      QJ_TRY(launch_real_part(dbl, P->c1, 1.0, nullptr, 0.0, nullptr, P->rho_tot, nc, st));
+    }
+    QJ_TRY(launch_argmax(dbl, P->rho_tot, nc, P->facc_part, P->facc_pi, nb, sc + 15, st));
+    double idx = 0.0;
+    QJ_TRY(host(15, 1, &idx));
+    const long long c = (long long)idx;
+    const long long ii[3] = {c / ((long long)n * n), (c / n) % n, c % n};
+    for (int d = 0; d < 3; ++d) {
+      S.x_bh[d] = ((double)ii[d] + 0.5) * dx;
+      S.v_bh[d] = 0.0;
+    }
+    S.placed = 1.0;
+  }
+  D.M_bh_eff_out = facc_seed(S.t, S.placed, q) + S.M_acc;
+  D.dt_eff = dt_eff;
+  return 0;
+}
+}  // namespace
+
+extern "C" {
+
+int qj_fluid_accretion_step(qj_plan *P, void *psi, void *rho, void *vx, void *vy, void *vz,
+                            qj_facc_state *state, const qj_facc_params *params, double dt,
+                            int nsteps, qj_facc_diag *diag, void *stream) {
+  if (!P || !psi || !rho || !vx || !vy || !vz || !state || !params || !(dt > 0) || nsteps < 0) {
+    set_error("qj_fluid_accretion_step: bad argument");
+    return QJ_ERR_ARG;
+  }
+  QJ_ONE_BOX(P, "qj_fluid_accretion_step");
+  if (!P->dbl) {
+    set_error("qj_fluid_accretion_step: needs a PLAIN_F64 plan (the reference runs in float64)");
+    return QJ_ERR_ARG;
+  }
+  if (P->n[0] != P->n[1] || P->n[0] != P->n[2] || P->g.Lx != P->g.Ly || P->g.Lx != P->g.Lz) {
+    set_error("qj_fluid_accretion_step: needs a cubic grid and box");
+    return QJ_ERR_ARG;
+  }
+  QJ_TRY(ensure_plain_ws(P));
+  QJ_TRY(ensure_gas_ws(P));
+  const int nb = 592;
+  if (!P->cfl_part) QJ_TRY(dev_alloc_t(P, &P->cfl_part, (size_t)nb));
+  if (!P->facc_bh) QJ_TRY(dev_alloc(P, &P->facc_bh, P->ncell * P->rsz));
+  if (!P->facc_scal) QJ_TRY(dev_alloc_t(P, &P->facc_scal, 16));
+  if (!P->facc_part) QJ_TRY(dev_alloc_t(P, &P->facc_part, (size_t)2 * nb));
+  if (!P->facc_pi) QJ_TRY(dev_alloc_t(P, &P->facc_pi, (size_t)nb));
+  void *v[3] = {vx, vy, vz};
+  qj_facc_diag D;
+  std::memset(&D, 0, sizeof(D));
+  for (int s = 0; s < nsteps; ++s)
+    QJ_TRY(facc_step(P, psi, rho, v, *state, *params, dt, D, (cudaStream_t)stream));
+  if (diag) *diag = D;
+  return QJ_OK;
 }
 
 int qj_plan_get_tuning(const qj_plan *P, int32_t *tune, int n) {

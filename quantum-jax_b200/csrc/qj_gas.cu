@@ -45,7 +45,10 @@ template <typename R> __device__ __forceinline__ R clamp01(R x) {
 
 // Limited gradients and half-step primitives of cell (x, y, z):
 // get_gradient (:188-193), slope_limiter (:340-395), predictor (:283-299).
-template <typename R>
+// FACC: solve_hydro of quantum-fluid-accretion.py:273-317 -- the velocity
+// predictor uses the limited gradient of P = rho c^2 divided by (rho + eps)
+// instead of c^2 grad(rho) / rho.
+template <typename R, bool FACC = false>
 __device__ Prim<R> cell_prim(const R *const F[4], const Idx3 &I, int x, int y, int z, R dx, R dt,
                              R cs) {
   Prim<R> P;
@@ -67,27 +70,60 @@ __device__ Prim<R> cell_prim(const R *const F[4], const Idx3 &I, int x, int y, i
   const R h = (R)0.5 * dt;
   P.f[0] = rho - h * (vx * P.g[0][0] + rho * P.g[1][0] + vy * P.g[0][1] + rho * P.g[2][1] +
                       vz * P.g[0][2] + rho * P.g[3][2]);
-  for (int v = 1; v < 4; ++v)
-    P.f[v] = c[v] - h * (vx * P.g[v][0] + vy * P.g[v][1] + vz * P.g[v][2] +
-                         ((R)1 / rho) * P.g[0][v - 1] * cs * cs);
+  if constexpr (FACC) {
+    const R c2 = cs * cs;
+    const R Pc = c[0] * c2;
+    R gP[3];
+    for (int d = 0; d < 3; ++d) {
+      const int ex = d == 0, ey = d == 1, ez = d == 2;
+      const R fp = F[0][I.at(x + ex, y + ey, z + ez)] * c2;
+      const R fm = F[0][I.at(x - ex, y - ey, z - ez)] * c2;
+      R g = (fp - fm) / ((R)2 * dx);
+      const R denom = adjust_denominator(g);
+      g = clamp01(((Pc - fm) / dx) / denom) * g;
+      g = clamp01((-(Pc - fp) / dx) / denom) * g;
+      gP[d] = g;
+    }
+    for (int v = 1; v < 4; ++v)
+      P.f[v] = c[v] - h * (vx * P.g[v][0] + vy * P.g[v][1] + vz * P.g[v][2] +
+                           gP[v - 1] / (rho + (R)1e-30));
+  } else {
+    for (int v = 1; v < 4; ++v)
+      P.f[v] = c[v] - h * (vx * P.g[v][0] + vy * P.g[v][1] + vz * P.g[v][2] +
+                           ((R)1 / rho) * P.g[0][v - 1] * cs * cs);
+  }
   return P;
 }
 
 // get_flux (:226-252) with the rotated variable order of :316-324.  u = the
 // velocity component normal to the face; w1, w2 the tangential ones.
-template <typename R>
+// FACC: get_flux_axis of quantum-fluid-accretion.py:252-271 (face-averaged
+// c^2, eps-guarded divisions, C = sqrt(c^2) + |u|).
+template <typename R, bool FACC = false>
 __device__ __forceinline__ void rusanov(R rL, R uL, R aL, R bL, R rR, R uR, R aR, R bR, R cs,
                                         R out[4]) {
   const R rho_star = (R)0.5 * (rL + rR);
   const R mu = (R)0.5 * (rL * uL + rR * uR);
   const R ma = (R)0.5 * (rL * aL + rR * aR);
   const R mb = (R)0.5 * (rL * bL + rR * bR);
-  const R P_star = rho_star * cs * cs;
-  R fM = mu;
-  R fU = mu * mu / rho_star + P_star;
-  R fA = mu * ma / rho_star;
-  R fB = mu * mb / rho_star;
-  const R C = fmax(cs + fabs(uL), cs + fabs(uR));
+  R fM, fU, fA, fB, C;
+  if constexpr (FACC) {
+    const R c2 = cs * cs;
+    const R P_star = rho_star * ((R)0.5 * (c2 + c2));
+    const R eps = (R)1e-30;
+    fM = mu;
+    fU = mu * mu / (rho_star + eps) + P_star;
+    fA = mu * ma / (rho_star + eps);
+    fB = mu * mb / (rho_star + eps);
+    C = fmax(sqrt(c2) + fabs(uL), sqrt(c2) + fabs(uR));
+  } else {
+    const R P_star = rho_star * cs * cs;
+    fM = mu;
+    fU = mu * mu / rho_star + P_star;
+    fA = mu * ma / rho_star;
+    fB = mu * mb / rho_star;
+    C = fmax(cs + fabs(uL), cs + fabs(uR));
+  }
   fM = fM - C * (R)0.5 * (rR - rL);
   fU = fU - C * (R)0.5 * (rR * uR - rL * uL);
   fA = fA - C * (R)0.5 * (rR * aR - rL * aL);
@@ -101,7 +137,7 @@ __device__ __forceinline__ void rusanov(R rL, R uL, R aL, R bL, R rR, R uR, R aR
 // Flux through the face between cell L and its +d neighbour R, returned in
 // conserved order (Mass, Momx, Momy, Momz).  Face states: extrap_to_face
 // (:196-209).
-template <typename R>
+template <typename R, bool FACC = false>
 __device__ void face_flux(const Prim<R> &L, const Prim<R> &Rt, int d, R dx, R cs, R out[4]) {
   R fl[4], fr[4];
   for (int v = 0; v < 4; ++v) {
@@ -110,19 +146,19 @@ __device__ void face_flux(const Prim<R> &L, const Prim<R> &Rt, int d, R dx, R cs
   }
   R o[4];
   if (d == 0) {
-    rusanov(fl[0], fl[1], fl[2], fl[3], fr[0], fr[1], fr[2], fr[3], cs, o);
+    rusanov<R, FACC>(fl[0], fl[1], fl[2], fl[3], fr[0], fr[1], fr[2], fr[3], cs, o);
     out[0] = o[0]; out[1] = o[1]; out[2] = o[2]; out[3] = o[3];
   } else if (d == 1) {  // (rho, vy, vz, vx) -> (Mass, Momy, Momz, Momx)
-    rusanov(fl[0], fl[2], fl[3], fl[1], fr[0], fr[2], fr[3], fr[1], cs, o);
+    rusanov<R, FACC>(fl[0], fl[2], fl[3], fl[1], fr[0], fr[2], fr[3], fr[1], cs, o);
     out[0] = o[0]; out[2] = o[1]; out[3] = o[2]; out[1] = o[3];
   } else {  // (rho, vz, vx, vy) -> (Mass, Momz, Momx, Momy)
-    rusanov(fl[0], fl[3], fl[1], fl[2], fr[0], fr[3], fr[1], fr[2], cs, o);
+    rusanov<R, FACC>(fl[0], fl[3], fl[1], fl[2], fr[0], fr[3], fr[1], fr[2], cs, o);
     out[0] = o[0]; out[3] = o[1]; out[1] = o[2]; out[2] = o[3];
   }
 }
 
 // Record of one cell: P[k * ncell + i], k = f[0..3] then g[v][d] at 4 + 3 v + d.
-template <typename R>
+template <typename R, bool FACC>
 __global__ void __launch_bounds__(256)
     k_hydro_prim(const R *rho, const R *vx, const R *vy, const R *vz, R *P, int n, R dx, R dt, R cs) {
   const long long ncell = (long long)n * n * n;
@@ -130,7 +166,7 @@ __global__ void __launch_bounds__(256)
   if (i >= ncell) return;
   const int z = (int)(i % n), y = (int)((i / n) % n), x = (int)(i / ((long long)n * n));
   const R *const F[4] = {rho, vx, vy, vz};
-  const Prim<R> C = cell_prim(F, Idx3{n}, x, y, z, dx, dt, cs);
+  const Prim<R> C = cell_prim<R, FACC>(F, Idx3{n}, x, y, z, dx, dt, cs);
 #pragma unroll
   for (int k = 0; k < 4; ++k) P[k * ncell + i] = C.f[k];
 #pragma unroll
@@ -149,7 +185,7 @@ __device__ __forceinline__ void load_face_prim(const R *P, long long ncell, long
   for (int v = 0; v < 4; ++v) q.g[v][d] = P[(4 + 3 * v + d) * ncell + j];
 }
 
-template <typename R>
+template <typename R, bool FACC>
 __global__ void __launch_bounds__(256)
     k_hydro_update(R *rho, R *vx, R *vy, R *vz, const R *P, int n, R dx, R cs, R vol, R fac,
                    int clamp_rho) {
@@ -175,8 +211,8 @@ __global__ void __launch_bounds__(256)
     Prim<R> Pp, Pm;
     load_face_prim(P, ncell, I.at(x + ex, y + ey, z + ez), d, Pp);
     load_face_prim(P, ncell, I.at(x - ex, y - ey, z - ez), d, Pm);
-    face_flux(C, Pp, d, dx, cs, up[d]);
-    face_flux(Pm, C, d, dx, cs, dn[d]);
+    face_flux<R, FACC>(C, Pp, d, dx, cs, up[d]);
+    face_flux<R, FACC>(Pm, C, d, dx, cs, dn[d]);
   }
 #pragma unroll
   for (int v = 0; v < 4; ++v) {
@@ -188,13 +224,14 @@ __global__ void __launch_bounds__(256)
     }
     U[v] = u;
   }
-  // get_primitive (:179-185)
+  // get_primitive (:179-185; quantum-fluid-accretion.py:200-206 with eps)
   R r = U[0] / vol;
   if (clamp_rho) r = fmax((R)0, r);
   rho[i] = r;
-  vx[i] = U[1] / U[0];
-  vy[i] = U[2] / U[0];
-  vz[i] = U[3] / U[0];
+  const R den = FACC ? U[0] + (R)1e-30 : U[0];
+  vx[i] = U[1] / den;
+  vy[i] = U[2] / den;
+  vz[i] = U[3] / den;
 }
 
 // do_accretion (quantum-gas-bh.py:497-530; quantum-bh.py:306-339 with sigma)
@@ -470,31 +507,38 @@ int launch_cfl_dt(bool dbl, const void *vx, const void *vy, const void *vz, long
   return 0;
 }
 
-int launch_hydro(bool dbl, void *rho, void *vx, void *vy, void *vz, void *prim, int n, double dx,
-                 double dt, double cs, int clamp_rho, cudaStream_t st, int block) {
+template <bool FACC>
+static int hydro_impl(bool dbl, void *rho, void *vx, void *vy, void *vz, void *prim, int n,
+                      double dx, double dt, double cs, int clamp_rho, cudaStream_t st, int block) {
   const long long ncell = (long long)n * n * n;
   const int T = (block == 64 || block == 128 || block == 256) ? block : 256;
   const int B = (int)((ncell + T - 1) / T);
   const double vol = dx * dx * dx, fac = dt * dx * dx;
   if (dbl) {
-    k_hydro_prim<double><<<B, T, 0, st>>>((const double *)rho, (const double *)vx,
-                                          (const double *)vy, (const double *)vz, (double *)prim,
-                                          n, dx, dt, cs);
+    k_hydro_prim<double, FACC><<<B, T, 0, st>>>((const double *)rho, (const double *)vx,
+                                                (const double *)vy, (const double *)vz,
+                                                (double *)prim, n, dx, dt, cs);
     QJ_CK_LAUNCH();
-    k_hydro_update<double><<<B, T, 0, st>>>((double *)rho, (double *)vx, (double *)vy,
-                                            (double *)vz, (const double *)prim, n, dx, cs, vol,
-                                            fac, clamp_rho);
+    k_hydro_update<double, FACC><<<B, T, 0, st>>>((double *)rho, (double *)vx, (double *)vy,
+                                                  (double *)vz, (const double *)prim, n, dx, cs,
+                                                  vol, fac, clamp_rho);
   } else {
-    k_hydro_prim<float><<<B, T, 0, st>>>((const float *)rho, (const float *)vx, (const float *)vy,
-                                         (const float *)vz, (float *)prim, n, (float)dx,
-                                         (float)dt, (float)cs);
+    k_hydro_prim<float, FACC><<<B, T, 0, st>>>((const float *)rho, (const float *)vx,
+                                               (const float *)vy, (const float *)vz,
+                                               (float *)prim, n, (float)dx, (float)dt, (float)cs);
     QJ_CK_LAUNCH();
-    k_hydro_update<float><<<B, T, 0, st>>>((float *)rho, (float *)vx, (float *)vy, (float *)vz,
-                                           (const float *)prim, n, (float)dx, (float)cs,
-                                           (float)vol, (float)fac, clamp_rho);
+    k_hydro_update<float, FACC><<<B, T, 0, st>>>((float *)rho, (float *)vx, (float *)vy,
+                                                 (float *)vz, (const float *)prim, n, (float)dx,
+                                                 (float)cs, (float)vol, (float)fac, clamp_rho);
   }
   QJ_CK_LAUNCH();
   return 0;
+}
+
+int launch_hydro(bool dbl, void *rho, void *vx, void *vy, void *vz, void *prim, int n, double dx,
+                 double dt, double cs, int clamp_rho, cudaStream_t st, int block, bool facc) {
+  return facc ? hydro_impl<true>(dbl, rho, vx, vy, vz, prim, n, dx, dt, cs, clamp_rho, st, block)
+              : hydro_impl<false>(dbl, rho, vx, vy, vz, prim, n, dx, dt, cs, clamp_rho, st, block);
 }
 
 int launch_accrete(bool dbl, void *psi, const void *pos, const void *vel, void *m_bh, int n,

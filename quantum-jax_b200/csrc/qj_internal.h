@@ -139,6 +139,18 @@ int launch_amax3(bool dbl, const void *ax, const void *ay, const void *az, long 
 int launch_gas_kick(bool dbl, void *vx, void *vy, void *vz, const void *ax, const void *ay,
                     const void *az, double dt, long long ncell, cudaStream_t st);
 
+// quantum-fluid-accretion pieces (qj_plain.cu)
+int launch_kfilter(bool dbl, void *c, const KTabs &k, int kind, double p, long long ncell,
+                   cudaStream_t st);
+int launch_cic_point(bool dbl, void *grid, int n, const double x[3], double dx, double M,
+                     cudaStream_t st);
+int launch_cic_sample3(bool dbl, const void *f0, const void *f1, const void *f2, int n,
+                       const double x[3], double dx, double *out, cudaStream_t st);
+int launch_mean_dm_gas(bool dbl, const void *psi, const void *rho, long long ncell, double *part,
+                       int nb, double *out, cudaStream_t st);
+int launch_argmax(bool dbl, const void *f, long long ncell, double *pv, long long *pi, int nb,
+                  double *out, cudaStream_t st);
+
 int launch_adj_mu(bool dbl, const void *g, const void *psi, const void *V, double coef, void *mu,
                   long long ncell, cudaStream_t st);
 int launch_adj_update(bool dbl, void *g, const void *psi, const void *V, const void *W, double coef,
@@ -149,7 +161,8 @@ int launch_adj_update(bool dbl, void *g, const void *psi, const void *V, const v
 int fused_max_ctas_per_sm(int mode, int n, bool contig);
 
 int launch_hydro(bool dbl, void *rho, void *vx, void *vy, void *vz, void *prim, int n, double dx,
-                 double dt, double cs, int clamp_rho, cudaStream_t st, int block = 256);
+                 double dt, double cs, int clamp_rho, cudaStream_t st, int block = 256,
+                 bool facc = false);
 int launch_bondi_ambient(bool dbl, void *rho, const void *vx, const void *vy, const void *vz,
                          int n, double dx, double L, const double x_bh[3], const double v_bh[3],
                          double M, double cs, double G, double dt, double r_acc_mult, double lam,

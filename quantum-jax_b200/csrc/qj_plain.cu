@@ -316,3 +316,215 @@ int launch_gas_kick(bool dbl, void *vx, void *vy, void *vz, const void *ax, cons
 }
 
 }  // namespace qj
+
+// ---------------------------------------------------------------------------
+// Pieces of the quantum-fluid-accretion step (quantum-fluid-accretion.py)
+// ---------------------------------------------------------------------------
+namespace qj {
+namespace {
+
+// c *= exp(-(k^2 / (p + 1e-30))^4)   (kind 0: the low-pass LP, p = k_cut^2, :143-145)
+// c *= exp((-0.5 p) k^2)             (kind 1: Gaussian smoothing, p = r^2, :731-733, 849)
+template <typename R>
+__global__ void k_kfilter(cplx<R> *c, KT<R> k, int kind, R p, long long n) {
+  GRID_LOOP(i, n) {
+    R kx, ky, kz;
+    cell_k(k, i, kx, ky, kz);
+    const R k2 = kx * kx + ky * ky + kz * kz;
+    const R f = kind == 0 ? exp(-pow(k2 / (p + (R)1e-30), (R)4)) : exp(((R)-0.5 * p) * k2);
+    c[i] = cplx<R>{c[i].x * f, c[i].y * f};
+  }
+}
+
+// CIC cells and weights of a point, the corner order of bh_cic_density (:388-417)
+template <typename R>
+__device__ void point_cic(const double *x, int n, double dx, long long cells[8], R w[8]) {
+  double f[3];
+  long long i0[3];
+  for (int d = 0; d < 3; ++d) {
+    const double xi = x[d] / dx - 0.5;
+    const double fl = floor(xi);
+    i0[d] = (long long)fl;
+    f[d] = xi - fl;
+  }
+  const int off[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1},
+                         {1, 1, 0}, {1, 0, 1}, {0, 1, 1}, {1, 1, 1}};
+  for (int c = 0; c < 8; ++c) {
+    long long id[3];
+    for (int d = 0; d < 3; ++d) id[d] = (((i0[d] + off[c][d]) % n) + n) % n;
+    cells[c] = (id[0] * n + id[1]) * n + id[2];
+    const double a = off[c][0] ? f[0] : 1.0 - f[0];
+    const double b = off[c][1] ? f[1] : 1.0 - f[1];
+    const double e = off[c][2] ? f[2] : 1.0 - f[2];
+    w[c] = (R)(a * b * e);
+  }
+}
+
+// grid[cell] += w M / dx^3 in corner order (bh_cic_density), one thread
+template <typename R>
+__global__ void k_cic_point(R *grid, int n, double x0, double x1, double x2, double dx, double M) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const double x[3] = {x0, x1, x2};
+  long long cells[8];
+  R w[8];
+  point_cic<R>(x, n, dx, cells, w);
+  for (int c = 0; c < 8; ++c) grid[cells[c]] = grid[cells[c]] + w[c] * (R)(M / (dx * dx * dx));
+}
+
+// sum_c w_c f[cell_c] for three fields (_sample_cic, :419-437), one thread
+template <typename R>
+__global__ void k_cic_sample3(const R *f0, const R *f1, const R *f2, int n, double x0, double x1,
+                              double x2, double dx, double *out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const double x[3] = {x0, x1, x2};
+  long long cells[8];
+  R w[8];
+  point_cic<R>(x, n, dx, cells, w);
+  const R *f[3] = {f0, f1, f2};
+  for (int d = 0; d < 3; ++d) {
+    double s = 0.0;
+    for (int c = 0; c < 8; ++c) s += (double)(w[c] * f[d][cells[c]]);
+    out[d] = s;
+  }
+}
+
+// per-block float64 sums of |psi|^2 and rho
+template <typename R>
+__global__ void k_sum_dm_gas(const cplx<R> *psi, const R *rho, long long n, double *part) {
+  __shared__ double red[2][256];
+  double a = 0.0, b = 0.0;
+  GRID_LOOP(i, n) {
+    const double m = hypot((double)psi[i].x, (double)psi[i].y);
+    a += m * m;
+    b += (double)rho[i];
+  }
+  red[0][threadIdx.x] = a;
+  red[1][threadIdx.x] = b;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s) {
+      red[0][threadIdx.x] += red[0][threadIdx.x + s];
+      red[1][threadIdx.x] += red[1][threadIdx.x + s];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    part[2 * blockIdx.x] = red[0][0];
+    part[2 * blockIdx.x + 1] = red[1][0];
+  }
+}
+__global__ void k_mean_final(const double *part, int nb, long long n, double *out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double a = 0.0, b = 0.0;
+  for (int i = 0; i < nb; ++i) {
+    a += part[2 * i];
+    b += part[2 * i + 1];
+  }
+  out[0] = a / (double)n;
+  out[1] = b / (double)n;
+}
+
+// first index of the maximum (jnp.argmax), per block then final
+template <typename R>
+__global__ void k_argmax_part(const R *f, long long n, double *pv, long long *pi) {
+  __shared__ double sv[256];
+  __shared__ long long si[256];
+  double bv = -INFINITY;
+  long long bi = n;
+  GRID_LOOP(i, n) {
+    const double v = (double)f[i];
+    if (v > bv || (v == bv && i < bi)) {
+      bv = v;
+      bi = i;
+    }
+  }
+  sv[threadIdx.x] = bv;
+  si[threadIdx.x] = bi;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s) {
+      const double v = sv[threadIdx.x + s];
+      const long long j = si[threadIdx.x + s];
+      if (v > sv[threadIdx.x] || (v == sv[threadIdx.x] && j < si[threadIdx.x])) {
+        sv[threadIdx.x] = v;
+        si[threadIdx.x] = j;
+      }
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    pv[blockIdx.x] = sv[0];
+    pi[blockIdx.x] = si[0];
+  }
+}
+__global__ void k_argmax_final(const double *pv, const long long *pi, int nb, double *out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double bv = -INFINITY;
+  long long bi = -1;
+  for (int b = 0; b < nb; ++b)
+    if (pv[b] > bv || (pv[b] == bv && pi[b] < bi)) {
+      bv = pv[b];
+      bi = pi[b];
+    }
+  out[0] = (double)bi;
+}
+
+}  // namespace
+
+int launch_kfilter(bool dbl, void *c, const KTabs &k, int kind, double p, long long ncell,
+                   cudaStream_t st) {
+  if (dbl)
+    k_kfilter<double><<<grid_blocks(ncell), 256, 0, st>>>((double2 *)c, cast_k<double>(k), kind, p, ncell);
+  else
+    k_kfilter<float><<<grid_blocks(ncell), 256, 0, st>>>((float2 *)c, cast_k<float>(k), kind, (float)p, ncell);
+  QJ_CK_LAUNCH();
+  return 0;
+}
+
+int launch_cic_point(bool dbl, void *grid, int n, const double x[3], double dx, double M,
+                     cudaStream_t st) {
+  if (dbl)
+    k_cic_point<double><<<1, 32, 0, st>>>((double *)grid, n, x[0], x[1], x[2], dx, M);
+  else
+    k_cic_point<float><<<1, 32, 0, st>>>((float *)grid, n, x[0], x[1], x[2], dx, M);
+  QJ_CK_LAUNCH();
+  return 0;
+}
+
+int launch_cic_sample3(bool dbl, const void *f0, const void *f1, const void *f2, int n,
+                       const double x[3], double dx, double *out, cudaStream_t st) {
+  if (dbl)
+    k_cic_sample3<double><<<1, 32, 0, st>>>((const double *)f0, (const double *)f1,
+                                            (const double *)f2, n, x[0], x[1], x[2], dx, out);
+  else
+    k_cic_sample3<float><<<1, 32, 0, st>>>((const float *)f0, (const float *)f1,
+                                           (const float *)f2, n, x[0], x[1], x[2], dx, out);
+  QJ_CK_LAUNCH();
+  return 0;
+}
+
+int launch_mean_dm_gas(bool dbl, const void *psi, const void *rho, long long ncell, double *part,
+                       int nb, double *out, cudaStream_t st) {
+  if (dbl)
+    k_sum_dm_gas<double><<<nb, 256, 0, st>>>((const double2 *)psi, (const double *)rho, ncell, part);
+  else
+    k_sum_dm_gas<float><<<nb, 256, 0, st>>>((const float2 *)psi, (const float *)rho, ncell, part);
+  QJ_CK_LAUNCH();
+  k_mean_final<<<1, 32, 0, st>>>(part, nb, ncell, out);
+  QJ_CK_LAUNCH();
+  return 0;
+}
+
+int launch_argmax(bool dbl, const void *f, long long ncell, double *pv, long long *pi, int nb,
+                  double *out, cudaStream_t st) {
+  if (dbl)
+    k_argmax_part<double><<<nb, 256, 0, st>>>((const double *)f, ncell, pv, pi);
+  else
+    k_argmax_part<float><<<nb, 256, 0, st>>>((const float *)f, ncell, pv, pi);
+  QJ_CK_LAUNCH();
+  k_argmax_final<<<1, 32, 0, st>>>(pv, pi, nb, out);
+  QJ_CK_LAUNCH();
+  return 0;
+}
+
+}  // namespace qj

@@ -72,6 +72,9 @@ SIGNATURES = {
     "qj_plan_workspace_bytes": (c_int64, [c_void_p]),
     "qj_plan_status": (c_int, [c_void_p]),
     "qj_plan_get_tuning": (c_int, [c_void_p, c_void_p, c_int]),
+    "qj_fluid_accretion_step": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                        c_void_p, c_void_p, c_void_p, c_double, c_int, c_void_p,
+                                        c_void_p]),
     "qj_bondi_ambient": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                  c_void_p, c_double, c_double, c_double, c_double, c_double,
                                  c_double, c_double, c_void_p, c_void_p]),
@@ -84,6 +87,26 @@ SIGNATURES = {
     "qj_profile_enable": (c_int, [c_int]),
     "qj_profile_read": (c_int, [ctypes.POINTER(c_double), ctypes.POINTER(c_int64), c_int]),
 }
+
+
+class QjFaccState(ctypes.Structure):
+    _fields_ = [("t", c_double), ("M_acc", c_double), ("x_bh", c_double * 3),
+                ("v_bh", c_double * 3), ("placed", c_double)]
+
+
+class QjFaccParams(ctypes.Structure):
+    _fields_ = [("cs", c_double), ("hydro_cfl", c_double), ("bh_on", c_int), ("bh_grav", c_int),
+                ("bh_move", c_int), ("bh_accretion", c_int), ("bh_init_m", c_double),
+                ("bh_inject_t", c_double), ("ramp_on", c_int), ("ramp_center", c_double),
+                ("ramp_w", c_double), ("r_acc_mult", c_double), ("lam", c_double),
+                ("fmax", c_double), ("ann_lo", c_double), ("ann_hi", c_double),
+                ("k_cut_frac", c_double), ("inject_smooth_on", c_int),
+                ("inject_smooth_kpc", c_double), ("rho_gas", c_double)]
+
+
+class QjFaccDiag(ctypes.Structure):
+    _fields_ = [(k, c_double) for k in ("dMdt", "rho_inf", "r_B", "dMdt_real", "cap_ratio",
+                                        "r_acc_eff", "M_bh_eff_out", "dt_eff")]
 
 
 class QjError(RuntimeError):

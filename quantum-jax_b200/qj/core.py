@@ -290,6 +290,32 @@ class Plan:
             _stream()))
         return tuple(float(x) for x in out.cpu())
 
+    def fluid_accretion_step(self, psi, rho, vx, vy, vz, state: dict, params: dict, dt,
+                             nsteps=1):
+        """nsteps x compute_step of quantum-fluid-accretion.py (:695-870) on a
+        PLAIN_F64 plan, fields in place.  state: t, M_acc, x_bh (3), v_bh (3),
+        placed -- updated; params: the script's toggles and constants (fields
+        of QjFaccParams; booleans as 0/1).  Returns the last step's
+        diagnostics (dMdt, rho_inf, r_B, dMdt_real, cap_ratio, r_acc_eff,
+        M_bh_eff_out, dt_eff)."""
+        self._field(psi, "psi", complex_=True)
+        for f, name in ((rho, "rho"), (vx, "vx"), (vy, "vy"), (vz, "vz")):
+            self._field(f, name)
+        st = _lib.QjFaccState(float(state["t"]), float(state["M_acc"]),
+                              (ctypes.c_double * 3)(*[float(x) for x in state["x_bh"]]),
+                              (ctypes.c_double * 3)(*[float(x) for x in state["v_bh"]]),
+                              float(state["placed"]))
+        pr = _lib.QjFaccParams()
+        for name, typ in _lib.QjFaccParams._fields_:
+            setattr(pr, name, typ(params[name]).value if name in params else 0)
+        dg = _lib.QjFaccDiag()
+        check(lib().qj_fluid_accretion_step(self._h, _ptr(psi), _ptr(rho), _ptr(vx), _ptr(vy),
+                                            _ptr(vz), ctypes.byref(st), ctypes.byref(pr),
+                                            float(dt), int(nsteps), ctypes.byref(dg), _stream()))
+        state.update(t=st.t, M_acc=st.M_acc, x_bh=list(st.x_bh), v_bh=list(st.v_bh),
+                     placed=st.placed)
+        return {name: getattr(dg, name) for name, _ in _lib.QjFaccDiag._fields_}
+
     def hydro_cfl_dt(self, vx, vy, vz, cs, cfl, dt):
         """min(dt, cfl dx / max(cs + |v|)), quantum-fluid-accretion.py:697-701."""
         for c, name in ((vx, "vx"), (vy, "vy"), (vz, "vz")):
