@@ -298,14 +298,9 @@ def main():
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    dist = None
-    if world > 1:
-        import datetime
+    from qj import dist as qdist
 
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=dev)
+    dist = qdist.init("nccl", device=dev)
 
     def barrier():
         if dist is not None:
@@ -313,11 +308,7 @@ def main():
         torch.cuda.synchronize()
 
     def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return qdist.max_over_ranks(x, dist, dev)
 
     n, n_s = a.n, a.stars
     psi0, pos0, vel0, g, p, dt = make_ic(n, n_s)
@@ -517,14 +508,21 @@ def main():
     # ---------------- ensemble: 16x64^3 + 8x96^3 + 8x128^3, 256 stars each -----
     ensemble = None
     if not a.no_ensemble:
-        groups = [(64, 16), (96, 8), (128, 8)]
-        ens_steps, seed = a.ens_steps, 100
+        all_groups = [(64, 16), (96, 8), (128, 8)]
+        # the 32 boxes (seeds 100..131) split across ranks by cost; one batched
+        # plan per size class a rank holds (no collective between ranks)
+        boxes = [(n_e, 100 + i) for i, n_e in enumerate(
+            [n_e for n_e, nb in all_groups for _ in range(nb)])]
+        mine = qdist.partition_boxes([qdist.box_cost(b[0] ** 3) for b in boxes], world)[rank]
+        groups = []
+        for n_e, _ in all_groups:
+            seeds = [boxes[i][1] for i in mine if boxes[i][0] == n_e]
+            if seeds:
+                groups.append((n_e, len(seeds), seeds))
+        ens_steps = a.ens_steps
         plans, state, singles = [], [], []
-        for n_e, nb in groups:
-            ics = []
-            for b in range(nb):
-                ics.append(O.stars_ic(n_e, 256, seed=seed))
-                seed += 1
+        for n_e, nb, seeds in groups:
+            ics = [O.stars_ic(n_e, 256, seed=sd) for sd in seeds]
             g_e, p_e = ics[0][3], ics[0][4]
             dt_e = O.default_dt(g_e, p_e)
             pl = qj.Plan(qj.Grid(n_e, n_e, n_e),
@@ -564,16 +562,18 @@ def main():
         ens_run(ens_steps)
         e1.record(stream)
         barrier()
-        ens_ms = e0.elapsed_time(e1)
-        cells = sum(n_e**3 * nb for n_e, nb in groups)
+        ens_ms = max_over_ranks(e0.elapsed_time(e1))
+        cells = sum(n_e**3 * nb for n_e, nb in all_groups)  # all ranks' boxes
         # one by one: each box alone through a single-box plan, same steps
-        views = []
-        for gi, (n_e, nb) in enumerate(groups):
+        views, first = [], []
+        for gi, (n_e, nb, _) in enumerate(groups):
+            first.append(len(views))
             for b in range(nb):
                 s = init[gi]
                 views.append((singles[gi], s[0][b].clone(), s[1][b].clone(), s[2][b].clone(),
                               s[3][b].clone(), s[4], s[5]))
-        for v in views[:1] + views[16:17] + views[24:25]:  # warm-up each size
+        for i in first:  # warm-up each size
+            v = views[i]
             v[0].kdk_step(v[1], v[2], v[3], v[4], v[5], 2, v[6])
         barrier()
         e0.record(stream)
@@ -581,10 +581,10 @@ def main():
             v[0].kdk_step(v[1], v[2], v[3], v[4], v[5], ens_steps, v[6])
         e1.record(stream)
         barrier()
-        seq_ms = e0.elapsed_time(e1)
+        seq_ms = max_over_ranks(e0.elapsed_time(e1))
         # per-box error of the ensemble against the float64 path (first box of each size)
         errs = {}
-        for gi, (n_e, nb) in enumerate(groups):
+        for gi, (n_e, nb, _) in enumerate(groups):
             pl64 = qj.Plan(qj.Grid(n_e, n_e, n_e),
                            qj.Phys(m_per_hbar=1.0, G=plans[gi].phys.G, rho_bar=plans[gi].phys.rho_bar),
                            qj.PLAIN_F64, 256)
@@ -600,7 +600,9 @@ def main():
                                      torch.linalg.vector_norm(ps64))
             pl64.close()
         ensemble = {"boxes": "16x64^3 + 8x96^3 + 8x128^3, 256 stars each",
-                    "tuning": {f"{n_e}^3": pl.tuning for (n_e, _), pl in zip(groups, plans)},
+                    "sharding": f"{world} rank(s), greedy by C log C; this rank: "
+                                + ", ".join(f"{nb}x{n_e}^3" for n_e, nb, _ in groups),
+                    "tuning": {f"{n_e}^3": pl.tuning for (n_e, _, _), pl in zip(groups, plans)},
                     "cells": cells, "steps": ens_steps, "graph_chunk": a.ens_chunk,
                     "ensemble_cell_steps_per_s": cells * ens_steps / (ens_ms * 1e-3),
                     "one_by_one_cell_steps_per_s": cells * ens_steps / (seq_ms * 1e-3),
