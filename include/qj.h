@@ -213,7 +213,8 @@ int64_t qj_plan_workspace_bytes(const qj_plan *plan);
  * rho (the plan's real type) is updated in place.  vx/vy/vz (may be NULL)
  * add the BHL term with the black-hole velocity v_bh.  fmax <= 0: no cap
  * beyond the sink's mass.  out (device, 7 doubles) = dMdt_target, rho_inf,
- * rB, dM_cap, r_acc, M_avail, dM_uncl. */
+ * rB, dM_cap, r_acc, M_avail, dM_uncl.  The shell must fit the grid
+ * (2 ceil(r_hi / dx) + 3 <= n), else QJ_ERR_ARG. */
 int qj_bondi_ambient(qj_plan *plan, void *rho, const void *vx, const void *vy, const void *vz,
                      const double *x_bh, const double *v_bh, double M_bh, double dt,
                      double r_acc_mult, double lam, double fmax, double ann_lo, double ann_hi,

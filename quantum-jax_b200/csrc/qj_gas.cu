@@ -477,7 +477,12 @@ int launch_bondi_ambient(bool dbl, void *rho, const void *vx, const void *vy, co
   const double r_acc = r_acc_mult * dx;
   const double r_lo = std::max(ann_lo * r_acc, r_acc + 0.25 * dx);
   const double r_hi = std::max(ann_hi * r_acc, r_lo + 0.5 * dx);
-  const int K = std::min((int)std::ceil(r_hi / dx) + 1, (n - 1) / 2);
+  const int K = (int)std::ceil(r_hi / dx) + 1;
+  if (2 * K + 1 > n) {
+    set_error("ambient Bondi sink: sampling shell radius %g cells is too large for a %d^3 grid",
+              r_hi / dx, n);
+    return QJ_ERR_ARG;
+  }
   if (dbl)
     k_bondi_ambient<double><<<1, 256, 0, st>>>(
         (double *)rho, (const double *)vx, (const double *)vy, (const double *)vz, n, dx, L,
