@@ -173,6 +173,9 @@ static int run_fused(const FusedArgs &a, cudaStream_t st) {
     }
   FusedArgs b = a;
   b.ntiles = grid_of<N, CONTIG>(a);
+  // y passes walk backwards: each follows (and precedes) a pass that walks
+  // forwards over the same slow index x
+  b.rev = (!CONTIG && a.axis == 1) ? 1 : 0;
   TileMaps maps;
   std::memset(&maps, 0, sizeof(maps));
   if (!CONTIG && stream_count<MODE>() > 0) {

@@ -88,6 +88,9 @@ struct FusedArgs {
   float gas_dt;
   // tiles of this pass per box (the persistent CTAs stride over them)
   int ntiles;
+  // walk the tiles from the last: a pass then first reads what the previous
+  // pass wrote last, which is still in L2
+  int rev;
   // host side only: the plan's launch tuning (QJ_TUNE_* of include/qj.h)
   const int *tune;
   // set to nonzero when a pass gave up waiting for a tile copy
@@ -587,13 +590,15 @@ __device__ __forceinline__ bool take_tile(float2 (&v)[E], float2 &c0, const Fuse
     if (threadIdx.x == 0 && a.err) atomicOr(a.err, 1u);
     return false;
   }
+  // tile here is the loop index; the copy goes to its logical tile
   int nf = f + 1, nt = tile;
   if (nf == NF) {
     nf = 0;
     nt = tile + gridDim.x;
   }
   f = nf;
-  if (nt < a.ntiles && threadIdx.x < 32) issue_tile<N, CONTIG, MODE>(a, maps, nf, nt, land, bar);
+  if (nt < a.ntiles && threadIdx.x < 32)
+    issue_tile<N, CONTIG, MODE>(a, maps, nf, a.rev ? a.ntiles - 1 - nt : nt, land, bar);
   return true;
 }
 
@@ -647,14 +652,16 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CO
   int fld = 0;
   if constexpr (LAY::LANDS)
     if ((int)blockIdx.x < a.ntiles && tid < 32)
-      issue_tile<N, CONTIG, MODE>(a, maps, 0, blockIdx.x, land, &lbar);
+      issue_tile<N, CONTIG, MODE>(a, maps, 0, a.rev ? a.ntiles - 1 - (int)blockIdx.x : (int)blockIdx.x,
+                                  land, &lbar);
 
-  for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
+  for (int it = blockIdx.x; it < a.ntiles; it += gridDim.x) {
+    const int tile = a.rev ? a.ntiles - 1 - it : it;  // logical tile
     const PencilPos pp = pencil_pos<CONTIG>(a, tile, p, TP);
     const long long base = pp.base, st = a.stride;
     float2 c0;
 #define QJ_TAKE(v) \
-  if (!take_tile<N, CONTIG, MODE, E>(v, c0, a, maps, land, &lbar, parity, fld, tile, p, t)) return
+  if (!take_tile<N, CONTIG, MODE, E>(v, c0, a, maps, land, &lbar, parity, fld, it, p, t)) return
 
     if constexpr (MODE == M_DENSITY) {
       float2 v[E];
