@@ -39,6 +39,33 @@ template <int DIR, typename C> __device__ __forceinline__ C cmul_i(C a) {
   return DIR > 0 ? C{-a.y, a.x} : C{a.y, -a.x};
 }
 
+// a + b and a - b as one packed instruction for float2 (sm_100's
+// add/sub.rn.f32x2: two IEEE round-to-nearest operations, the same results as
+// the scalar pair); other types fall back to the scalar pair.  Used where both
+// operands are already whole register pairs: an operand that still needs a
+// swap or a sign (a +-i rotation) goes through the scalar cadd / csub, whose
+// negation folds into the add.
+template <typename C> __device__ __forceinline__ C padd(C a, C b) { return cadd(a, b); }
+template <typename C> __device__ __forceinline__ C psub(C a, C b) { return csub(a, b); }
+__device__ __forceinline__ float2 padd(float2 a, float2 b) {
+  float2 r;
+  asm("{\n\t.reg .b64 qa, qb, qr;\n\t"
+      "mov.b64 qa, {%2, %3};\n\tmov.b64 qb, {%4, %5};\n\t"
+      "add.rn.f32x2 qr, qa, qb;\n\tmov.b64 {%0, %1}, qr;\n\t}"
+      : "=f"(r.x), "=f"(r.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return r;
+}
+__device__ __forceinline__ float2 psub(float2 a, float2 b) {
+  float2 r;
+  asm("{\n\t.reg .b64 qa, qb, qr;\n\t"
+      "mov.b64 qa, {%2, %3};\n\tmov.b64 qb, {%4, %5};\n\t"
+      "sub.rn.f32x2 qr, qa, qb;\n\tmov.b64 {%0, %1}, qr;\n\t}"
+      : "=f"(r.x), "=f"(r.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return r;
+}
+
 // float ops with explicit round-to-nearest and no contraction, used where the
 // reference's float32 operation order is reproduced exactly (CIC weights).
 __device__ __forceinline__ float fmul_rn(float a, float b) { return __fmul_rn(a, b); }

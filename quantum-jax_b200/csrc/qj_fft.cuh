@@ -69,8 +69,13 @@ template <int R, int DIR, typename C> struct Dft {
 #pragma unroll
     for (int k = 0; k < R / 2; ++k) {
       C t = twc<R, DIR>(o[k], k);
-      a[k] = cadd(e[k], t);
-      a[k + R / 2] = csub(e[k], t);
+      if ((k * (16 / R)) % 16 == 4) {  // t = +-i o: scalar, the sign folds into the adds
+        a[k] = cadd(e[k], t);
+        a[k + R / 2] = csub(e[k], t);
+      } else {
+        a[k] = padd(e[k], t);
+        a[k + R / 2] = psub(e[k], t);
+      }
     }
   }
 };
@@ -80,17 +85,17 @@ template <int DIR, typename C> struct Dft<1, DIR, C> {
 template <int DIR, typename C> struct Dft<2, DIR, C> {
   __device__ __forceinline__ static void run(C *a) {
     C t = a[1];
-    a[1] = csub(a[0], t);
-    a[0] = cadd(a[0], t);
+    a[1] = psub(a[0], t);
+    a[0] = padd(a[0], t);
   }
 };
 template <int DIR, typename C> struct Dft<4, DIR, C> {
   __device__ __forceinline__ static void run(C *a) {
-    C s02 = cadd(a[0], a[2]), d02 = csub(a[0], a[2]);
-    C s13 = cadd(a[1], a[3]), d13 = csub(a[1], a[3]);
+    C s02 = padd(a[0], a[2]), d02 = psub(a[0], a[2]);
+    C s13 = padd(a[1], a[3]), d13 = psub(a[1], a[3]);
     C r = cmul_i<DIR>(d13);
-    a[0] = cadd(s02, s13);
-    a[2] = csub(s02, s13);
+    a[0] = padd(s02, s13);
+    a[2] = psub(s02, s13);
     a[1] = cadd(d02, r);
     a[3] = csub(d02, r);
   }
