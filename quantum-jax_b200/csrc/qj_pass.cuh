@@ -307,11 +307,12 @@ __device__ __forceinline__ void for_star_corners(const FusedArgs &a, StarRanges 
 // the thread's float64 partial sum of rho.
 template <int N, int E>
 __device__ __forceinline__ double build_density(float2 (&v)[E], const FusedArgs &a,
-                                                const PencilPos &pp, int t, int P) {
+                                                const PencilPos &pp, const StarRanges &sr, int t,
+                                                int P) {
 #pragma unroll
   for (int e = 0; e < E; ++e) v[e] = float2{v[e].x * v[e].x + v[e].y * v[e].y, 0.0f};
   if (a.has_stars) {
-    for_star_corners<N, true>(a, star_ranges(a, pp), t, P,
+    for_star_corners<N, true>(a, sr, t, P,
                               [&](unsigned, int, int m, float wx, float wy, float wz, float fac) {
                                 const float val = fmul_rn(fmul_rn(fmul_rn(wx, wy), wz), fac);
                                 const int e = m / P;
@@ -659,6 +660,12 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CO
     const int tile = a.rev ? a.ntiles - 1 - it : it;  // logical tile
     const PencilPos pp = pencil_pos<CONTIG>(a, tile, p, TP);
     const long long base = pp.base, st = a.stride;
+    // the density passes load the pencil's star buckets before the transforms
+    // they would otherwise wait behind (in the kick the extra live registers
+    // cost more than the latency they hide)
+    StarRanges sr;
+    if constexpr (MODE == M_DENSITY || MODE == M_DRIFT_DENSITY)
+      if (a.has_stars) sr = star_ranges(a, pp);
     float2 c0;
 #define QJ_TAKE(v) \
   if (!take_tile<N, CONTIG, MODE, E>(v, c0, a, maps, land, &lbar, parity, fld, it, p, t)) return
@@ -666,7 +673,7 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CO
     if constexpr (MODE == M_DENSITY) {
       float2 v[E];
       QJ_TAKE(v);
-      double s = build_density<N, E>(v, a, pp, t, P);
+      double s = build_density<N, E>(v, a, pp, sr, t, P);
       s = block_sum<THREADS>(s, red);
       if (tid == 0) a.part[tile] = s;
       fft_pencil<N, -1, true>(v, t, smv, tw);
@@ -859,7 +866,7 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CO
       drift_pencil<N, E, P, THREADS>(v, c0, a.prop, t, smv, tw, save);
       store_pencil<E>(v, a.psi, base, st, t, P);
       if constexpr (MODE == M_DRIFT_DENSITY) {
-        double s = build_density<N, E>(v, a, pp, t, P);
+        double s = build_density<N, E>(v, a, pp, sr, t, P);
         s = block_sum<THREADS>(s, red);
         if (tid == 0) a.part[tile] = s;
         fft_pencil<N, -1, true>(v, t, smv, tw);
