@@ -239,8 +239,8 @@ __device__ __forceinline__ StarRanges star_ranges(const FusedArgs &a, const Penc
   r.u = q == 1 ? 0 : (q == 2 ? 0 : 1);
   r.v = q == 2 ? 1 : 2;
   const int nu = r.u == 0 ? a.nx : a.ny, nv = r.v == 1 ? a.ny : a.nz;
-  r.cu = pp.c[r.u];
-  r.cv = pp.c[r.v];
+  r.cu = r.u == 0 ? pp.c[0] : pp.c[1];
+  r.cv = r.v == 1 ? pp.c[1] : pp.c[2];
   const int cum = r.cu == 0 ? nu - 1 : r.cu - 1, cvm = r.cv == 0 ? nv - 1 : r.cv - 1;
   const int b[4] = {r.cu * nv + r.cv, cum * nv + r.cv, r.cu * nv + cvm, cum * nv + cvm};
 #pragma unroll
@@ -642,8 +642,8 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CO
     for (int i = tid; i < N; i += THREADS) tab2[i] = a.prop[i];
   } else if constexpr (MODE == M_POISSON) {
     for (int i = tid; i < N; i += THREADS) {
-      tabk[i] = a.k[a.axis][i];
-      tabk[N + i] = a.kt[a.axis][i];
+      tabk[i] = (a.axis == 0 ? a.k[0] : (a.axis == 1 ? a.k[1] : a.k[2]))[i];
+      tabk[N + i] = (a.axis == 0 ? a.kt[0] : (a.axis == 1 ? a.kt[1] : a.kt[2]))[i];
     }
   }
   if (tid == 0) mbar_init(&lbar, 1);
@@ -696,10 +696,13 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CO
       fft_pencil<N, -1, true>(v, t, smv, tw);
       const int ax = a.axis;  // r: 0 or 2
       const int aq = 2 - ax;  // the other non-y axis
-      const float kq2 = a.k[aq][pp.c[aq]] * a.k[aq][pp.c[aq]];
+      // (selects, not runtime indices: small arrays indexed at run time live in local memory)
+      const int cq = aq == 0 ? pp.c[0] : pp.c[2];
+      const float kqv = aq == 0 ? a.k[0][cq] : a.k[2][cq];
+      const float kq2 = kqv * kqv;
       const float ky = a.k[1][pp.c[1]];
       const float kperp2 = kq2 + ky * ky;
-      const float ktq = a.kt[aq][pp.c[aq]], kty = a.kt[1][pp.c[1]];
+      const float ktq = aq == 0 ? a.kt[0][cq] : a.kt[2][cq], kty = a.kt[1][pp.c[1]];
       const float g0 = (float)(-a.fourpiG * a.inv_ncell);
 #pragma unroll
       for (int e = 0; e < E; ++e) {
@@ -717,7 +720,7 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CO
             vh = float2{(float)v0, 0.0f};
           }
         } else {
-          const float g = g0 / k2;
+          const float g = __fdividef(g0, k2);
           vh = float2{v[e].x * g, v[e].y * g};
         }
         const float f1 = 1.0f + tabk[N + i];
@@ -764,7 +767,7 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CO
                                      });
         }
         if (a.gv[0]) {
-          float *gq = a.gv[aq], *gy = a.gv[1];
+          float *gq = aq == 0 ? a.gv[0] : a.gv[2], *gy = a.gv[1];
 #pragma unroll
           for (int e = 0; e < E; ++e) {
             gq[gb + e * gs] = gq[gb + e * gs] + v2[e].x * a.gas_dt;
@@ -792,7 +795,7 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CO
                                      });
         }
         if (a.gv[0]) {  // gas half kick, quantum-gas-bh.py:255-266
-          float *g = a.gv[aq == 0 ? 2 : 0];
+          float *g = aq == 0 ? a.gv[2] : a.gv[0];
 #pragma unroll
           for (int e = 0; e < E; ++e) g[gb + e * gs] = g[gb + e * gs] + v1[e].y * a.gas_dt;
         }
