@@ -554,7 +554,7 @@ int adjoint_sweep(qj_plan *P, const void *ckpt, void *g, int nsteps, int K, doub
   }
   const int nseg = (nsteps + K - 1) / K;
   const double half = P->ph.m_per_hbar * dt / 2.0;
-  void *mu = P->ax, *W = P->ay;
+  void *mu = P->ax;
   for (int seg = nseg - 1; seg >= 0; --seg) {
     const int m = std::min(K, nsteps - seg * K);
     const void *c0 = (const char *)ckpt + (size_t)seg * fb;
@@ -568,20 +568,29 @@ int adjoint_sweep(qj_plan *P, const void *ckpt, void *g, int nsteps, int K, doub
         QJ_TRY(plain_potential(P, pre, nullptr, nullptr, P->V, si, vext, st));
       else
         Vj = (const float *)P->adj_V + (size_t)j * P->ncell;
-      QJ_TRY(launch_adj_mu(P->dbl, g, pre, Vj, coef, mu, P->ncell, st));
-      // W = (L + b) mu: the Poisson operator without the rho_bar shift
-      QJ_TRY(launch_build_rho(P->dbl, nullptr, nullptr, nullptr, mu, 4.0 * M_PI * P->ph.G, 0.0,
-                              nullptr, P->c0, P->ncell, st));
+      // W = (L + b) mu: the Poisson operator without the rho_bar shift; mu
+      // itself is kept only for the self-interaction term
+      QJ_TRY(launch_adj_mu(P->dbl, g, pre, Vj, coef, si ? mu : nullptr, 4.0 * M_PI * P->ph.G, P->c0,
+                           P->ncell, st));
       QJ_TRY(fft3d(P, P->c0, -1, st));
       QJ_TRY(launch_poisson_div(P->dbl, P->c0, ktabs(P), P->ncell, st));
       QJ_TRY(fft3d(P, P->c0, +1, st));
-      QJ_TRY(launch_real_part(P->dbl, P->c0, 1.0, si ? mu : nullptr, P->ph.b_coeff, nullptr, W,
-                              P->ncell, st));
-      QJ_TRY(launch_adj_update(P->dbl, g, pre, Vj, W, coef, P->ncell, st));
-      if (j > 0) {  // adjoint of drift j - 1
-        QJ_TRY(fft3d(P, g, -1, st));
-        QJ_TRY(launch_drift_mul(P->dbl, g, ktabs(P), -dt, P->ph.m_per_hbar, P->ncell, st));
-        QJ_TRY(fft3d(P, g, +1, st));
+      QJ_TRY(launch_adj_update(P->dbl, g, pre, Vj, P->c0, si ? mu : nullptr, P->ph.b_coeff, coef,
+                               P->ncell, st));
+      if (j > 0) {  // adjoint of drift j - 1: the drift with -dt
+        if (P->dbl) {
+          QJ_TRY(fft3d(P, g, -1, st));
+          QJ_TRY(launch_drift_mul(P->dbl, g, ktabs(P), -dt, P->ph.m_per_hbar, P->ncell, st));
+          QJ_TRY(fft3d(P, g, +1, st));
+        } else {
+          // the separable drift as three fused forward-multiply-inverse passes
+          QJ_TRY(ensure_prop(P, -dt, st));
+          for (int ax = 0; ax < 3; ++ax) {
+            FusedArgs a = fused_args(P, ax);
+            a.psi = (float2 *)g;
+            QJ_TRY(launch_fused(M_DRIFT, P->n[ax], a, st));
+          }
+        }
       }
     }
   }

@@ -190,11 +190,12 @@ static int run_fused(const FusedArgs &a, cudaStream_t st) {
   return 0;
 }
 
-// Modes used along y (axis 1) are only instantiated strided; the others for
-// both the strided x pass and the contiguous z pass.
+// The y-only transforms are instantiated strided; the others for both the
+// strided x or y pass and the contiguous z pass (the plain drift runs along
+// every axis in the adjoint's reverse sweep).
 template <int MODE>
 static int dispatch_mode(int n, const FusedArgs &a, cudaStream_t st) {
-  constexpr bool ONLY_Y = (MODE == M_FFT_FWD || MODE == M_IFFT2 || MODE == M_DRIFT);
+  constexpr bool ONLY_Y = (MODE == M_FFT_FWD || MODE == M_IFFT2);
   const bool contig = a.axis == 2;
   if (ONLY_Y && contig) {
     set_error("internal: pass mode %d requested along z", MODE);
@@ -255,7 +256,7 @@ static int launch_fused_impl(int mode, int n, const FusedArgs &a, cudaStream_t s
 template <int MODE> static int occupancy_of(int n, bool contig) {
   int per_sm = 0, sms = 0;
   cudaError_t e = cudaSuccess;
-  constexpr bool ONLY_Y = (MODE == M_FFT_FWD || MODE == M_IFFT2 || MODE == M_DRIFT);
+  constexpr bool ONLY_Y = (MODE == M_FFT_FWD || MODE == M_IFFT2);
   constexpr bool ONLY_Z = (MODE == M_DEPOSIT);
 #define QJ_OCC(NN)                                                                          \
   case NN:                                                                                  \

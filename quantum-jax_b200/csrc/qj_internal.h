@@ -151,10 +151,13 @@ int launch_mean_dm_gas(bool dbl, const void *psi, const void *rho, long long nce
 int launch_argmax(bool dbl, const void *f, long long ncell, double *pv, long long *pi, int nb,
                   double *out, cudaStream_t st);
 
+// adjoint kick: mu = coef Im(conj(g) psi') (stored when mu is non-null) and the
+// Poisson source fourpiG mu in cbuf; then g <- exp(+i coef V) g + 2 W psi with
+// W = Re(cbuf) (+ b mu when mu is non-null)
 int launch_adj_mu(bool dbl, const void *g, const void *psi, const void *V, double coef, void *mu,
-                  long long ncell, cudaStream_t st);
-int launch_adj_update(bool dbl, void *g, const void *psi, const void *V, const void *W, double coef,
-                      long long ncell, cudaStream_t st);
+                  double fourpiG, void *cbuf, long long ncell, cudaStream_t st);
+int launch_adj_update(bool dbl, void *g, const void *psi, const void *V, const void *cbuf,
+                      const void *mu, double b, double coef, long long ncell, cudaStream_t st);
 
 // ----- gas and black hole (qj_gas.cu) -----
 // CTAs of a fused pass that fit one SM (occupancy), 0 if unknown.

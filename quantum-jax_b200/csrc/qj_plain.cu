@@ -170,50 +170,58 @@ template <typename R> __device__ __forceinline__ void phase_sc(double th, R &s, 
 // mu = c Im(conj(g) psi'), psi' = exp(-i c V) psi
 template <typename R>
 __global__ void k_adj_mu(const cplx<R> *g, const cplx<R> *psi, const R *V, double coef, R *mu,
-                         long long n) {
+                         R fourpiG, cplx<R> *cbuf, long long n) {
   GRID_LOOP(i, n) {
     R s, c;
     phase_sc<R>(coef * (double)V[i], s, c);
     const cplx<R> z = psi[i];
     const cplx<R> zp = cplx<R>{z.x * c + z.y * s, z.y * c - z.x * s};
     const cplx<R> w = g[i];
-    mu[i] = (R)coef * (w.x * zp.y - w.y * zp.x);
+    const R m = (R)coef * (w.x * zp.y - w.y * zp.x);
+    if (mu) mu[i] = m;
+    cbuf[i] = cplx<R>{fourpiG * m, (R)0};  // the source of L mu
   }
 }
 
-// g <- exp(+i c V) g + 2 W psi
+// g <- exp(+i c V) g + 2 W psi with W = Re(cbuf) (+ b mu)
 template <typename R>
-__global__ void k_adj_update(cplx<R> *g, const cplx<R> *psi, const R *V, const R *W, double coef,
-                             long long n) {
+__global__ void k_adj_update(cplx<R> *g, const cplx<R> *psi, const R *V, const cplx<R> *cbuf,
+                             const R *mu, R b, double coef, long long n) {
   GRID_LOOP(i, n) {
     R s, c;
     phase_sc<R>(coef * (double)V[i], s, c);
+    R W = cbuf[i].x;
+    if (mu) W = W + b * mu[i];
     const cplx<R> w = g[i];
-    const R two_w = (R)2 * W[i];
+    const R two_w = (R)2 * W;
     g[i] = cplx<R>{w.x * c - w.y * s + two_w * psi[i].x, w.y * c + w.x * s + two_w * psi[i].y};
   }
 }
 
 int launch_adj_mu(bool dbl, const void *g, const void *psi, const void *V, double coef, void *mu,
-                  long long ncell, cudaStream_t st) {
+                  double fourpiG, void *cbuf, long long ncell, cudaStream_t st) {
   if (dbl)
-    k_adj_mu<double><<<grid_blocks(ncell), 256, 0, st>>>((const double2 *)g, (const double2 *)psi,
-                                                         (const double *)V, coef, (double *)mu, ncell);
+    k_adj_mu<double><<<grid_blocks(ncell), 256, 0, st>>>(
+        (const double2 *)g, (const double2 *)psi, (const double *)V, coef, (double *)mu, fourpiG,
+        (double2 *)cbuf, ncell);
   else
-    k_adj_mu<float><<<grid_blocks(ncell), 256, 0, st>>>((const float2 *)g, (const float2 *)psi,
-                                                        (const float *)V, coef, (float *)mu, ncell);
+    k_adj_mu<float><<<grid_blocks(ncell), 256, 0, st>>>(
+        (const float2 *)g, (const float2 *)psi, (const float *)V, coef, (float *)mu, (float)fourpiG,
+        (float2 *)cbuf, ncell);
   QJ_CK_LAUNCH();
   return 0;
 }
 
-int launch_adj_update(bool dbl, void *g, const void *psi, const void *V, const void *W, double coef,
-                      long long ncell, cudaStream_t st) {
+int launch_adj_update(bool dbl, void *g, const void *psi, const void *V, const void *cbuf,
+                      const void *mu, double b, double coef, long long ncell, cudaStream_t st) {
   if (dbl)
     k_adj_update<double><<<grid_blocks(ncell), 256, 0, st>>>(
-        (double2 *)g, (const double2 *)psi, (const double *)V, (const double *)W, coef, ncell);
+        (double2 *)g, (const double2 *)psi, (const double *)V, (const double2 *)cbuf,
+        (const double *)mu, b, coef, ncell);
   else
     k_adj_update<float><<<grid_blocks(ncell), 256, 0, st>>>(
-        (float2 *)g, (const float2 *)psi, (const float *)V, (const float *)W, coef, ncell);
+        (float2 *)g, (const float2 *)psi, (const float *)V, (const float2 *)cbuf, (const float *)mu,
+        (float)b, coef, ncell);
   QJ_CK_LAUNCH();
   return 0;
 }
