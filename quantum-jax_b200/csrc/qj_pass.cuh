@@ -171,13 +171,23 @@ __device__ __forceinline__ void load_pencil(C (&v)[E], const C *__restrict__ f, 
 #pragma unroll
   for (int e = 0; e < E; ++e) v[e] = __ldcs(&f[b + (unsigned)e * s]);  // read once: evict first
 }
-template <int E, typename C>
+// Store a thread's E elements t + P e of a pencil.  WIDE: one base pointer
+// plus a 64-bit constant multiple of the element step per store; otherwise a
+// 32-bit element index per store.  The two compile to different code; each
+// pass uses the one measured faster for it.
+template <int E, bool WIDE = true, typename C>
 __device__ __forceinline__ void store_pencil(const C (&v)[E], C *__restrict__ f, long long base,
                                              long long stride, int t, int P) {
   const unsigned b = (unsigned)base + (unsigned)t * (unsigned)stride;
   const unsigned s = (unsigned)P * (unsigned)stride;
+  if constexpr (WIDE) {
+    C *__restrict__ q = f + b;
 #pragma unroll
-  for (int e = 0; e < E; ++e) f[b + (unsigned)e * s] = v[e];
+    for (int e = 0; e < E; ++e) q[(unsigned long long)s * (unsigned)e] = v[e];
+  } else {
+#pragma unroll
+    for (int e = 0; e < E; ++e) f[b + (unsigned)e * s] = v[e];
+  }
 }
 
 // Register select with a runtime index (unrolled compare, no local memory).
@@ -738,10 +748,10 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CO
       float2 v[E];
       QJ_TAKE(v);
       fft_pencil<N, +1, true>(v, t, smv, tw);
-      store_pencil<E>(v, a.S1, base, st, t, P);
+      store_pencil<E, false>(v, a.S1, base, st, t, P);
       QJ_TAKE(v);
       fft_pencil<N, +1, true>(v, t, smv, tw);
-      store_pencil<E>(v, a.S2, base, st, t, P);
+      store_pencil<E, false>(v, a.S2, base, st, t, P);
     } else if constexpr (MODE == M_KICK) {
       const int aq = a.axis;  // the kick axis; ar = 2 - aq is the Poisson axis
       const unsigned gb = (unsigned)base + (unsigned)t * (unsigned)st, gs = (unsigned)P * (unsigned)st;
