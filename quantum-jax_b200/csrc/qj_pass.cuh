@@ -719,24 +719,27 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CO
         const int i = t + P * e;
         const float kr = tabk[i];
         const float k2 = kperp2 + kr * kr;
-        float2 vh;
-        if (k2 == 0.0f) {
-          // V^(0) = -4 pi G (sum rho - ncell rho_bar) / 1, scaled by 1/ncell
-          const double v0 = -a.fourpiG * (mean - a.rho_bar);
-          if (a.phi) {
-            *a.phi += a.phi_coef * v0;  // the one k = 0 element of the grid
-            vh = float2{0.0f, 0.0f};
-          } else {
-            vh = float2{(float)v0, 0.0f};
-          }
-        } else {
-          const float g = __fdividef(g0, k2);
-          vh = float2{v[e].x * g, v[e].y * g};
-        }
+        const float g = __fdividef(g0, k2);  // (k = 0 is replaced below)
+        const float2 vh = float2{v[e].x * g, v[e].y * g};
         const float f1 = 1.0f + tabk[N + i];
         v[e] = float2{vh.x * f1, vh.y * f1};
         // (kty - i ktq) * vh waits in the thread's save slots
         save[e * THREADS + tid] = float2{kty * vh.x + ktq * vh.y, kty * vh.y - ktq * vh.x};
+      }
+      if (t == 0 && kperp2 == 0.0f) {
+        // element 0 of the pencil with k_perp = 0 is k = 0:
+        // V^(0) = -4 pi G (sum rho - ncell rho_bar) / 1, scaled by 1/ncell
+        const double v0 = -a.fourpiG * (mean - a.rho_bar);
+        float2 vh;
+        if (a.phi) {
+          *a.phi += a.phi_coef * v0;  // the one k = 0 element of the grid
+          vh = float2{0.0f, 0.0f};
+        } else {
+          vh = float2{(float)v0, 0.0f};
+        }
+        const float f1 = 1.0f + tabk[N];
+        v[0] = float2{vh.x * f1, vh.y * f1};
+        save[tid] = float2{kty * vh.x + ktq * vh.y, kty * vh.y - ktq * vh.x};
       }
       fft_pencil<N, +1, true>(v, t, smv, tw);
       store_pencil<E>(v, a.S1, base, st, t, P);
