@@ -350,7 +350,14 @@ __device__ __forceinline__ double build_density(float2 (&v)[E], const FusedArgs 
 // degree 9 and 10 (truncation below 2e-10 for |r| <= pi/4), evaluated in
 // float32 by Horner's rule.
 __device__ __forceinline__ void sincos_reduced(double theta, float &sn, float &cs) {
-  const double n = rint(theta * 0.63661977236758134308);
+  // n = the integer nearest 2 theta / pi, by adding 1.5 * 2^52 (|2 theta / pi|
+  // < 2^51): the sum's low word is n in two's complement, so the quadrant
+  // needs no conversion.  (A product within an ulp of a half-integer may round
+  // the other way than rint of the rounded product; r then lies a hair beyond
+  // pi/4, where the series is still accurate.)
+  const double nm = fma(theta, 0.63661977236758134308, 6755399441055744.0);
+  const int qn = __double2loint(nm);
+  const double n = nm - 6755399441055744.0;
   const double r = (theta - n * 1.5707963267948965580e+00) - n * 6.1232339957367660359e-17;
   const float x = (float)r, x2 = x * x;
   const float s = x * (1.0f + x2 * (-1.6666667163e-01f +
@@ -359,7 +366,7 @@ __device__ __forceinline__ void sincos_reduced(double theta, float &sn, float &c
   const float c = 1.0f + x2 * (-0.5f + x2 * (4.1666667908e-02f +
                                     x2 * (-1.3888889225e-03f + x2 * (2.4801587642e-05f +
                                                                    x2 * -2.7557318845e-07f))));
-  const int q = (int)((long long)n & 3);
+  const int q = qn & 3;
   sn = q == 0 ? s : (q == 1 ? c : (q == 2 ? -s : -c));
   cs = q == 0 ? c : (q == 1 ? -s : (q == 2 ? -c : s));
 }
