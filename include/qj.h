@@ -278,6 +278,13 @@ int qj_autotune_kdk(qj_plan *plan, const void *psi, const void *pos, const void 
  * counterpart: the reference's XLA kernels have no device-side waits. */
 int qj_plan_status(qj_plan *plan);
 
+/* qj_plan_selftest_wait: exercises the failure report without a fault.  One
+ * warp waits, with the fused passes' bounded wait and a limit of limit_ns
+ * (1 ms .. 2 s), for an mbarrier that nothing completes; when the wait gives
+ * up it sets the plan's error word, so the next qj_plan_status returns
+ * QJ_ERR_TIMEOUT (and clears it).  No reference counterpart. */
+int qj_plan_selftest_wait(qj_plan *plan, int64_t limit_ns, void *stream);
+
 /* Instrumentation (no reference counterpart; used by the benchmark).
  * qj_launch_count: kernels libqj has launched in this process.
  * qj_profile_enable(1) clears and starts per-pass CUDA-event timing;

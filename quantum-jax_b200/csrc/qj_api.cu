@@ -1358,6 +1358,14 @@ int qj_plan_status(qj_plan *P) {
   return QJ_ERR_TIMEOUT;
 }
 
+int qj_plan_selftest_wait(qj_plan *P, int64_t limit_ns, void *stream) {
+  if (!P || limit_ns < 1000000 || limit_ns > 2000000000) {
+    set_error("qj_plan_selftest_wait: bad argument (limit_ns in [1e6, 2e9])");
+    return QJ_ERR_ARG;
+  }
+  return launch_selftest_wait(P->err, (long long)limit_ns, (cudaStream_t)stream);
+}
+
 int64_t qj_launch_count(void) { return (int64_t)g_launches.load(); }
 
 int qj_profile_enable(int on) {

@@ -293,6 +293,27 @@ int fused_max_ctas_per_sm(int mode, int n, bool contig) {
   return 0;
 }
 
+// Self-test of the bounded wait and its error report: one warp arms an
+// mbarrier for 16 bytes that no copy brings, waits for it with the fused
+// passes' bounded wait (limit_ns) and, when the wait gives up, sets bit 2 of
+// the error word.  No copy is in flight, so giving up is safe.
+__global__ void k_selftest_wait(unsigned *err, unsigned long long limit_ns) {
+  __shared__ __align__(8) unsigned long long bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    mbar_expect_tx(&bar, 16);
+  }
+  __syncthreads();
+  const bool ok = __syncthreads_and(mbar_wait_bounded(&bar, 0, limit_ns));
+  if (!ok && threadIdx.x == 0) atomicOr(err, 2u);
+}
+
+int launch_selftest_wait(unsigned *err, long long limit_ns, cudaStream_t st) {
+  k_selftest_wait<<<1, 32, 0, st>>>(err, (unsigned long long)limit_ns);
+  QJ_CK_LAUNCH();
+  return 0;
+}
+
 int launch_fused(int mode, int n, const FusedArgs &a, cudaStream_t st) {
   const bool prof = prof_on();
   if (prof) prof_mark_begin(st);

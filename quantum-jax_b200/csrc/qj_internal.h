@@ -43,6 +43,7 @@ std::vector<float2> stage_twiddles(int n);
 
 // ----- pencil passes (qj_fused.cu, qj_fftpass.cu) -----
 // Launch one fused single-precision pass of `mode` along `a.axis` (length n).
+int launch_selftest_wait(unsigned *err, long long limit_ns, cudaStream_t st);
 int launch_fused(int mode, int n, const FusedArgs &a, cudaStream_t st);
 // Number of CTAs a pass along `axis` launches (= partial sums written).
 int pass_blocks(int n_axis, int axis, int nx, int ny, int nz);

@@ -521,15 +521,16 @@ __device__ __forceinline__ unsigned long long global_ns() {
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
-// Bounded wait for phase `parity` of the landing barrier: gives up after 2 s
-// (or 2^24 polls) and returns false, so a copy that never completes cannot
-// hang the GPU.
-__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long *bar, unsigned parity) {
+// Bounded wait for phase `parity` of the landing barrier: gives up after
+// limit_ns (2 s by default) or 2^24 polls and returns false, so a copy that
+// never completes cannot hang the GPU.
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long *bar, unsigned parity,
+                                                  unsigned long long limit_ns = 2000000000ull) {
   if (mbar_try_wait(bar, parity)) return true;
   const unsigned long long t0 = global_ns();
   for (unsigned i = 0; i < (1u << 24); ++i) {
     if (mbar_try_wait(bar, parity)) return true;
-    if (global_ns() - t0 > 2000000000ull) break;
+    if (global_ns() - t0 > limit_ns) break;
   }
   return false;
 }
@@ -605,7 +606,13 @@ __device__ __forceinline__ bool take_tile(float2 (&v)[E], float2 &c0, const Fuse
   ok = __syncthreads_and(ok);
   parity ^= 1u;
   if (!ok) {
-    if (threadIdx.x == 0 && a.err) atomicOr(a.err, 1u);
+    if (threadIdx.x == 0) {
+      if (a.err) atomicOr(a.err, 1u);
+      // a copy still in flight would land in this CTA's shared memory: give
+      // it one more bounded wait before the CTA (kept alive by this thread)
+      // leaves
+      mbar_wait_bounded(bar, parity ^ 1u, 1000000000ull);
+    }
     return false;
   }
   // tile here is the loop index; the copy goes to its logical tile

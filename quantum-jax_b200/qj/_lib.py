@@ -71,6 +71,7 @@ SIGNATURES = {
                                              c_void_p, c_void_p, c_int, c_void_p]),
     "qj_plan_workspace_bytes": (c_int64, [c_void_p]),
     "qj_plan_status": (c_int, [c_void_p]),
+    "qj_plan_selftest_wait": (c_int, [c_void_p, c_int64, c_void_p]),
     "qj_plan_get_tuning": (c_int, [c_void_p, c_void_p, c_int]),
     "qj_fluid_accretion_step": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                         c_void_p, c_void_p, c_void_p, c_double, c_int, c_void_p,

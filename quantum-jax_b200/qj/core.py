@@ -179,6 +179,12 @@ class Plan:
         bounded wait for a tile copy since the last call."""
         check(lib().qj_plan_status(self._h))
 
+    def selftest_wait(self, limit_ms=20.0):
+        """Make one bounded device wait give up (nothing completes it) so that
+        the next status() reports the timeout; exercises the failure path
+        without a fault."""
+        check(lib().qj_plan_selftest_wait(self._h, int(limit_ms * 1e6), _stream()))
+
     # ----- argument checks -----
     def _field(self, t, name, complex_=False):
         dt = self.cdtype if complex_ else self.rdtype
