@@ -34,6 +34,17 @@ struct Idx3 {
   }
 };
 
+// a / b in the hydro stencils: correctly rounded in float64 (the path pinned
+// to the reference at 1e-10); the fast divide (within 2 ulp) in float32,
+// whose stencils are bound by their divisions
+template <typename R> __device__ __forceinline__ R hdiv(R a, R b) {
+  if constexpr (sizeof(R) == 4) {
+    return __fdividef(a, b);
+  } else {
+    return a / b;
+  }
+}
+
 // quantum-gas-bh.py:353-357
 template <typename R> __device__ __forceinline__ R adjust_denominator(R d) {
   const R eps = (R)1.0e-12;
@@ -59,10 +70,10 @@ __device__ Prim<R> cell_prim(const R *const F[4], const Idx3 &I, int x, int y, i
       const int ex = d == 0, ey = d == 1, ez = d == 2;
       const R fp = F[v][I.at(x + ex, y + ey, z + ez)];
       const R fm = F[v][I.at(x - ex, y - ey, z - ez)];
-      R g = (fp - fm) / ((R)2 * dx);
+      R g = hdiv(fp - fm, (R)2 * dx);
       const R denom = adjust_denominator(g);
-      g = clamp01(((c[v] - fm) / dx) / denom) * g;
-      g = clamp01((-(c[v] - fp) / dx) / denom) * g;
+      g = clamp01(hdiv(hdiv(c[v] - fm, dx), denom)) * g;
+      g = clamp01(hdiv(hdiv(-(c[v] - fp), dx), denom)) * g;
       P.g[v][d] = g;
     }
   }
@@ -78,19 +89,19 @@ __device__ Prim<R> cell_prim(const R *const F[4], const Idx3 &I, int x, int y, i
       const int ex = d == 0, ey = d == 1, ez = d == 2;
       const R fp = F[0][I.at(x + ex, y + ey, z + ez)] * c2;
       const R fm = F[0][I.at(x - ex, y - ey, z - ez)] * c2;
-      R g = (fp - fm) / ((R)2 * dx);
+      R g = hdiv(fp - fm, (R)2 * dx);
       const R denom = adjust_denominator(g);
-      g = clamp01(((Pc - fm) / dx) / denom) * g;
-      g = clamp01((-(Pc - fp) / dx) / denom) * g;
+      g = clamp01(hdiv(hdiv(Pc - fm, dx), denom)) * g;
+      g = clamp01(hdiv(hdiv(-(Pc - fp), dx), denom)) * g;
       gP[d] = g;
     }
     for (int v = 1; v < 4; ++v)
       P.f[v] = c[v] - h * (vx * P.g[v][0] + vy * P.g[v][1] + vz * P.g[v][2] +
-                           gP[v - 1] / (rho + (R)1e-30));
+                           hdiv(gP[v - 1], rho + (R)1e-30));
   } else {
     for (int v = 1; v < 4; ++v)
       P.f[v] = c[v] - h * (vx * P.g[v][0] + vy * P.g[v][1] + vz * P.g[v][2] +
-                           ((R)1 / rho) * P.g[0][v - 1] * cs * cs);
+                           hdiv((R)1, rho) * P.g[0][v - 1] * cs * cs);
   }
   return P;
 }
@@ -112,16 +123,16 @@ __device__ __forceinline__ void rusanov(R rL, R uL, R aL, R bL, R rR, R uR, R aR
     const R P_star = rho_star * ((R)0.5 * (c2 + c2));
     const R eps = (R)1e-30;
     fM = mu;
-    fU = mu * mu / (rho_star + eps) + P_star;
-    fA = mu * ma / (rho_star + eps);
-    fB = mu * mb / (rho_star + eps);
+    fU = hdiv(mu * mu, rho_star + eps) + P_star;
+    fA = hdiv(mu * ma, rho_star + eps);
+    fB = hdiv(mu * mb, rho_star + eps);
     C = fmax(sqrt(c2) + fabs(uL), sqrt(c2) + fabs(uR));
   } else {
     const R P_star = rho_star * cs * cs;
     fM = mu;
-    fU = mu * mu / rho_star + P_star;
-    fA = mu * ma / rho_star;
-    fB = mu * mb / rho_star;
+    fU = hdiv(mu * mu, rho_star) + P_star;
+    fA = hdiv(mu * ma, rho_star);
+    fB = hdiv(mu * mb, rho_star);
     C = fmax(cs + fabs(uL), cs + fabs(uR));
   }
   fM = fM - C * (R)0.5 * (rR - rL);
@@ -225,13 +236,13 @@ __global__ void __launch_bounds__(256)
     U[v] = u;
   }
   // get_primitive (:179-185; quantum-fluid-accretion.py:200-206 with eps)
-  R r = U[0] / vol;
+  R r = hdiv(U[0], vol);
   if (clamp_rho) r = fmax((R)0, r);
   rho[i] = r;
   const R den = FACC ? U[0] + (R)1e-30 : U[0];
-  vx[i] = U[1] / den;
-  vy[i] = U[2] / den;
-  vz[i] = U[3] / den;
+  vx[i] = hdiv(U[1], den);
+  vy[i] = hdiv(U[2], den);
+  vz[i] = hdiv(U[3], den);
 }
 
 // do_accretion (quantum-gas-bh.py:497-530; quantum-bh.py:306-339 with sigma)
