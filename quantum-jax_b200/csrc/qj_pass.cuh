@@ -794,11 +794,15 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CO
                                      });
         }
         if (a.gv[0]) {
+          // v += a dt/2 as fire-and-forget adds at L2: each element has one
+          // writer, so this is the same single rounding as load-add-store, but
+          // nothing waits on it (a load-add-store could not move the next load
+          // above the store: the compiler cannot tell the elements apart)
           float *gq = aq == 0 ? a.gv[0] : a.gv[2], *gy = a.gv[1];
 #pragma unroll
           for (int e = 0; e < E; ++e) {
-            gq[gb + e * gs] = gq[gb + e * gs] + v2[e].x * a.gas_dt;
-            gy[gb + e * gs] = gy[gb + e * gs] + v2[e].y * a.gas_dt;
+            atomicAdd(gq + (gb + e * gs), v2[e].x * a.gas_dt);
+            atomicAdd(gy + (gb + e * gs), v2[e].y * a.gas_dt);
           }
         }
       }
@@ -821,10 +825,10 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CO
                                            save[(m / P) * THREADS + tid].x;
                                      });
         }
-        if (a.gv[0]) {  // gas half kick, quantum-gas-bh.py:255-266
+        if (a.gv[0]) {  // gas half kick, quantum-gas-bh.py:255-266 (adds as above)
           float *g = aq == 0 ? a.gv[2] : a.gv[0];
 #pragma unroll
-          for (int e = 0; e < E; ++e) g[gb + e * gs] = g[gb + e * gs] + v1[e].y * a.gas_dt;
+          for (int e = 0; e < E; ++e) atomicAdd(g + (gb + e * gs), v1[e].y * a.gas_dt);
         }
       }
       // phase 3: psi <- exp(-i c V) psi with V = Poisson + b rho + V_ext, then
