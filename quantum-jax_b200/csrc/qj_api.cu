@@ -153,7 +153,7 @@ struct qj_plan {
   int tune[QJ_TUNE_N] = {0, 0, 0, 0, 0, 0, 0, 0, -1, 0};  // launch tuning (include/qj.h)
   void *tmp_scalar = nullptr;
   void *tmp_diag = nullptr;
-  void *gas_prim = nullptr;  // hydro: 16 values per cell (limited gradients, predicted primitives)
+  void *gas_prim = nullptr;  // hydro: 16 values per cell as 4 quads (predicted primitives, gradients by axis)
   // adjoint: recomputed chunk states
   void *adj_psi = nullptr, *adj_states = nullptr, *adj_V = nullptr;
   int adj_cap = 0;

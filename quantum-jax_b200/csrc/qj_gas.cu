@@ -168,7 +168,15 @@ __device__ void face_flux(const Prim<R> &L, const Prim<R> &Rt, int d, R dx, R cs
   }
 }
 
-// Record of one cell: P[k * ncell + i], k = f[0..3] then g[v][d] at 4 + 3 v + d.
+// Four values of one cell's record, stored together (16-byte loads and
+// stores in float32, two per group in float64).
+template <typename R> struct alignas(4 * sizeof(R)) Quad {
+  R a, b, c, e;
+};
+
+// Record of one cell, four quads: Q[i] = the predicted primitives f[0..3],
+// Q[(1 + d) ncell + i] = the gradients g[0..3][d] along axis d -- so a face
+// along d reads two quads of each neighbour.
 template <typename R, bool FACC>
 __global__ void __launch_bounds__(256)
     k_hydro_prim(const R *rho, const R *vx, const R *vy, const R *vz, R *P, int n, R dx, R dt, R cs) {
@@ -178,22 +186,26 @@ __global__ void __launch_bounds__(256)
   const int z = (int)(i % n), y = (int)((i / n) % n), x = (int)(i / ((long long)n * n));
   const R *const F[4] = {rho, vx, vy, vz};
   const Prim<R> C = cell_prim<R, FACC>(F, Idx3{n}, x, y, z, dx, dt, cs);
+  Quad<R> *Q = reinterpret_cast<Quad<R> *>(P);
+  Q[i] = Quad<R>{C.f[0], C.f[1], C.f[2], C.f[3]};
 #pragma unroll
-  for (int k = 0; k < 4; ++k) P[k * ncell + i] = C.f[k];
-#pragma unroll
-  for (int v = 0; v < 4; ++v)
-#pragma unroll
-    for (int d = 0; d < 3; ++d) P[(4 + 3 * v + d) * ncell + i] = C.g[v][d];
+  for (int d = 0; d < 3; ++d) Q[(1 + d) * ncell + i] = Quad<R>{C.g[0][d], C.g[1][d], C.g[2][d], C.g[3][d]};
 }
 
 // the primitives and the axis-d gradients of cell j (what face_flux uses)
 template <typename R>
 __device__ __forceinline__ void load_face_prim(const R *P, long long ncell, long long j, int d,
                                                Prim<R> &q) {
-#pragma unroll
-  for (int k = 0; k < 4; ++k) q.f[k] = P[k * ncell + j];
-#pragma unroll
-  for (int v = 0; v < 4; ++v) q.g[v][d] = P[(4 + 3 * v + d) * ncell + j];
+  const Quad<R> *Q = reinterpret_cast<const Quad<R> *>(P);
+  const Quad<R> f = Q[j], g = Q[(1 + d) * ncell + j];
+  q.f[0] = f.a;
+  q.f[1] = f.b;
+  q.f[2] = f.c;
+  q.f[3] = f.e;
+  q.g[0][d] = g.a;
+  q.g[1][d] = g.b;
+  q.g[2][d] = g.c;
+  q.g[3][d] = g.e;
 }
 
 template <typename R, bool FACC>
