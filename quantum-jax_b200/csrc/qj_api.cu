@@ -250,6 +250,7 @@ FusedArgs fused_args(const qj_plan *P, int axis) {
   a.stride = axis == 0 ? (long long)P->n[1] * P->n[2] : (axis == 1 ? P->n[2] : 1);
   a.outer_stride = axis == 0 ? P->n[2] : (long long)P->n[1] * P->n[2];
   a.ztiles = P->n[2] / 16;
+  a.full_nx = P->n[0];
   a.R = P->R;
   a.S1 = P->S1;
   a.S2 = P->S2;
@@ -282,6 +283,18 @@ void set_stars(FusedArgs &a, const qj_plan *P) {
   a.perm = P->sb.perm;
   a.bstart = P->sb.bstart;
   a.A = P->sb.A;
+}
+
+// The forward y and Poisson passes over half of the density's spectrum along
+// axis q (0 or 2), the axis its first forward transform ran along: the density
+// is real, so k_q > n_q / 2 follows from k_q < n_q / 2 (the Poisson pass writes
+// those as mirrors).  x: the first n/2 + 1 planes; z: the 16-wide tiles that
+// hold k_z <= n/2.
+void half_spectrum(FusedArgs &a, const qj_plan *P, int q) {
+  if (q == 0)
+    a.nx = P->n[0] / 2 + 1;
+  else
+    a.ztiles = (P->n[2] / 2 + 1 + 15) / 16;
 }
 
 int ensure_prop(qj_plan *P, double dtk, cudaStream_t st) {
@@ -356,10 +369,13 @@ int fused_kdk(qj_plan *P, float2 *psi, float *pos, float *vel, int n_s, double m
     if (!last) QJ_TRY(ensure_prop(P, drift_dt(k), st));
     {
       FusedArgs a = fused_args(P, 1);
+      half_spectrum(a, P, q);
       QJ_TRY(launch_fused(M_FFT_FWD, P->n[1], a, st));
     }
     {
       FusedArgs a = fused_args(P, r);
+      a.half = 1;
+      half_spectrum(a, P, q);
       a.part_in = P->part;
       a.n_part = pass_blocks(P->n[q], q, P->n[0], P->n[1], P->n[2]);
       if (use_phi) {
@@ -641,8 +657,11 @@ int fused_gas_step(qj_plan *P, const GasArgs &g, cudaStream_t st, bool first, bo
   };
   auto poisson = [&](int q, int r) -> int {
     FusedArgs a = fused_args(P, 1);
+    half_spectrum(a, P, q);
     QJ_TRY(launch_fused(M_FFT_FWD, P->n[1], a, st));
     a = fused_args(P, r);
+    a.half = 1;
+    half_spectrum(a, P, q);
     a.part_in = P->part;
     a.n_part = pass_blocks(P->n[q], q, P->n[0], P->n[1], P->n[2]);
     a.phi = P->phi;

@@ -22,8 +22,13 @@ bool fft_length_supported(int n) {
 template <int N, bool CONTIG>
 static int grid_of(const FusedArgs &a) {
   using SH = PassShape<N, CONTIG>;
-  if (CONTIG) return (a.nx * a.ny) / SH::TP;
-  return (a.axis == 0 ? a.ny : a.nx) * (a.nz / 16);
+  if (CONTIG) {
+    // a reduced range (half spectrum) rounds up to whole tiles, within the
+    // grid; the rows past it are pencils the pass does not store
+    const int full = ((a.full_nx > 0 ? a.full_nx : a.nx) * a.ny) / SH::TP;
+    return std::min(full, (a.nx * a.ny + SH::TP - 1) / SH::TP);
+  }
+  return (a.axis == 0 ? a.ny : a.nx) * a.ztiles;
 }
 
 // Stage twiddle table of length n (see stage_tw_off), long double, rounded once.

@@ -88,6 +88,10 @@ struct FusedArgs {
   float gas_dt;
   // tiles of this pass per box (the persistent CTAs stride over them)
   int ntiles;
+  // forward y / Poisson passes over half of the real density's spectrum (the
+  // other non-y axis to n/2); the Poisson pass then also writes the mirrors
+  int half;
+  int full_nx;  // nx of the grid (nx itself may hold a pass's reduced range)
   // walk the tiles from the last: a pass then first reads what the previous
   // pass wrote last, which is still in L2
   int rev;
@@ -735,10 +739,9 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CO
         const float k2 = kperp2 + kr * kr;
         const float g = __fdividef(g0, k2);  // (k = 0 is replaced below)
         const float2 vh = float2{v[e].x * g, v[e].y * g};
-        const float f1 = 1.0f + tabk[N + i];
-        v[e] = float2{vh.x * f1, vh.y * f1};
-        // (kty - i ktq) * vh waits in the thread's save slots
-        save[e * THREADS + tid] = float2{kty * vh.x + ktq * vh.y, kty * vh.y - ktq * vh.x};
+        v[e] = vh;  // A = IFFT(V^)
+        const float kb = tabk[N + i];
+        save[e * THREADS + tid] = float2{vh.x * kb, vh.y * kb};  // B = IFFT(kt_r V^), later
       }
       if (t == 0 && kperp2 == 0.0f) {
         // element 0 of the pencil with k_perp = 0 is k = 0:
@@ -751,16 +754,57 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CO
         } else {
           vh = float2{(float)v0, 0.0f};
         }
-        const float f1 = 1.0f + tabk[N];
-        v[0] = float2{vh.x * f1, vh.y * f1};
-        save[tid] = float2{kty * vh.x + ktq * vh.y, kty * vh.y - ktq * vh.x};
+        v[0] = vh;
+        save[tid] = float2{vh.x * tabk[N], vh.y * tabk[N]};
       }
-      fft_pencil<N, +1, true>(v, t, smv, tw);
-      store_pencil<E>(v, a.S1, base, st, t, P);
+      // S1 = IFFT((1 + kt_r) V^) = A + B and S2 = IFFT((kty - i ktq) V^) =
+      // (kty - i ktq) A (the factor is constant along the pencil).
+      // With a.half the pass covers k_q <= n_q / 2 of the real density's
+      // Hermitian spectrum (q = the other non-y axis), and pencil (k_q, k_y)
+      // also writes its mirror (-k_q, -k_y), whose V^ is conj(V^(-k)): for a
+      // spectrum m(k) V^_mirror(k) the inverse is conj(IFFT[conj(m(-k)) V^](n)),
+      // so S1' = conj(A - B) and S2' = conj((-kty - i ktq) A).  Pencils past
+      // n_q / 2 (padding of a z tile) write nothing; k_q = 0 and n_q / 2 are
+      // their own mirrors' partners and write only themselves.
+      const int nq = aq == 0 ? a.full_nx : a.nz;
+      const bool own = !a.half || 2 * cq <= nq;
+      const bool mirror = a.half && cq >= 1 && 2 * cq < nq;
+      const int m0 = ax == 0 ? 0 : (a.full_nx - pp.c[0]) % a.full_nx;
+      const int m1 = (a.ny - pp.c[1]) % a.ny;
+      const int m2 = ax == 2 ? 0 : (a.nz - pp.c[2]) % a.nz;
+      const unsigned es = (unsigned)P * (unsigned)st;  // element step of a thread
+      float2 *__restrict__ o1 = a.S1 + ((unsigned)base + (unsigned)t * (unsigned)st);
+      float2 *__restrict__ o2 = a.S2 + ((unsigned)base + (unsigned)t * (unsigned)st);
+      const long long mb = ((long long)m0 * a.ny + m1) * a.nz + m2;
+      float2 *__restrict__ q1 = a.S1 + ((unsigned)mb + (unsigned)t * (unsigned)st);
+      float2 *__restrict__ q2 = a.S2 + ((unsigned)mb + (unsigned)t * (unsigned)st);
+      fft_pencil<N, +1, true>(v, t, smv, tw);  // A
+      if (own) {
 #pragma unroll
-      for (int e = 0; e < E; ++e) v[e] = save[e * THREADS + tid];
-      fft_pencil<N, +1, true>(v, t, smv, tw);
-      store_pencil<E>(v, a.S2, base, st, t, P);
+        for (int e = 0; e < E; ++e)
+          o2[(unsigned long long)es * (unsigned)e] =
+              float2{kty * v[e].x + ktq * v[e].y, kty * v[e].y - ktq * v[e].x};
+      }
+      if (mirror) {
+#pragma unroll
+        for (int e = 0; e < E; ++e)
+          q2[(unsigned long long)es * (unsigned)e] =
+              float2{-kty * v[e].x + ktq * v[e].y, kty * v[e].y + ktq * v[e].x};
+      }
+      // A waits in the save slots while B is transformed
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const float2 b = save[e * THREADS + tid];
+        save[e * THREADS + tid] = v[e];
+        v[e] = b;
+      }
+      fft_pencil<N, +1, true>(v, t, smv, tw);  // B
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const float2 A = save[e * THREADS + tid];
+        if (own) o1[(unsigned long long)es * (unsigned)e] = float2{A.x + v[e].x, A.y + v[e].y};
+        if (mirror) q1[(unsigned long long)es * (unsigned)e] = float2{A.x - v[e].x, v[e].y - A.y};
+      }
     } else if constexpr (MODE == M_IFFT2) {
       float2 v[E];
       QJ_TAKE(v);
