@@ -42,11 +42,12 @@ UNIT = "cell-steps/s"
 # input read once, each output written once).
 PASS_NAMES = ["density", "fft_y", "poisson", "ifft2_y", "kick_drift", "drift_y",
               "drift_density", "deposit_sort", "particles"]
-# The forward y and Poisson passes cover half of the real density's spectrum:
-# forward y reads and writes half of R (8), Poisson reads half of R and writes
-# S1 and S2 whole (4 + 16).
-PASS_BYTES = {0: 16, 1: 8, 2: 20, 3: 32, 4: 32, 5: 16, 6: 24}
-STEP_BYTES = 132  # per cell per steady-state step: passes 1..6 once each
+# The forward y, Poisson and inverse y passes cover half of the real density's
+# spectrum: forward y reads and writes half of R (8), Poisson reads half of R
+# and writes half of A~ and B~ (4 + 8), inverse y reads those halves and writes
+# S1 and S2 whole (8 + 16).
+PASS_BYTES = {0: 16, 1: 8, 2: 12, 3: 24, 4: 32, 5: 16, 6: 24}
+STEP_BYTES = 116  # per cell per steady-state step: passes 1..6 once each
 
 
 def parse():

@@ -291,6 +291,7 @@ void set_stars(FusedArgs &a, const qj_plan *P) {
 // those as mirrors).  x: the first n/2 + 1 planes; z: the 16-wide tiles that
 // hold k_z <= n/2.
 void half_spectrum(FusedArgs &a, const qj_plan *P, int q) {
+  a.hq = q;
   if (q == 0)
     a.nx = P->n[0] / 2 + 1;
   else
@@ -386,6 +387,8 @@ int fused_kdk(qj_plan *P, float2 *psi, float *pos, float *vel, int n_s, double m
     }
     {
       FusedArgs a = fused_args(P, 1);
+      a.half = 1;
+      half_spectrum(a, P, q);
       QJ_TRY(launch_fused(M_IFFT2, P->n[1], a, st));
     }
     {
@@ -668,6 +671,8 @@ int fused_gas_step(qj_plan *P, const GasArgs &g, cudaStream_t st, bool first, bo
     a.phi_coef = half;
     QJ_TRY(launch_fused(M_POISSON, P->n[r], a, st));
     a = fused_args(P, 1);
+    a.half = 1;
+    half_spectrum(a, P, q);
     return launch_fused(M_IFFT2, P->n[1], a, st);
   };
   auto kick = [&](int q, int drift) -> int {

@@ -91,6 +91,7 @@ struct FusedArgs {
   // forward y / Poisson passes over half of the real density's spectrum (the
   // other non-y axis to n/2); the Poisson pass then also writes the mirrors
   int half;
+  int hq;       // the half axis q (0 or 2)
   int full_nx;  // nx of the grid (nx itself may hold a pass's reduced range)
   // walk the tiles from the last: a pass then first reads what the previous
   // pass wrote last, which is still in L2
@@ -461,10 +462,12 @@ template <int N, bool CONTIG, int MODE> struct FusedSmem {
   using SH = PassShape<N, CONTIG>;
   static constexpr bool DRIFTS = MODE == M_KICK || MODE == M_DRIFT || MODE == M_DRIFT_DENSITY;
   static constexpr bool LANDS = MODE != M_DEPOSIT;
-  static constexpr bool SAVES = DRIFTS || MODE == M_POISSON;
+  static constexpr bool SAVES = DRIFTS || MODE == M_POISSON || MODE == M_IFFT2;
   static constexpr size_t a16(size_t x) { return (x + 15) & ~(size_t)15; }
   // per-axis tables: the drift propagator (N complex) or k and k~ (2 N floats)
-  static constexpr size_t TAB_BYTES = DRIFTS ? N * sizeof(float2) : (MODE == M_POISSON ? 2 * N * sizeof(float) : 0);
+  static constexpr size_t TAB_BYTES = DRIFTS ? N * sizeof(float2)
+                                      : (MODE == M_POISSON ? 2 * N * sizeof(float)
+                                                           : (MODE == M_IFFT2 ? N * sizeof(float) : 0));
   static constexpr size_t TW = a16(SH::template smem_bytes<float2>());
   static constexpr size_t TAB = a16(TW + (size_t)stage_tw_size<N>() * sizeof(float2));
   static constexpr size_t SAVE = a16(TAB + TAB_BYTES);
@@ -668,6 +671,8 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CO
   for (int i = tid; i < stage_tw_size<N>(); i += THREADS) tw_s[i] = a.tw[i];
   if constexpr (LAY::DRIFTS) {
     for (int i = tid; i < N; i += THREADS) tab2[i] = a.prop[i];
+  } else if constexpr (MODE == M_IFFT2) {
+    for (int i = tid; i < N; i += THREADS) tabk[i] = a.kt[1][i];  // kt along y
   } else if constexpr (MODE == M_POISSON) {
     for (int i = tid; i < N; i += THREADS) {
       tabk[i] = (a.axis == 0 ? a.k[0] : (a.axis == 1 ? a.k[1] : a.k[2]))[i];
@@ -779,6 +784,16 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CO
       float2 *__restrict__ q1 = a.S1 + ((unsigned)mb + (unsigned)t * (unsigned)st);
       float2 *__restrict__ q2 = a.S2 + ((unsigned)mb + (unsigned)t * (unsigned)st);
       fft_pencil<N, +1, true>(v, t, smv, tw);  // A
+      if (a.half) {
+        // A~ and B~ of this half pencil go to S1 and S2 as they are; the
+        // inverse y pass forms S1, S2 and their mirrors from them
+        if (own) store_pencil<E>(v, a.S1, base, st, t, P);
+#pragma unroll
+        for (int e = 0; e < E; ++e) v[e] = save[e * THREADS + tid];
+        fft_pencil<N, +1, true>(v, t, smv, tw);  // B
+        if (own) store_pencil<E>(v, a.S2, base, st, t, P);
+        continue;
+      }
       if (own) {
 #pragma unroll
         for (int e = 0; e < E; ++e)
@@ -808,6 +823,59 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CO
     } else if constexpr (MODE == M_IFFT2) {
       float2 v[E];
       QJ_TAKE(v);
+      if (a.half) {
+        // y pencils (k_q <= n_q / 2, n_r) of A~ = IFFT_r V^ and B~ = IFFT_r kt_r V^
+        // (in S1, S2).  Their mirrors (-k_q, -k_y) are conj(A~) and -conj(B~), so
+        // along y: S1 = A~ + B~, S2 = (kt_y - i kt_q) A~, and the mirror y pencil
+        // (-k_q, n_r) is conj(IFFT_y[A~ - B~]), conj(IFFT_y[(-kt_y - i kt_q) A~]).
+        const int cq = a.hq == 0 ? pp.c[0] : pp.c[2];
+        const int nq = a.hq == 0 ? a.full_nx : a.nz;
+        const bool own = 2 * cq <= nq, mirror = cq >= 1 && 2 * cq < nq;
+        const float ktq = a.hq == 0 ? a.kt[0][cq] : a.kt[2][cq];
+        const long long mb = a.hq == 0
+                                 ? (long long)((a.full_nx - cq) % a.full_nx) * a.ny * a.nz + pp.c[2]
+                                 : (long long)pp.c[0] * a.ny * a.nz + (a.nz - cq) % a.nz;
+        float2 w[E];
+#pragma unroll
+        for (int e = 0; e < E; ++e) save[e * THREADS + tid] = v[e];  // A~
+        QJ_TAKE(w);                                                 // B~
+#pragma unroll
+        for (int e = 0; e < E; ++e) v[e] = float2{v[e].x + w[e].x, v[e].y + w[e].y};
+        fft_pencil<N, +1, true>(v, t, smv, tw);
+        if (own) store_pencil<E, false>(v, a.S1, base, st, t, P);
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+          const float2 A = save[e * THREADS + tid];
+          v[e] = float2{A.x - w[e].x, A.y - w[e].y};
+        }
+        fft_pencil<N, +1, true>(v, t, smv, tw);
+        if (mirror) {
+#pragma unroll
+          for (int e = 0; e < E; ++e) v[e].y = -v[e].y;
+          store_pencil<E, false>(v, a.S1, mb, st, t, P);
+        }
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+          const float2 A = save[e * THREADS + tid];
+          const float ky = tabk[t + P * e];
+          v[e] = float2{ky * A.x + ktq * A.y, ky * A.y - ktq * A.x};
+        }
+        fft_pencil<N, +1, true>(v, t, smv, tw);
+        if (own) store_pencil<E, false>(v, a.S2, base, st, t, P);
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+          const float2 A = save[e * THREADS + tid];
+          const float ky = tabk[t + P * e];
+          v[e] = float2{-ky * A.x + ktq * A.y, -ky * A.y - ktq * A.x};
+        }
+        fft_pencil<N, +1, true>(v, t, smv, tw);
+        if (mirror) {
+#pragma unroll
+          for (int e = 0; e < E; ++e) v[e].y = -v[e].y;
+          store_pencil<E, false>(v, a.S2, mb, st, t, P);
+        }
+        continue;
+      }
       fft_pencil<N, +1, true>(v, t, smv, tw);
       store_pencil<E, false>(v, a.S1, base, st, t, P);
       QJ_TAKE(v);
