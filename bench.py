@@ -42,12 +42,12 @@ UNIT = "cell-steps/s"
 # input read once, each output written once).
 PASS_NAMES = ["density", "fft_y", "poisson", "ifft2_y", "kick_drift", "drift_y",
               "drift_density", "deposit_sort", "particles"]
-# The forward y, Poisson and inverse y passes cover half of the real density's
-# spectrum: forward y reads and writes half of R (8), Poisson reads half of R
-# and writes half of A~ and B~ (4 + 8), inverse y reads those halves and writes
-# S1 and S2 whole (8 + 16).
-PASS_BYTES = {0: 16, 1: 8, 2: 12, 3: 24, 4: 32, 5: 16, 6: 24}
-STEP_BYTES = 116  # per cell per steady-state step: passes 1..6 once each
+# Only half of the real density's spectrum R is kept: the density passes write
+# half of R (density 8 + 4, drift + density 16 + 4), forward y reads and writes
+# half of R (8), Poisson reads half of R and writes half of A~ and B~ (4 + 8),
+# inverse y reads those halves and writes S1 and S2 whole (8 + 16).
+PASS_BYTES = {0: 12, 1: 8, 2: 12, 3: 24, 4: 32, 5: 16, 6: 20}
+STEP_BYTES = 112  # per cell per steady-state step: passes 1..6 once each
 
 
 def parse():

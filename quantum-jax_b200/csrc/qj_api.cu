@@ -362,6 +362,7 @@ int fused_kdk(qj_plan *P, float2 *psi, float *pos, float *vel, int n_s, double m
     FusedArgs a = fused_args(P, q);
     a.psi = psi;
     if (parts) set_stars(a, P);
+    a.half = 1;  // the passes after it read k <= n/2 of R
     QJ_TRY(launch_fused(M_DENSITY, P->n[q], a, st));
   }
   for (int k = 0; k <= nsteps; ++k) {
@@ -444,6 +445,7 @@ int fused_kdk(qj_plan *P, float2 *psi, float *pos, float *vel, int n_s, double m
           QJ_CK(cudaStreamWaitEvent(st, P->ev_parts, 0));
           set_stars(a, P);
         }
+        a.half = 1;  // the passes after it read k <= n/2 of R
         QJ_TRY(launch_fused(M_DRIFT_DENSITY, P->n[r], a, st));
       }
       if (save)  // the state after drift k (before kick k + 1), for the adjoint
@@ -704,6 +706,7 @@ int fused_gas_step(qj_plan *P, const GasArgs &g, cudaStream_t st, bool first, bo
     FusedArgs a = fused_args(P, 2);
     a.psi = (float2 *)g.psi;
     stars(a);
+    a.half = 1;  // the passes after it read k <= n/2 of R
     QJ_TRY(launch_fused(M_DENSITY, P->n[2], a, st));
   }
   QJ_TRY(poisson(2, 0));
@@ -732,6 +735,7 @@ int fused_gas_step(qj_plan *P, const GasArgs &g, cudaStream_t st, bool first, bo
     FusedArgs a = fused_args(P, 0);
     a.psi = (float2 *)g.psi;
     stars(a);
+    a.half = 1;  // the passes after it read k <= n/2 of R
     QJ_TRY(launch_fused(M_DRIFT_DENSITY, P->n[0], a, st));
   }
   // (1/2) kick

@@ -195,6 +195,18 @@ __device__ __forceinline__ void store_pencil(const C (&v)[E], C *__restrict__ f,
   }
 }
 
+// store_pencil of the elements t + P e <= N / 2 only: the half of a real
+// field's spectrum the passes after it read.
+template <int N, int E, typename C>
+__device__ __forceinline__ void store_pencil_half(const C (&v)[E], C *__restrict__ f, long long base,
+                                                  long long stride, int t, int P) {
+  C *__restrict__ q = f + ((unsigned)base + (unsigned)t * (unsigned)stride);
+  const unsigned s = (unsigned)P * (unsigned)stride;
+#pragma unroll
+  for (int e = 0; e < E; ++e)
+    if (2 * (t + P * e) <= N) q[(unsigned long long)s * (unsigned)e] = v[e];
+}
+
 // Register select with a runtime index (unrolled compare, no local memory).
 template <int E>
 __device__ __forceinline__ void reg_add(float2 (&v)[E], int e, float add) {
@@ -710,7 +722,10 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CO
       s = block_sum<THREADS>(s, red);
       if (tid == 0) a.part[tile] = s;
       fft_pencil<N, -1, true>(v, t, smv, tw);
-      store_pencil<E>(v, a.R, base, st, t, P);
+      if (a.half)
+        store_pencil_half<N, E>(v, a.R, base, st, t, P);
+      else
+        store_pencil<E>(v, a.R, base, st, t, P);
     } else if constexpr (MODE == M_FFT_FWD) {
       float2 v[E];
       QJ_TAKE(v);
@@ -1016,7 +1031,10 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CO
         s = block_sum<THREADS>(s, red);
         if (tid == 0) a.part[tile] = s;
         fft_pencil<N, -1, true>(v, t, smv, tw);
-        store_pencil<E>(v, a.R, base, st, t, P);
+        if (a.half)
+          store_pencil_half<N, E>(v, a.R, base, st, t, P);
+        else
+          store_pencil<E>(v, a.R, base, st, t, P);
       }
     }
 #undef QJ_TAKE
