@@ -311,6 +311,16 @@ int ensure_prop(qj_plan *P, double dtk, cudaStream_t st) {
 
 int n_pencils(const qj_plan *P, int q) { return (int)(P->ncell / P->n[q]); }
 
+// Particle data of a single box, sorted by bucket (pencil of the lower corner
+// along q): one launch for a few particles (black holes), else prepare + sort.
+int stars_prepare_sort(qj_plan *P, const void *pos, int n, const void *masses, double m_s, int q,
+                       cudaStream_t st) {
+  if (n <= 32) return launch_stars_small(pos, n, masses, m_s, geom(P), q, n_pencils(P, q), P->sb, st);
+  QJ_TRY(launch_stars_prepare(pos, n, masses, m_s, geom(P), q, P->sb, st));
+  return launch_bucket_sort(n, n_pencils(P, q), P->sb, st);
+}
+
+
 // CIC deposit list of `pos` in orientation q: sorted unique cells + starts.
 int deposit_list(qj_plan *P, const void *pos, int n, double m_s, const void *masses, int q,
                  bool keys_ready, void *dts_reset, cudaStream_t st) {
@@ -699,8 +709,7 @@ int fused_gas_step(qj_plan *P, const GasArgs &g, cudaStream_t st, bool first, bo
   u.masses = g.m_bh;
   // (1/2) kick
   if (bh) {
-    QJ_TRY(launch_stars_prepare(g.pos, g.n_bh, g.m_bh, 0.0, geom(P), 2, P->sb, st));
-    QJ_TRY(launch_bucket_sort(g.n_bh, n_pencils(P, 2), P->sb, st));
+    QJ_TRY(stars_prepare_sort(P, g.pos, g.n_bh, g.m_bh, 0.0, 2, st));
   }
   {
     FusedArgs a = fused_args(P, 2);
@@ -728,8 +737,7 @@ int fused_gas_step(qj_plan *P, const GasArgs &g, cudaStream_t st, bool first, bo
                         g.bondi, st));
   if (bh) {
     // deposit of the drifted black holes (their mass may have changed)
-    QJ_TRY(launch_stars_prepare(g.pos, g.n_bh, g.m_bh, 0.0, geom(P), 0, P->sb, st));
-    QJ_TRY(launch_bucket_sort(g.n_bh, n_pencils(P, 0), P->sb, st));
+    QJ_TRY(stars_prepare_sort(P, g.pos, g.n_bh, g.m_bh, 0.0, 0, st));
   }
   {
     FusedArgs a = fused_args(P, 0);

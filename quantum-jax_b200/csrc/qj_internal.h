@@ -115,6 +115,9 @@ int launch_stars_prepare(const void *pos, int n, const void *masses, double m_s,
 // stride bstride.
 int launch_bucket_sort(int n, int n_buckets, const StarBufs &b, cudaStream_t st, int nbox = 1,
                        int bstride = 0);
+// n <= 32 particles, one box: launch_stars_prepare + launch_bucket_sort in one launch
+int launch_stars_small(const void *pos, int n, const void *masses, double m_s, const CicGeomD &g,
+                       int q, int n_buckets, const StarBufs &b, cudaStream_t st);
 int launch_update_fused(void *pos, void *vel, const CicGeomD &g, const UpdateArgs &u,
                         const StarBufs &b, cudaStream_t st);
 

@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <mutex>
 
+#include "../../include/qj.h"
 #include "qj_internal.h"
 
 namespace qj {
@@ -480,6 +481,66 @@ int launch_stars_prepare(const void *pos, int n, const void *masses, double m_s,
   const double fac = m_s / (g.d[0] * g.d[1] * g.d[2]);
   k_stars_prepare<<<B, T, 0, st>>>((const float *)pos, n, (const float *)masses, (float)fac,
                                    cast_geom<float>(g), q, b.sidx, b.sw0, b.sw1, b.bkey);
+  QJ_CK_LAUNCH();
+  return 0;
+}
+
+// A few particles (n <= 32: black holes): star_prepare, the sort by (bucket,
+// index) and the bucket starts in one launch.  Every block works out the n
+// keys; block 0 also stores the particle data, the permutation and the sorted
+// keys (each particle's rank by counting, the order of the stable sort); every
+// block fills its share of bstart[b] = the number of keys below b, the lower
+// bound k_bucket_starts finds.
+constexpr int kSmallStars = 32;
+__global__ void __launch_bounds__(256)
+    k_stars_small(const float *pos, int n, const float *masses, float fac_all, CicGeom<float> g,
+                  int q, int4 *sidx, float4 *sw0, float4 *sw1, unsigned *bkey, unsigned *perm,
+                  unsigned *skey, int *bstart, int n_buckets) {
+  __shared__ unsigned keys[kSmallStars];
+  const int s = threadIdx.x;
+  if (s < kSmallStars) {
+    unsigned key = 0xffffffffu;
+    if (s < n) {
+      if (blockIdx.x == 0) {
+        star_prepare(pos, s, g, cic_fac<float>(masses, s, fac_all, g.vol), q, sidx, sw0, sw1, bkey);
+        key = bkey[s];
+      } else {
+        int i0[3], i1[3];
+        float w0[3], w1[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+          cic_axis<float>(pos[3 * s + d], g.d[d], g.n[d], i0[d], i1[d], w0[d], w1[d]);
+        key = bucket_of(i0[0], i0[1], i0[2], q, g.n);
+      }
+    }
+    keys[s] = key;
+  }
+  __syncthreads();
+  if (blockIdx.x == 0 && s < n) {
+    const unsigned key = keys[s];
+    int rank = 0;
+    for (int j = 0; j < n; ++j) rank += (keys[j] < key || (keys[j] == key && j < s)) ? 1 : 0;
+    perm[rank] = (unsigned)s;
+    skey[rank] = key;
+  }
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b <= n_buckets; b += gridDim.x * blockDim.x) {
+    int c = 0;
+    for (int j = 0; j < n; ++j) c += keys[j] < (unsigned)b ? 1 : 0;
+    bstart[b] = c;
+  }
+}
+
+int launch_stars_small(const void *pos, int n, const void *masses, double m_s, const CicGeomD &g,
+                       int q, int n_buckets, const StarBufs &b, cudaStream_t st) {
+  if (n <= 0 || n > kSmallStars) {
+    set_error("internal: launch_stars_small with %d particles", n);
+    return QJ_ERR_ARG;
+  }
+  const double fac = m_s / (g.d[0] * g.d[1] * g.d[2]);
+  const int T = 256, B = (n_buckets + 1 + T - 1) / T;
+  k_stars_small<<<B, T, 0, st>>>((const float *)pos, n, (const float *)masses, (float)fac,
+                                 cast_geom<float>(g), q, b.sidx, b.sw0, b.sw1, b.bkey, b.perm, b.skey,
+                                 b.bstart, n_buckets);
   QJ_CK_LAUNCH();
   return 0;
 }
