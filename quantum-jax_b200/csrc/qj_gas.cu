@@ -34,6 +34,31 @@ struct Idx3 {
   }
 };
 
+// Coordinates of linear cell index i of an n^3 box; 32-bit divisions (the
+// hydro grids hold fewer than 2^32 cells, checked on the host)
+__device__ __forceinline__ void cell_xyz(long long i, int n, int &x, int &y, int &z) {
+  const unsigned u = (unsigned)i, un = (unsigned)n, q = u / un;
+  z = (int)(u - q * un);
+  x = (int)(q / un);
+  y = (int)(q - (unsigned)x * un);
+}
+
+// Linear index of cell (x, y, z) of an n^3 periodic box and of its six face
+// neighbours: up[d] / dn[d] = the next / previous cell along x, y, z.
+struct Nbr {
+  long long c, up[3], dn[3];
+  __device__ __forceinline__ Nbr(int n, int x, int y, int z) {
+    const long long n1 = n, n2 = n1 * n1;
+    c = ((long long)x * n1 + y) * n1 + z;
+    up[0] = x == n - 1 ? c - (n1 - 1) * n2 : c + n2;
+    dn[0] = x == 0 ? c + (n1 - 1) * n2 : c - n2;
+    up[1] = y == n - 1 ? c - (n1 - 1) * n1 : c + n1;
+    dn[1] = y == 0 ? c + (n1 - 1) * n1 : c - n1;
+    up[2] = z == n - 1 ? c - (n1 - 1) : c + 1;
+    dn[2] = z == 0 ? c + (n1 - 1) : c - 1;
+  }
+};
+
 // a / b in the hydro stencils: correctly rounded in float64 (the path pinned
 // to the reference at 1e-10); the fast divide (within 2 ulp) in float32,
 // whose stencils are bound by their divisions
@@ -64,12 +89,12 @@ __device__ Prim<R> cell_prim(const R *const F[4], const Idx3 &I, int x, int y, i
                              R cs) {
   Prim<R> P;
   R c[4];
-  for (int v = 0; v < 4; ++v) c[v] = F[v][I.at(x, y, z)];
+  const Nbr nb(I.n, x, y, z);
+  for (int v = 0; v < 4; ++v) c[v] = F[v][nb.c];
   for (int v = 0; v < 4; ++v) {
     for (int d = 0; d < 3; ++d) {
-      const int ex = d == 0, ey = d == 1, ez = d == 2;
-      const R fp = F[v][I.at(x + ex, y + ey, z + ez)];
-      const R fm = F[v][I.at(x - ex, y - ey, z - ez)];
+      const R fp = F[v][nb.up[d]];
+      const R fm = F[v][nb.dn[d]];
       R g = hdiv(fp - fm, (R)2 * dx);
       const R denom = adjust_denominator(g);
       g = clamp01(hdiv(hdiv(c[v] - fm, dx), denom)) * g;
@@ -86,9 +111,8 @@ __device__ Prim<R> cell_prim(const R *const F[4], const Idx3 &I, int x, int y, i
     const R Pc = c[0] * c2;
     R gP[3];
     for (int d = 0; d < 3; ++d) {
-      const int ex = d == 0, ey = d == 1, ez = d == 2;
-      const R fp = F[0][I.at(x + ex, y + ey, z + ez)] * c2;
-      const R fm = F[0][I.at(x - ex, y - ey, z - ez)] * c2;
+      const R fp = F[0][nb.up[d]] * c2;
+      const R fm = F[0][nb.dn[d]] * c2;
       R g = hdiv(fp - fm, (R)2 * dx);
       const R denom = adjust_denominator(g);
       g = clamp01(hdiv(hdiv(Pc - fm, dx), denom)) * g;
@@ -183,7 +207,8 @@ __global__ void __launch_bounds__(256)
   const long long ncell = (long long)n * n * n;
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i >= ncell) return;
-  const int z = (int)(i % n), y = (int)((i / n) % n), x = (int)(i / ((long long)n * n));
+  int x, y, z;
+  cell_xyz(i, n, x, y, z);
   const R *const F[4] = {rho, vx, vy, vz};
   const Prim<R> C = cell_prim<R, FACC>(F, Idx3{n}, x, y, z, dx, dt, cs);
   Quad<R> *Q = reinterpret_cast<Quad<R> *>(P);
@@ -215,8 +240,8 @@ __global__ void __launch_bounds__(256)
   const long long ncell = (long long)n * n * n;
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i >= ncell) return;
-  const int z = (int)(i % n), y = (int)((i / n) % n), x = (int)(i / ((long long)n * n));
-  const Idx3 I{n};
+  int x, y, z;
+  cell_xyz(i, n, x, y, z);
   Prim<R> C;
 #pragma unroll
   for (int d = 0; d < 3; ++d) load_face_prim(P, ncell, i, d, C);
@@ -228,12 +253,12 @@ __global__ void __launch_bounds__(256)
   U[3] = rho[i] * vz[i] * vol;
   // apply_fluxes (:212-223): per axis, F += -fac * flux(+face); F += fac * flux(-face)
   R up[3][4], dn[3][4];
+  const Nbr nb(n, x, y, z);
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
-    const int ex = d == 0, ey = d == 1, ez = d == 2;
     Prim<R> Pp, Pm;
-    load_face_prim(P, ncell, I.at(x + ex, y + ey, z + ez), d, Pp);
-    load_face_prim(P, ncell, I.at(x - ex, y - ey, z - ez), d, Pm);
+    load_face_prim(P, ncell, nb.up[d], d, Pp);
+    load_face_prim(P, ncell, nb.dn[d], d, Pm);
     face_flux<R, FACC>(C, Pp, d, dx, cs, up[d]);
     face_flux<R, FACC>(Pm, C, d, dx, cs, dn[d]);
   }
@@ -539,6 +564,10 @@ template <bool FACC>
 static int hydro_impl(bool dbl, void *rho, void *vx, void *vy, void *vz, void *prim, int n,
                       double dx, double dt, double cs, int clamp_rho, cudaStream_t st, int block) {
   const long long ncell = (long long)n * n * n;
+  if (ncell >= (1LL << 32)) {
+    set_error("hydro: %d^3 cells exceed 2^32", n);
+    return QJ_ERR_ARG;
+  }
   const int T = (block == 64 || block == 128 || block == 256) ? block : 256;
   const int B = (int)((ncell + T - 1) / T);
   const double vol = dx * dx * dx, fac = dt * dx * dx;
