@@ -246,26 +246,38 @@ def gas_bh_leg(a, dev, stream, barrier):
 
 
 def cpu_baseline(n, n_s, steps=2):
-    """The float64 NumPy oracle on the host cores (scipy.fft workers = all)."""
+    """The oracle's stars step on the host cores (scipy.fft workers = all).
+
+    The baseline value is the complex64 / float32 restatement, the
+    reference's own precision (x64 off); the float64 restatement is timed on
+    the same sample and reported beside it."""
     import numpy as np
 
     from oracle import oracle as O
 
     O.WORKERS = os.cpu_count() or 1
     psi, pos, vel, g, p, dt = make_ic(n, n_s)
-    k = O.kgrid(g)
-    state = (psi, pos, vel, 0.0, 0.0, dt)
-    state = O.stars_compute_step(*state, g, p, dt, k)  # warm-up
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        state = O.stars_compute_step(*state, g, p, dt, k)
-    el = time.perf_counter() - t0
-    assert np.isfinite(state[0]).all()
-    return {"value": g.ncell * steps / el, "unit": UNIT, "cores": O.WORKERS, "kind": "port",
+
+    def timed(step, state, k):
+        state = step(*state, g, p, dt, k)  # warm-up
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            state = step(*state, g, p, dt, k)
+        el = time.perf_counter() - t0
+        assert np.isfinite(state[0]).all()
+        return el / steps
+
+    s32 = timed(O.stars_compute_step_f32, (psi.astype(np.complex64), pos.astype(np.float32),
+                                           vel.astype(np.float32), 0.0, 0.0, dt), O.kgrid_f32(g))
+    s64 = timed(O.stars_compute_step, (psi, pos, vel, 0.0, 0.0, dt), O.kgrid(g))
+    return {"value": g.ncell / s32, "unit": UNIT, "cores": O.WORKERS, "kind": "port",
             "sample": f"{steps} timed steps (after 1 warm-up) of the {n}^3, {n_s}-star "
-                      f"workload; float64 NumPy/SciPy restatement of quantum-stars.py:295-330 "
-                      f"(reference JAX is not installable)",
-            "s_per_step": el / steps}
+                      f"workload; complex64/float32 NumPy/SciPy restatement of "
+                      f"quantum-stars.py:295-330, the reference's own precision (x64 off); "
+                      f"reference JAX is not installable",
+            "s_per_step": s32,
+            "float64": {"value": g.ncell / s64, "s_per_step": s64,
+                        "sample": "the float64 restatement (the oracle), same steps"}}
 
 
 def run_reference(a, rank):
@@ -276,10 +288,12 @@ def run_reference(a, rank):
     line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT,
             "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": cb["s_per_step"] * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None, "dtype": "c64/f32 (x64 off, as the reference)",
+            "data": "synthetic",
             "config": {"workload": f"stars KDK {a.n}^3 complex, {a.stars} stars",
                        "grid": [a.n] * 3, "n_stars": a.stars, "l2_flush": "inputs > L2"},
-            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample",
+                                                "float64")},
             "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)

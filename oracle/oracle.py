@@ -897,6 +897,70 @@ def bin_stars_f32(pos32, g: Grid, m_s):
     return rho
 
 
+def bin_stars_f32_vec(pos32, g: Grid, m_s):
+    """``bin_stars_f32`` vectorised, bit for bit: the same float32 products,
+    added by ``np.add.at`` (unbuffered, in index order) in star-major,
+    corner-minor order -- the sequential order of quantum-stars.py:220-246."""
+    ii, ip, w_i, w_ip1 = cic_weights_f32(pos32, g)
+    fac = np.float32(m_s / (g.dx * g.dy * g.dz))
+    idx = (ii, ip)
+    w = (w_i, w_ip1)
+    vals = np.stack([((w[c[0]][:, 0] * w[c[1]][:, 1]) * w[c[2]][:, 2]) * fac for c in CORNERS],
+                    axis=1)
+    cells = np.stack([np.ravel_multi_index((idx[c[0]][:, 0], idx[c[1]][:, 1], idx[c[2]][:, 2]),
+                                           g.shape) for c in CORNERS], axis=1)
+    rho = np.zeros(g.ncell, dtype=np.float32)
+    np.add.at(rho, cells.ravel(), vals.ravel())
+    return rho.reshape(g.shape)
+
+
+def kgrid_f32(g: Grid):
+    """R1 in float32, as the x64-off reference builds it (quantum-stars.py:142-149)."""
+    return tuple(a.astype(np.float32) for a in kgrid(g))
+
+
+def stars_compute_step_f32(psi, pos, vel, t, a_max, dt_s, g: Grid, p: Phys, dt, k32):
+    """quantum-stars.py:295-330 in the reference's own precision: complex64
+    psi, float32 fields and particles (x64 is off, quantum-stars.py:70).
+
+    The CPU baseline's timed step.  The deposit and the gather are vectorised
+    (the deposit bit for bit as ``bin_stars_f32``); the kinetic factor is
+    evaluated every step, as the reference does (:307-309)."""
+    f = np.float32
+    kx, ky, kz, k_sq = k32
+    L = np.array([g.Lx, g.Ly, g.Lz], dtype=np.float32)
+    four_pi_G = f(4.0 * np.pi * p.G)
+    div = k_sq + (k_sq == 0)
+
+    def potential_and_accel(psi, pos):
+        rho = np.abs(psi) ** 2 + bin_stars_f32_vec(pos, g, p.m_s)
+        V_hat = -_fftn(four_pi_G * (rho - f(p.rho_bar)), WORKERS) / div
+        V = np.real(_ifftn(V_hat, WORKERS))
+        a_grid = np.stack([-np.real(_ifftn(1j * kd * V_hat, WORKERS)) for kd in (kx, ky, kz)],
+                          axis=-1)
+        ii, ip, w_i, w_ip1 = cic_weights_f32(pos, g)
+        idx = (ii, ip)
+        w = (w_i, w_ip1)
+        acc = np.zeros((pos.shape[0], 3), dtype=np.float32)
+        for c in CORNERS:
+            acc += ((w[c[0]][:, 0] * w[c[1]][:, 1]) * w[c[2]][:, 2])[:, None] * a_grid[
+                idx[c[0]][:, 0], idx[c[1]][:, 1], idx[c[2]][:, 2]]
+        return V, acc, np.max(np.abs(a_grid))
+
+    V, acc, a1 = potential_and_accel(psi, pos)
+    psi = np.exp(-1j * f(p.m_per_hbar * dt / 2.0) * V) * psi
+    vel = vel + acc * f(dt / 2.0)
+    psi = _ifftn(np.exp(f(dt) * (-1j * k_sq / f(p.m_per_hbar) / f(2.0))) * _fftn(psi, WORKERS),
+                 WORKERS)
+    pos = np.mod(pos + vel * f(dt), L)
+    V, acc, a2 = potential_and_accel(psi, pos)
+    psi = np.exp(-1j * f(p.m_per_hbar * dt / 2.0) * V) * psi
+    vel = vel + acc * f(dt / 2.0)
+    with np.errstate(divide="ignore"):
+        dt_s = np.min(np.abs(f(g.dx) / vel)) if vel.size else np.inf
+    return psi, pos, vel, t + dt, max(a_max, a1, a2), dt_s
+
+
 # ---------------------------------------------------------------------------
 # Seeded initial conditions (the benchmark IC family)
 # ---------------------------------------------------------------------------
