@@ -1,7 +1,9 @@
 """CPU oracle for the quantum-jax kick-drift-kick Schroedinger-Poisson step.
 
 TEST INFRASTRUCTURE ONLY.  This module is the float64 NumPy/SciPy restatement
-of the reference's step functions, op for op, used as the correctness checker.
+of the reference's step functions, op for op, used as the correctness checker,
+plus the stars step in the reference's own complex64 / float32 precision
+(``stars_compute_step_f32``), the CPU baseline's timed step.
 Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg
 may import it; the product path (``qj``) never does and has no CPU fallback.
 
