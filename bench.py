@@ -639,7 +639,7 @@ def main():
     cb = None
     if rank == 0 and world == 1 and not a.no_cpu:
         cb = cpu_baseline(n, n_s, 2)
-        cb = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        cb = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample", "float64")}
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
