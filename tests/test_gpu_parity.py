@@ -181,6 +181,23 @@ def test_kdk_fused_f32(name, n, shape, L, n_s):
     assert got[3][2] == pytest.approx(ref[3][2], rel=1e-4)
 
 
+def test_fused_f32_64cube_400_stars_100_steps():
+    """The small stars configuration at its own size: 64^3, 400 stars at rest,
+    seed 0, 100 steps of dt = dx^2/6; fused float32 against the float64 oracle."""
+    qj = qj_mod()
+    psi, pos, vel, g, p = O.stars_ic(64, 400, seed=0)
+    dt = O.default_dt(g, p)
+    got = run_qj(g, p, psi, pos, vel, dt, 100, qj.FUSED_F32)
+    ref = oracle_run(g, p, psi, pos, vel, dt, 100)
+    assert O.rel_l2(got[0], ref[0]) < 1e-5
+    assert O.rel_l2(np.abs(got[0]) ** 2, np.abs(ref[0]) ** 2) < 1e-5
+    assert O.rel_l2(got[1], ref[1]) < 1e-5
+    assert O.rel_l2(got[2], ref[2]) < 1e-3
+    m0 = np.sum(np.abs(psi) ** 2)
+    assert abs(np.sum(np.abs(got[0].astype(np.complex128)) ** 2) / m0 - 1.0) < 1e-6
+    assert got[3][1] == pytest.approx(ref[3][1], rel=1e-4)
+
+
 def test_fused_deterministic_and_chunking():
     qj = qj_mod()
     psi, pos, vel, g, p = O.stars_ic(32, 200, seed=4)
