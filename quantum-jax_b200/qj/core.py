@@ -74,6 +74,43 @@ def _ptr(t):
     return ctypes.c_void_p(t.data_ptr()) if t is not None else None
 
 
+def read_tuning_cache(path):
+    """The autotuner's cache as a dict; a missing or unreadable file (e.g.
+    one cut short by a crash) reads as empty, so tuning is redone."""
+    import json
+    import os
+
+    if not os.path.exists(path):
+        return {}
+    try:
+        with open(path) as f:
+            cache = json.load(f)
+    except (OSError, ValueError):
+        return {}
+    return cache if isinstance(cache, dict) else {}
+
+
+def write_tuning_cache(path, cache):
+    """Replace the cache file atomically (write a temporary file in the same
+    folder, then rename): processes tuning at the same time never leave a
+    half-written file; the last writer's entries win."""
+    import json
+    import os
+    import tempfile
+
+    folder = os.path.dirname(os.path.abspath(path))
+    os.makedirs(folder, exist_ok=True)
+    fd, tmp = tempfile.mkstemp(prefix=".tuning.", suffix=".json", dir=folder)
+    try:
+        with os.fdopen(fd, "w") as f:
+            json.dump(cache, f, indent=1)
+        os.replace(tmp, path)
+    except BaseException:
+        if os.path.exists(tmp):
+            os.unlink(tmp)
+        raise
+
+
 class Plan:
     """A libqj plan: grid, constants, tables and device workspace.
 
@@ -139,7 +176,6 @@ class Plan:
         ~/.cache/qj/tuning.json) keyed by device, grid, boxes, stars and
         precision; a cached entry is applied without timing.  Returns the
         tuning list."""
-        import json
         import os
 
         n_s = 0 if pos is None else int(pos.shape[-2])
@@ -148,10 +184,7 @@ class Plan:
             self.nbox, n_s, self.precision))
         path = cache_file or os.environ.get(
             "QJ_TUNING_CACHE", os.path.join(os.path.expanduser("~"), ".cache", "qj", "tuning.json"))
-        cache = {}
-        if os.path.exists(path):
-            with open(path) as f:
-                cache = json.load(f)
+        cache = read_tuning_cache(path)
         if key in cache:
             self.tuning = cache[key]
             return self.tuning
@@ -168,11 +201,11 @@ class Plan:
         check(lib().qj_autotune_kdk(self._h, _ptr(psi), _ptr(pos) if n_s else None,
                                     _ptr(vel) if n_s else None, n_s, float(m_s), float(dt),
                                     int(probe_steps), _stream()))
-        cache[key] = self.tuning
-        os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
-        with open(path, "w") as f:
-            json.dump(cache, f, indent=1)
-        return cache[key]
+        tuning = self.tuning
+        cache = read_tuning_cache(path)  # entries other processes added meanwhile
+        cache[key] = tuning
+        write_tuning_cache(path, cache)
+        return tuning
 
     def status(self):
         """Wait for the device; raise if a fused pass of this plan gave up a
