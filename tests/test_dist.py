@@ -1,11 +1,14 @@
 """Multi-process host logic on CPU (gloo, world size 2): the max-over-ranks
-timing, the box partition every rank computes identically, and the
-reference arm's rank-0-only output."""
+timing, the box partition every rank computes identically, the
+reference arm's rank-0-only output, and a rank that leaves: the other rank's
+next collective ends with an error within the short process-group timeout
+instead of waiting for good."""
 
 import os
 import socket
 import subprocess
 import sys
+import time
 
 import pytest
 import torch.multiprocessing as mp
@@ -71,3 +74,40 @@ def test_reference_arm_prints_only_on_rank_zero():
                         "--gpus", "2", "--steps", "1", "--warmup", "0"],
                        capture_output=True, text=True, env=env, timeout=120)
     assert r.returncode == 0 and r.stdout.strip() == ""
+
+
+def _leaving_worker(rank, world, port, out):
+    os.environ.update(RANK=str(rank), WORLD_SIZE=str(world), LOCAL_RANK=str(rank),
+                      MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    sys.path.insert(0, os.path.join(ROOT, "quantum-jax_b200"))
+    from qj import dist as qd
+
+    d = qd.init("gloo", timeout_s=5)
+    if rank == 1:
+        os._exit(3)  # leaves between steps, before the timing collective
+    t0 = time.time()
+    try:
+        qd.max_over_ranks(1.0, d)
+        res = "returned"
+    except Exception as e:  # the error a surviving rank sees
+        res = type(e).__name__
+    out.put((rank, res, time.time() - t0))
+    out.close()
+    out.join_thread()
+    os._exit(0)
+
+
+@pytest.mark.timeout(120)
+def test_rank_that_leaves_ends_the_others_collective_with_an_error():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = free_port()
+    procs = [ctx.Process(target=_leaving_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    rank, res, waited = q.get(timeout=100)
+    for p in procs:
+        p.join(30)
+    assert rank == 0 and res != "returned"
+    assert waited < 60
+    assert [p.exitcode for p in procs] == [0, 3]
