@@ -10,8 +10,6 @@ with libqj's checkpointed adjoint (ckpt every K steps, recompute in between).
 
 from __future__ import annotations
 
-import ctypes
-
 import torch
 
 from ._lib import check, lib
