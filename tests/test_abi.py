@@ -1,4 +1,5 @@
-"""The C ABI library loads without a GPU and exports every declared symbol."""
+"""The C ABI library loads without a GPU, exports every declared symbol, and
+turns bad arguments into status codes before any CUDA call."""
 
 import os
 import re
@@ -41,3 +42,43 @@ def test_error_path_without_gpu_is_a_status_not_a_crash():
     ph = qj._lib.QjPhys(1.0, 1.0, 1.0, 0.0, 1.0, 1.0)
     assert lib.qj_plan_create(ctypes.byref(h), ctypes.byref(g), ctypes.byref(ph), 1, 8) == 1
     assert b"unsupported" in lib.qj_last_error()
+
+
+# Entry points whose zero / null call is defined to succeed: destroying
+# nothing, the error text, the launch counter, the profiler switches, and the
+# workspace size of no plan (0).
+_OK_ON_NULL = {"qj_plan_destroy", "qj_ensemble_destroy", "qj_last_error", "qj_launch_count",
+               "qj_profile_enable", "qj_profile_read", "qj_plan_workspace_bytes"}
+
+
+def _zero_args(argtypes):
+    import ctypes
+
+    vals = []
+    for a in argtypes:
+        if a in (ctypes.c_int, ctypes.c_int32, ctypes.c_int64, ctypes.c_uint64, ctypes.c_size_t):
+            vals.append(0)
+        elif a in (ctypes.c_double, ctypes.c_float):
+            vals.append(0.0)
+        else:
+            vals.append(None)
+    return vals
+
+
+def test_every_entry_point_rejects_null_arguments_without_a_gpu():
+    """Null plans, tensors and sizes come back as QJ_ERR_ARG with a message,
+    checked before any CUDA call (no exception, no exit, no crash across the
+    ABI)."""
+    import qj
+
+    lib = qj.lib()
+    for name, (_, argtypes) in sorted(qj._lib.SIGNATURES.items()):
+        if name in _OK_ON_NULL:
+            continue
+        rc = getattr(lib, name)(*_zero_args(argtypes))
+        assert rc == qj._lib.QJ_ERR_ARG, name
+        assert lib.qj_last_error(), name
+    n = qj._lib.QJ_TUNE_N
+    assert lib.qj_plan_get_tuning(None, None, n) == qj._lib.QJ_ERR_ARG
+    assert lib.qj_plan_set_tuning(None, None, n) == qj._lib.QJ_ERR_ARG
+    assert lib.qj_plan_destroy(None) == 0
