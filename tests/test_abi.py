@@ -4,6 +4,8 @@ turns bad arguments into status codes before any CUDA call."""
 import os
 import re
 
+import pytest
+
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
@@ -82,3 +84,43 @@ def test_every_entry_point_rejects_null_arguments_without_a_gpu():
     assert lib.qj_plan_get_tuning(None, None, n) == qj._lib.QJ_ERR_ARG
     assert lib.qj_plan_set_tuning(None, None, n) == qj._lib.QJ_ERR_ARG
     assert lib.qj_plan_destroy(None) == 0
+
+
+@pytest.mark.parametrize("dims,prec,max_particles,nbox,text", [
+    ((32, 32, 24), 1, 8, 1, "length 24 unsupported"),
+    ((17, 32, 32), 1, 8, 1, "length 17 unsupported"),
+    ((32, 32, 32), 7, 8, 1, "precision must be"),
+    ((32, 32, 32), 1, -1, 1, "max_particles must be"),
+    ((32, 32, 32), 0, 8, 2, "batches need QJ_FUSED_F32"),
+    ((32, 32, 32), 1, 8, 0, "nbox must be"),
+])
+def test_plan_create_rejects_bad_configurations(dims, prec, max_particles, nbox, text):
+    import ctypes
+
+    import qj
+
+    lib = qj.lib()
+    h = ctypes.c_void_p()
+    g = qj._lib.QjGrid(*dims, 1.0, 1.0, 1.0)
+    ph = qj._lib.QjPhys(1.0, 1.0, 1.0, 0.0, 1.0, 1.0)
+    rc = lib.qj_plan_create_batched(ctypes.byref(h), ctypes.byref(g), ctypes.byref(ph), prec,
+                                    max_particles, nbox)
+    assert rc == qj._lib.QJ_ERR_ARG and h.value is None
+    assert text.encode() in lib.qj_last_error()
+
+
+def test_valid_plan_without_a_device_is_a_cuda_status():
+    import ctypes
+
+    import qj
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a device is present")
+    lib = qj.lib()
+    h = ctypes.c_void_p()
+    g = qj._lib.QjGrid(32, 32, 32, 1.0, 1.0, 1.0)
+    ph = qj._lib.QjPhys(1.0, 1.0, 1.0, 0.0, 1.0, 1.0)
+    rc = lib.qj_plan_create(ctypes.byref(h), ctypes.byref(g), ctypes.byref(ph), 1, 8)
+    assert rc == qj._lib.QJ_ERR_CUDA and h.value is None
+    assert b"CUDA error" in lib.qj_last_error()
