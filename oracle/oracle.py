@@ -175,19 +175,22 @@ def bin_stars(pos, g: Grid, masses):
     """quantum-stars.py:212-247 / quantum-gas-bh.py:414-449.
 
     ``masses`` is the per-particle mass (m_s for every star, m_bh[s] for black
-    holes).  Deposits in star order, corners in the fixed order."""
-    rho = np.zeros(g.shape)
+    holes).  Deposits in star order, corners in the fixed order: the products
+    w_x w_y w_z fac are formed left to right and added by ``np.add.at``
+    (unbuffered, in index order) star-major, corner-minor, so each cell sums
+    its contributions in the reference's sequential order."""
     i, ip1, w_i, w_ip1 = get_cic_indices_and_weights(pos, g)
     vol = g.dx * g.dy * g.dz
     idx = (i, ip1)
     w = (w_i, w_ip1)
-    for s in range(pos.shape[0]):
-        fac = masses[s] / vol
-        for c in CORNERS:
-            rho[idx[c[0]][s, 0], idx[c[1]][s, 1], idx[c[2]][s, 2]] += (
-                w[c[0]][s, 0] * w[c[1]][s, 1] * w[c[2]][s, 2] * fac
-            )
-    return rho
+    fac = np.asarray(masses, dtype=np.float64) / vol
+    vals = np.stack([w[c[0]][:, 0] * w[c[1]][:, 1] * w[c[2]][:, 2] * fac for c in CORNERS],
+                    axis=1)
+    cells = np.stack([np.ravel_multi_index((idx[c[0]][:, 0], idx[c[1]][:, 1], idx[c[2]][:, 2]),
+                                           g.shape) for c in CORNERS], axis=1)
+    rho = np.zeros(g.ncell)
+    np.add.at(rho, cells.ravel(), vals.ravel())
+    return rho.reshape(g.shape)
 
 
 def grid_accelerations(rho, g: Grid, p: Phys, k=None):

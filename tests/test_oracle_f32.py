@@ -1,7 +1,8 @@
-"""The oracle's complex64 / float32 stars step (the CPU baseline's timed step,
-in the reference's own precision): its vectorised deposit is bit-identical to
-the sequential float32 deposit, it keeps complex64 / float32 throughout, and
-it follows the float64 restatement to float32 rounding."""
+"""The oracle's vectorised deposits and its complex64 / float32 stars step
+(the CPU baseline's timed step, in the reference's own precision): both
+deposits are bit-identical to the sequential star-by-star loop, the float32
+step keeps complex64 / float32 throughout, and it follows the float64
+restatement to float32 rounding."""
 
 import numpy as np
 
@@ -35,3 +36,26 @@ def test_f32_step_follows_the_f64_restatement():
     assert O.rel_l2(s32[1], s64[1]) < 1e-5
     assert O.rel_l2(s32[2], s64[2]) < 1e-4
     assert abs(s32[4] - s64[4]) < 1e-5 * s64[4]
+
+
+def _bin_stars_loop(pos, g, masses):
+    """The sequential deposit written as the reference's loop (star by star,
+    corners in the fixed order), kept here to pin the vectorised oracle."""
+    rho = np.zeros(g.shape)
+    i, ip1, w_i, w_ip1 = O.get_cic_indices_and_weights(pos, g)
+    vol = g.dx * g.dy * g.dz
+    idx, w = (i, ip1), (w_i, w_ip1)
+    for s in range(pos.shape[0]):
+        fac = masses[s] / vol
+        for c in O.CORNERS:
+            rho[idx[c[0]][s, 0], idx[c[1]][s, 1], idx[c[2]][s, 2]] += (
+                w[c[0]][s, 0] * w[c[1]][s, 1] * w[c[2]][s, 2] * fac)
+    return rho
+
+
+def test_vectorised_f64_deposit_is_bit_identical_to_the_loop():
+    psi, pos, vel, g, p = O.stars_ic(16, 300, seed=8)
+    pos[:10] = 0.5  # a clump: repeated cells
+    pos[10:14, 1] = 1.0  # on the upper face (wraps to cell 0)
+    masses = np.random.default_rng(2).uniform(0.5, 2.0, len(pos))
+    assert np.array_equal(O.bin_stars(pos, g, masses), _bin_stars_loop(pos, g, masses))
