@@ -12,8 +12,8 @@ larger than L2 (126 MB), so no explicit flush is needed between steps.
 
 Printed (one JSON line on rank 0): value = fused float32 cell-steps/s over all
 ranks (device time, CUDA events, max over ranks); the plain float64 GPU path's
-rate; psi / rho rel-L2 of the fused path against the float64 path after the
-same steps; e2e through the public API with host buffers; the roofline of the
+rate; psi / rho rel-L2 of the fused path against the float64 path after
+1000 steps (--err-steps, outside the timed region); e2e through the public API with host buffers; the roofline of the
 dominant pass; the CPU baseline (the float64 NumPy oracle on the host cores);
 SM clocks sampled during the timed region.
 
@@ -58,8 +58,12 @@ def parse():
     ap.add_argument("--impl", default="qj", choices=["qj", "reference"])
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--stars", type=int, default=4096)
-    ap.add_argument("--err-steps", type=int, default=None,
-                    help="steps of the fused-vs-float64 error check (default: --steps)")
+    ap.add_argument("--err-steps", type=int, default=1000,
+                    help="steps of the fused-vs-float64 error check, run outside the timed "
+                         "region (1000: the accuracy target's run length)")
+    ap.add_argument("--ref-budget-s", type=float, default=150.0,
+                    help="reference arm: most seconds of timed CPU steps (fewer steps are "
+                         "timed, and reported as such, when --steps would take longer)")
     ap.add_argument("--plain-steps", type=int, default=10)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -280,21 +284,59 @@ def cpu_baseline(n, n_s, steps=2):
                         "sample": "the float64 restatement (the oracle), same steps"}}
 
 
-def run_reference(a, rank):
+def bench_config(n, n_s, dt, world):
+    """The `config` of both arms' JSON lines (the same workload)."""
+    return {"workload": f"stars KDK {n}^3 complex64, {n_s} stars, one box per GPU (replicas)",
+            "grid": [n, n, n], "n_stars": n_s, "dt": dt,
+            "l2_flush": (f"inputs larger than L2 (psi {n ** 3 * 8 >> 20} MiB)" if n ** 3 * 8 > 126e6
+                         else f"none: psi ({n ** 3 * 8 >> 20} MiB) fits in L2"),
+            "parallelism": f"replicas x{world}"}
+
+
+def run_reference(a, rank, world):
+    """The reference arm: the complex64 / float32 restatement of the stars step
+    (quantum-stars.py:295-330) on the host cores, rank 0 only.  It runs
+    --warmup untimed steps, then times --steps steps of the same 256^3
+    workload; when --steps would take longer than --ref-budget-s (estimated
+    from the warm-up), it times as many as fit and reports that number in
+    `steps` (with `steps_requested`)."""
     if rank != 0:
         return
-    steps = max(1, min(a.steps, 3))
-    cb = cpu_baseline(a.n, a.stars, steps)
-    line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT,
-            "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
-            "ms_per_step": cb["s_per_step"] * 1e3, "higher_is_better": True,
+    import numpy as np
+
+    from oracle import oracle as O
+
+    O.WORKERS = os.cpu_count() or 1
+    psi, pos, vel, g, p, dt = make_ic(a.n, a.stars)
+    k = O.kgrid_f32(g)
+    state = (psi.astype(np.complex64), pos.astype(np.float32), vel.astype(np.float32), 0.0, 0.0, dt)
+    t0 = time.perf_counter()
+    state = O.stars_compute_step_f32(*state, g, p, dt, k)
+    t_step = time.perf_counter() - t0
+    warm = 1
+    while warm < a.warmup and (warm + 1) * t_step < 60.0:
+        state = O.stars_compute_step_f32(*state, g, p, dt, k)
+        warm += 1
+    steps = max(1, min(a.steps, int(a.ref_budget_s / max(t_step, 1e-9))))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        state = O.stars_compute_step_f32(*state, g, p, dt, k)
+    el = time.perf_counter() - t0
+    assert np.isfinite(state[0]).all()
+    value = g.ncell * steps / el
+    sample = (f"{steps} timed steps (after {warm} warm-up) of the {a.n}^3, {a.stars}-star "
+              f"workload; complex64/float32 NumPy/SciPy restatement of "
+              f"quantum-stars.py:295-330, the reference's own precision (x64 off); reference "
+              f"JAX is not installable")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+            "n_gpus": world, "steps": steps, "steps_requested": a.steps, "warmup": warm,
+            "ms_per_step": el / steps * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "c64/f32 (x64 off, as the reference)",
-            "data": "synthetic",
-            "config": {"workload": f"stars KDK {a.n}^3 complex, {a.stars} stars",
-                       "grid": [a.n] * 3, "n_stars": a.stars, "l2_flush": "inputs > L2"},
-            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample",
-                                                "float64")},
-            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+            "data": "synthetic (seeded Gaussian random field, uniform stars)",
+            "config": bench_config(a.n, a.stars, dt, world),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": O.WORKERS, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -305,7 +347,7 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if a.impl == "reference":
-        run_reference(a, rank)
+        run_reference(a, rank, world)
         return
 
     import numpy as np
@@ -412,7 +454,7 @@ def main():
     plain_value = world * C * a.plain_steps / (pl_ms * 1e-3)
 
     # ---------------- accuracy: fused vs float64 after the same steps --------
-    err_steps = a.err_steps if a.err_steps is not None else a.steps
+    err_steps = a.err_steps
     ps, po, ve, diag = fresh(qj.FUSED_F32)
     qs, qo, qv, qd = fresh(qj.PLAIN_F64)
     mass0 = float((qs.abs() ** 2).sum())
@@ -638,7 +680,7 @@ def main():
 
     cb = None
     if rank == 0 and world == 1 and not a.no_cpu:
-        cb = cpu_baseline(n, n_s, 2)
+        cb = cpu_baseline(n, n_s, 5)
         cb = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample", "float64")}
 
     if rank == 0:
@@ -647,10 +689,7 @@ def main():
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "c64/f32 (phases, k=0 mode, mean density in f64)",
                 "data": "synthetic (seeded Gaussian random field, uniform stars)",
-                "config": {"workload": f"stars KDK {n}^3 complex64, {n_s} stars, one box per "
-                                       f"GPU (replicas)", "grid": [n, n, n], "n_stars": n_s,
-                           "dt": dt, "l2_flush": "inputs larger than L2 (psi 128 MiB)",
-                           "parallelism": f"replicas x{world}"},
+                "config": bench_config(n, n_s, dt, world),
                 "plain_f64": {"value": plain_value, "ms_per_step": pl_ms / a.plain_steps,
                               "steps": a.plain_steps},
                 "fused_over_plain": value / plain_value,

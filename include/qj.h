@@ -25,6 +25,7 @@
 #ifndef QJ_H
 #define QJ_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -178,9 +179,10 @@ int qj_fft3d(qj_plan *plan, const void *in, void *out, int direction,
  * rho, V: float32 device arrays [nx][ny][nz]; each axis 16, 32 or 64 cells
  * (at most QJ_NOALLOC_MAX_CELLS), nz a multiple of 16; other sizes return
  * QJ_ERR_ARG.  Its scratch is a fixed 2 MiB array held by every GPU that
- * loads libqj until the process exits; the first call on a device looks up
- * that array's device address, so make that first call before any stream
- * capture.  All calls on a device share the array: calls that overlap on the
+ * loads libqj until the process exits; the first call on a device (and the
+ * first after a cudaDeviceReset, which frees the array) looks up that array's
+ * device address, so make that first call before any stream capture.  All
+ * calls on a device share the array: calls that overlap on the
  * GPU (unordered streams) race; calls on one stream are safe. */
 #define QJ_NOALLOC_MAX_AXIS 64
 #define QJ_NOALLOC_MAX_CELLS (64 * 64 * 64)
@@ -284,6 +286,64 @@ int qj_plan_status(qj_plan *plan);
  * up it sets the plan's error word, so the next qj_plan_status returns
  * QJ_ERR_TIMEOUT (and clears it).  No reference counterpart. */
 int qj_plan_selftest_wait(qj_plan *plan, int64_t limit_ns, void *stream);
+
+/* ---- XLA custom-call targets (the JAX binding) ----
+ * Inside a jitted JAX program the reference's step (the `update` body that
+ * jax.lax.fori_loop runs, quantum-stars.py:333-351, :454) and get_potential
+ * (:189-193) become XLA custom calls to these targets.  They use XLA's GPU
+ * custom-call convention, status-returning form (custom_call api_version 2;
+ * jax.ffi.register_ffi_target(name, capsule, platform="CUDA",
+ * api_version=0)): buffers = operands' device pointers, then the results';
+ * opaque = the call's backend_config, one of the packed descriptors below.
+ *
+ * qj_xla_kdk_step_f32: operands psi complex64 [nx][ny][nz], pos float32
+ *   [n_s][3], vel float32 [n_s][3], diag float64 [3] (t, a_max, dt_s), then
+ *   v_ext float32 [nx][ny][nz] if has_v_ext; results psi, pos, vel, diag
+ *   after nsteps steps (qj_kdk_step on a cached QJ_FUSED_F32 plan).  Results
+ *   may alias their operands; unaliased operands are copied first.
+ * qj_xla_get_potential_f32: operand rho float32 [nx][ny][nz], result V.
+ *   Grids of 16 / 32 / 64 cells per axis run allocation-free
+ *   (qj_get_potential_f32_noalloc); larger ones on a cached plan.
+ * Plans are created on a configuration's first call on a device (outside
+ * stream capture) and kept until qj_xla_release_plans().  A failing call
+ * reports through the status function set by qj_xla_set_status_fn (the
+ * binding passes jaxlib's XlaCustomCallStatusSetFailure; libqj does not link
+ * jaxlib) when status is non-null, and always to qj_xla_last_status() (the
+ * QJ_* code of the last target call) and qj_last_error(). */
+#define QJ_XLA_DESC_VERSION 1
+typedef struct qj_xla_kdk_desc {
+  int32_t version; /* QJ_XLA_DESC_VERSION */
+  int32_t nsteps;
+  int32_t n_s;
+  int32_t self_interaction;
+  int32_t has_v_ext;
+  int32_t reserved;
+  qj_grid grid;
+  qj_phys phys;
+  double m_s;
+  double dt;
+} qj_xla_kdk_desc;
+typedef struct qj_xla_poisson_desc {
+  int32_t version; /* QJ_XLA_DESC_VERSION */
+  int32_t self_interaction;
+  qj_grid grid;
+  qj_phys phys;
+} qj_xla_poisson_desc;
+typedef void (*qj_xla_status_fn)(void *status, const char *message, size_t message_len);
+void qj_xla_kdk_step_f32(void *stream, void **buffers, const char *opaque, size_t opaque_len,
+                         void *status);
+void qj_xla_get_potential_f32(void *stream, void **buffers, const char *opaque,
+                              size_t opaque_len, void *status);
+void qj_xla_set_status_fn(qj_xla_status_fn fn);
+int qj_xla_last_status(void);
+int qj_xla_release_plans(void);
+
+/* qj_selftest_sincos: sin_cos[2 i], sin_cos[2 i + 1] = sin and cos of
+ * theta[i] (device float64 in, device float32 pairs out) by the kick pass's
+ * own routine (float64 quadrant reduction, float32 series), so that its
+ * accuracy can be tested directly.  No reference counterpart (the reference
+ * takes exp(-1j V dt / 2) of a complex64 array, quantum-stars.py:300). */
+int qj_selftest_sincos(const double *theta, float *sin_cos, int n, void *stream);
 
 /* Instrumentation (no reference counterpart; used by the benchmark).
  * qj_launch_count: kernels libqj has launched in this process.

@@ -1402,6 +1402,16 @@ int qj_plan_selftest_wait(qj_plan *P, int64_t limit_ns, void *stream) {
   return launch_selftest_wait(P->err, (long long)limit_ns, (cudaStream_t)stream);
 }
 
+int qj_selftest_sincos(const double *theta, float *sin_cos, int n, void *stream) {
+  if (n < 0 || !theta || !sin_cos) {
+    set_error("qj_selftest_sincos: bad argument (n >= 0, theta and sin_cos non-null)");
+    return QJ_ERR_ARG;
+  }
+  if (n == 0) return QJ_OK;
+  return launch_selftest_sincos(theta, reinterpret_cast<float2 *>(sin_cos), n,
+                                (cudaStream_t)stream);
+}
+
 int64_t qj_launch_count(void) { return (int64_t)g_launches.load(); }
 
 int qj_profile_enable(int on) {

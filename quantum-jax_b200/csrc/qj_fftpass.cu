@@ -10,13 +10,14 @@ template <typename R, int N, bool CONTIG, int DIR>
 static int run_fft(const FftArgs &a, cudaStream_t st) {
   using SH = PassShape<N, CONTIG>;
   const size_t smem = SH::template smem_bytes<cplx<R>>();
-  static std::once_flag once;
-  static cudaError_t attr_err = cudaSuccess;
-  std::call_once(once, [&] {
-    attr_err = cudaFuncSetAttribute(k_fft<R, N, CONTIG, DIR>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  });
-  QJ_CK(attr_err);
+  // the attribute belongs to the current device's context: set once per device
+  static PerDevice<cudaError_t> attr;
+  const cudaError_t *attr_err = nullptr;
+  QJ_CK(per_device(attr, attr_err, [&](cudaError_t &r) {
+    r = cudaFuncSetAttribute(k_fft<R, N, CONTIG, DIR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
+  }));
+  QJ_CK(*attr_err);
   const int grid = CONTIG ? (a.nx * a.ny) / SH::TP : (a.axis == 0 ? a.ny : a.nx) * (a.nz / 16);
   k_fft<R, N, CONTIG, DIR><<<grid, SH::THREADS, smem, st>>>(a);
   QJ_CK_LAUNCH();

@@ -132,29 +132,34 @@ static int strided_maps(const FusedArgs &a, TileMaps &maps) {
   return 0;
 }
 
-// Resident CTAs per SM of a pass (occupancy) and the SM count, queried once.
+// Resident CTAs per SM of a pass (occupancy) and the SM count, queried once
+// per device (the shared-memory attribute belongs to that device's context).
+struct Occupancy {
+  cudaError_t err = cudaSuccess;
+  int per_sm = 1, sms = 1;
+};
 template <int N, bool CONTIG, int MODE>
 static cudaError_t fused_occupancy(int &per_sm, int &sms) {
   using SH = PassShape<N, CONTIG>;
-  static std::once_flag once;
-  static cudaError_t err = cudaSuccess;
-  static int c_per_sm = 1, c_sms = 1;
-  std::call_once(once, [&] {
+  static PerDevice<Occupancy> cache;
+  const Occupancy *o = nullptr;
+  const cudaError_t e = per_device(cache, o, [](Occupancy &r) {
     const size_t smem = fused_smem_bytes<N, CONTIG, MODE>();
-    err = cudaFuncSetAttribute(k_fused<N, CONTIG, MODE>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    r.err = cudaFuncSetAttribute(k_fused<N, CONTIG, MODE>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int dev = 0, n_sm = 0, p = 0;
-    if (err == cudaSuccess) err = cudaGetDevice(&dev);
-    if (err == cudaSuccess) err = cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-    if (err == cudaSuccess)
-      err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&p, k_fused<N, CONTIG, MODE>, SH::THREADS,
-                                                          smem);
-    c_per_sm = std::max(1, p);
-    c_sms = std::max(1, n_sm);
+    if (r.err == cudaSuccess) r.err = cudaGetDevice(&dev);
+    if (r.err == cudaSuccess) r.err = cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+    if (r.err == cudaSuccess)
+      r.err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&p, k_fused<N, CONTIG, MODE>, SH::THREADS,
+                                                            smem);
+    r.per_sm = std::max(1, p);
+    r.sms = std::max(1, n_sm);
   });
-  per_sm = c_per_sm;
-  sms = c_sms;
-  return err;
+  if (e != cudaSuccess) return e;
+  per_sm = o->per_sm;
+  sms = o->sms;
+  return o->err;
 }
 
 template <int N, bool CONTIG, int MODE>
@@ -315,6 +320,23 @@ __global__ void k_selftest_wait(unsigned *err, unsigned long long limit_ns) {
 
 int launch_selftest_wait(unsigned *err, long long limit_ns, cudaStream_t st) {
   k_selftest_wait<<<1, 32, 0, st>>>(err, (unsigned long long)limit_ns);
+  QJ_CK_LAUNCH();
+  return 0;
+}
+
+// The kick pass's sin / cos of a float64 phase, one value per thread, for a
+// direct accuracy test of sincos_reduced.
+__global__ void k_selftest_sincos(const double *theta, float2 *out, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    float s, c;
+    sincos_reduced(theta[i], s, c);
+    out[i] = float2{s, c};
+  }
+}
+
+int launch_selftest_sincos(const double *theta, float2 *out, int n, cudaStream_t st) {
+  k_selftest_sincos<<<(n + 255) / 256, 256, 0, st>>>(theta, out, n);
   QJ_CK_LAUNCH();
   return 0;
 }

@@ -5,11 +5,32 @@
 #include <stdint.h>
 
 #include <atomic>
+#include <mutex>
 #include <vector>
 
 #include "qj_pass.cuh"
 
 namespace qj {
+
+// Set-up that belongs to one device's context (a kernel's shared-memory
+// attribute, occupancy, the SM count), done once per device ordinal: the
+// first call with device d current runs init(value of d); later calls on d
+// reuse it.  A process that drives several GPUs gets each one's own set-up.
+constexpr int kMaxDevices = 64;
+template <class T> struct PerDevice {
+  std::once_flag once[kMaxDevices];
+  T val[kMaxDevices];
+};
+template <class T, class F>
+cudaError_t per_device(PerDevice<T> &pd, const T *&out, F &&init) {
+  int dev = 0;
+  const cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  std::call_once(pd.once[dev], [&] { init(pd.val[dev]); });
+  out = &pd.val[dev];
+  return cudaSuccess;
+}
 
 // ----- error state (qj_api.cu) -----
 void set_error(const char *fmt, ...);
@@ -44,6 +65,8 @@ std::vector<float2> stage_twiddles(int n);
 // ----- pencil passes (qj_fused.cu, qj_fftpass.cu) -----
 // Launch one fused single-precision pass of `mode` along `a.axis` (length n).
 int launch_selftest_wait(unsigned *err, long long limit_ns, cudaStream_t st);
+// out[i] = (sin, cos) of theta[i] by the kick pass's own sincos_reduced.
+int launch_selftest_sincos(const double *theta, float2 *out, int n, cudaStream_t st);
 int launch_fused(int mode, int n, const FusedArgs &a, cudaStream_t st);
 // Number of CTAs a pass along `axis` launches (= partial sums written).
 int pass_blocks(int n_axis, int axis, int nx, int ny, int nz);

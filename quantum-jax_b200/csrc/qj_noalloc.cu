@@ -18,6 +18,9 @@
 #include <cmath>
 #include <mutex>
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include "../../include/qj.h"
 #include "qj_internal.h"
 
@@ -35,25 +38,66 @@ constexpr size_t kScratchBytes = kWorkBytes + kTwBytes + kKBytes;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
-// Device address of the scratch array on each device, looked up once per
-// device (with that device current) on its first call.
+// Device address of the scratch array on each device, looked up on the first
+// call with that device current and cached with the id of the context it
+// belongs to.  A later call in another context of the same device (after
+// cudaDeviceReset, which unloads the module and frees the array) looks the
+// address up again instead of handing out the old one.
+struct ScratchAddr {
+  unsigned long long ctx_id = 0;
+  void *addr = nullptr;
+};
 std::mutex g_mu;
-void *g_addr[256] = {};
+ScratchAddr g_addr[kMaxDevices];
+
+// cuCtxGetCurrent and cuCtxGetId from the driver, looked up once.
+struct CtxFns {
+  PFN_cuCtxGetCurrent_v4000 current = nullptr;
+  PFN_cuCtxGetId_v12000 id = nullptr;
+};
+const CtxFns &ctx_fns() {
+  static CtxFns f;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      f.current = reinterpret_cast<PFN_cuCtxGetCurrent_v4000>(p);
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      f.id = reinterpret_cast<PFN_cuCtxGetId_v12000>(p);
+  });
+  return f;
+}
+
+// Id of the calling thread's current context, 0 if none or unknown.
+unsigned long long current_ctx_id() {
+  const CtxFns &f = ctx_fns();
+  CUcontext c = nullptr;
+  unsigned long long id = 0;
+  if (f.current && f.id && f.current(&c) == CUDA_SUCCESS && c && f.id(c, &id) == CUDA_SUCCESS)
+    return id;
+  return 0;
+}
 
 int scratch_address(void **out) {
   int dev = 0;
   QJ_CK(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= 256) {
+  if (dev < 0 || dev >= kMaxDevices) {
     set_error("qj_get_potential_f32_noalloc: device ordinal %d out of range", dev);
     return QJ_ERR_ARG;
   }
   std::lock_guard<std::mutex> lock(g_mu);
-  if (!g_addr[dev]) {
+  ScratchAddr &s = g_addr[dev];
+  const unsigned long long id = current_ctx_id();
+  if (!s.addr || id == 0 || id != s.ctx_id) {
     void *p = nullptr;
     QJ_CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
-    g_addr[dev] = p;
+    s.addr = p;
+    s.ctx_id = current_ctx_id();  // the lookup made the device's context current
   }
-  *out = g_addr[dev];
+  *out = s.addr;
   return 0;
 }
 

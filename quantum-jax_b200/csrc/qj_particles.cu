@@ -666,13 +666,14 @@ int launch_bucket_sort(int n, int n_buckets, const StarBufs &b, cudaStream_t st,
   const unsigned nbits = cell_bits(n_buckets);
   const int use_smem = n <= kSortSmemMax;
   const size_t smem = use_smem ? (size_t)16 * n : 0;
-  static std::once_flag once;
-  static cudaError_t attr_err = cudaSuccess;
-  std::call_once(once, [&] {
-    attr_err = cudaFuncSetAttribute(k_bucket_sort, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    16 * kSortSmemMax);
-  });
-  QJ_CK(attr_err);
+  // the attribute belongs to the current device's context: set once per device
+  static PerDevice<cudaError_t> attr;
+  const cudaError_t *attr_err = nullptr;
+  QJ_CK(per_device(attr, attr_err, [](cudaError_t &r) {
+    r = cudaFuncSetAttribute(k_bucket_sort, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             16 * kSortSmemMax);
+  }));
+  QJ_CK(*attr_err);
   k_bucket_sort<<<nbox, 1024, smem, st>>>(b.bkey, n, nbits < 8 ? 8 : nbits, b.sortbuf, use_smem,
                                           b.perm, b.skey);
   QJ_CK_LAUNCH();

@@ -84,10 +84,35 @@ SIGNATURES = {
     "qj_plan_set_tuning": (c_int, [c_void_p, c_void_p, c_int]),
     "qj_autotune_kdk": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_double,
                                 c_double, c_int, c_void_p]),
+    "qj_selftest_sincos": (c_int, [c_void_p, c_void_p, c_int, c_void_p]),
+    "qj_xla_kdk_step_f32": (None, [c_void_p, ctypes.POINTER(c_void_p), ctypes.c_char_p,
+                                   ctypes.c_size_t, c_void_p]),
+    "qj_xla_get_potential_f32": (None, [c_void_p, ctypes.POINTER(c_void_p), ctypes.c_char_p,
+                                        ctypes.c_size_t, c_void_p]),
+    "qj_xla_set_status_fn": (None, [c_void_p]),
+    "qj_xla_last_status": (c_int, []),
+    "qj_xla_release_plans": (c_int, []),
     "qj_launch_count": (c_int64, []),
     "qj_profile_enable": (c_int, [c_int]),
     "qj_profile_read": (c_int, [ctypes.POINTER(c_double), ctypes.POINTER(c_int64), c_int]),
 }
+
+
+QJ_XLA_DESC_VERSION = 1
+
+
+class QjXlaKdkDesc(ctypes.Structure):
+    """qj_xla_kdk_desc: the backend_config of a qj_xla_kdk_step_f32 custom call."""
+    _fields_ = [("version", ctypes.c_int32), ("nsteps", ctypes.c_int32), ("n_s", ctypes.c_int32),
+                ("self_interaction", ctypes.c_int32), ("has_v_ext", ctypes.c_int32),
+                ("reserved", ctypes.c_int32), ("grid", QjGrid), ("phys", QjPhys),
+                ("m_s", c_double), ("dt", c_double)]
+
+
+class QjXlaPoissonDesc(ctypes.Structure):
+    """qj_xla_poisson_desc: the backend_config of a qj_xla_get_potential_f32 call."""
+    _fields_ = [("version", ctypes.c_int32), ("self_interaction", ctypes.c_int32),
+                ("grid", QjGrid), ("phys", QjPhys)]
 
 
 class QjFaccState(ctypes.Structure):

@@ -519,9 +519,12 @@ def gen_ics(ref_dir):
 
 def main():
     ap = _argparse.ArgumentParser()
-    ap.add_argument("ref_dir", nargs="?", default="/root/reference")
+    ap.add_argument("ref_dir", nargs="?", default=os.environ.get("QJ_REFERENCE_DIR"),
+                    help="checkout of the reference scripts (or $QJ_REFERENCE_DIR)")
     ap.add_argument("--only", default=None, help="generate one case, e.g. gen_ics")
     a = ap.parse_args()
+    if not a.ref_dir:
+        ap.error("give the reference checkout as ref_dir or in $QJ_REFERENCE_DIR")
     fns = (gen_stars, gen_gasbh, gen_tidal, gen_cosmo, gen_bondi, gen_bh, gen_ics, gen_bondi_ambient, gen_facc)
     for fn in fns:
         if a.only and fn.__name__ != a.only:

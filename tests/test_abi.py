@@ -50,7 +50,10 @@ def test_error_path_without_gpu_is_a_status_not_a_crash():
 # nothing, the error text, the launch counter, the profiler switches, and the
 # workspace size of no plan (0).
 _OK_ON_NULL = {"qj_plan_destroy", "qj_ensemble_destroy", "qj_last_error", "qj_launch_count",
-               "qj_profile_enable", "qj_profile_read", "qj_plan_workspace_bytes"}
+               "qj_profile_enable", "qj_profile_read", "qj_plan_workspace_bytes",
+               "qj_xla_set_status_fn", "qj_xla_last_status", "qj_xla_release_plans"}
+# XLA custom-call targets return nothing; their status is qj_xla_last_status().
+_VOID_TARGETS = {"qj_xla_kdk_step_f32", "qj_xla_get_potential_f32"}
 
 
 def _zero_args(argtypes):
@@ -78,6 +81,8 @@ def test_every_entry_point_rejects_null_arguments_without_a_gpu():
         if name in _OK_ON_NULL:
             continue
         rc = getattr(lib, name)(*_zero_args(argtypes))
+        if name in _VOID_TARGETS:
+            rc = lib.qj_xla_last_status()
         assert rc == qj._lib.QJ_ERR_ARG, name
         assert lib.qj_last_error(), name
     n = qj._lib.QJ_TUNE_N
@@ -124,3 +129,49 @@ def test_valid_plan_without_a_device_is_a_cuda_status():
     rc = lib.qj_plan_create(ctypes.byref(h), ctypes.byref(g), ctypes.byref(ph), 1, 8)
     assert rc == qj._lib.QJ_ERR_CUDA and h.value is None
     assert b"CUDA error" in lib.qj_last_error()
+
+
+def test_xla_descriptors_match_the_c_layout():
+    """The packed backend_config of each XLA target has the size the library
+    expects: a descriptor of the right length with a bad field is rejected as
+    a bad descriptor (not a wrong length), one byte short as a wrong length;
+    no CUDA call is reached."""
+    import ctypes
+
+    import qj
+    from qj import jax_ffi
+
+    lib = qj.lib()
+    g, ph = qj.Grid(32, 32, 32), qj.Phys()
+    bufs = (ctypes.c_void_p * 8)()
+    good = jax_ffi.pack_kdk(g, ph, n_s=-1, m_s=0.0, dt=1.0, nsteps=1)
+    assert len(good) == ctypes.sizeof(qj._lib.QjXlaKdkDesc) == 128
+    lib.qj_xla_kdk_step_f32(None, bufs, good, len(good), None)
+    assert lib.qj_xla_last_status() == qj._lib.QJ_ERR_ARG
+    assert b"bad descriptor" in lib.qj_last_error()
+    lib.qj_xla_kdk_step_f32(None, bufs, good, len(good) - 1, None)
+    assert b"descriptor of 127 bytes, expected 128" in lib.qj_last_error()
+    pot = jax_ffi.pack_poisson(g, ph)
+    assert len(pot) == ctypes.sizeof(qj._lib.QjXlaPoissonDesc)
+    lib.qj_xla_get_potential_f32(None, bufs, pot, len(pot), None)
+    assert lib.qj_xla_last_status() == qj._lib.QJ_ERR_ARG
+    assert b"null buffer" in lib.qj_last_error()
+
+
+def test_xla_failure_reaches_the_status_function():
+    """A failing target hands its message to the status function the binding
+    installs (jaxlib's XlaCustomCallStatusSetFailure in a JAX process)."""
+    import ctypes
+
+    import qj
+
+    lib = qj.lib()
+    seen = []
+    FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t)
+    cb = FN(lambda status, msg, n: seen.append((status, msg[:n])))
+    lib.qj_xla_set_status_fn(ctypes.cast(cb, ctypes.c_void_p))
+    try:
+        lib.qj_xla_kdk_step_f32(None, None, b"x", 1, ctypes.c_void_p(0x1234))
+    finally:
+        lib.qj_xla_set_status_fn(None)
+    assert seen and seen[0][0] == 0x1234 and b"descriptor of 1 bytes" in seen[0][1]

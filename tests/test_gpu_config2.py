@@ -1,0 +1,132 @@
+"""The headline configuration at its own size: 256^3 complex64 psi, 4096 stars,
+the seeded IC family (psi = sqrt(1 + 0.1 delta), uniform stars at rest with
+10 % of the dark-matter mass), dt = dx^2 / 6, 1000 KDK steps
+(quantum-stars.py:295-330 iterated as the fori_loop of :452-459).
+
+- fused float32 path against the plain float64 GPU path after 1000 steps:
+  psi and rho = |psi|^2 rel-L2 <= 1e-5 (the stated target), total-mass drift
+  |M / M0 - 1| <= 1e-6, star positions rel-L2 <= 1e-4;
+- the plain float64 path against the float64 oracle at 256^3 for 2 steps
+  (<= 1e-11), which ties the comparator of the first test to the oracle at
+  this size;
+- bin_stars of the 4096 stars: bit-exact against the sequential float32
+  deposit in the reference's order, and identical over 3 repeats;
+- two fused runs of 20 steps from the same state are bit-identical (the
+  deterministic deposit inside the step).
+"""
+
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+N, N_S = 256, 4096
+
+
+@pytest.fixture(scope="module")
+def ic():
+    psi, pos, vel, g, p = O.stars_ic(N, N_S, seed=0)
+    return psi, pos, vel, g, p, O.default_dt(g, p)
+
+
+def plan_of(g, p, precision):
+    import qj
+
+    return qj.Plan(qj.Grid(g.nx, g.ny, g.nz, g.Lx, g.Ly, g.Lz),
+                   qj.Phys(m_per_hbar=p.m_per_hbar, G=p.G, rho_bar=p.rho_bar), precision, N_S)
+
+
+def state(psi, pos, vel, dt, dbl):
+    ct, rt = (torch.complex128, torch.float64) if dbl else (torch.complex64, torch.float32)
+    return (torch.as_tensor(psi, dtype=ct, device="cuda"),
+            torch.as_tensor(pos, dtype=rt, device="cuda"),
+            torch.as_tensor(vel, dtype=rt, device="cuda"),
+            torch.tensor([0.0, 0.0, dt], dtype=torch.float64, device="cuda"))
+
+
+def rel(a, b):
+    return float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b))
+
+
+def test_config2_fused_vs_plain_f64_1000_steps(ic):
+    import qj
+
+    psi, pos, vel, g, p, dt = ic
+    steps = 1000
+    out = {}
+    for prec, dbl in ((qj.FUSED_F32, False), (qj.PLAIN_F64, True)):
+        plan = plan_of(g, p, prec)
+        ps, po, ve, dg = state(psi, pos, vel, dt, dbl)
+        plan.kdk_step(ps, po, ve, dg, dt, steps, p.m_s)
+        plan.status()
+        out[dbl] = (ps.to(torch.complex128), po.double(), ve.double(), dg.cpu().numpy())
+        plan.close()
+    f, d = out[False], out[True]
+    psi_err = rel(f[0], d[0])
+    rho_err = rel(f[0].abs() ** 2, d[0].abs() ** 2)
+    m0 = float(np.sum(np.abs(psi) ** 2))
+    drift = float((f[0].abs() ** 2).sum()) / m0 - 1.0
+    pos_err = rel(f[1], d[1])
+    print(f"256^3 x 1000: psi {psi_err:.3e} rho {rho_err:.3e} mass drift {drift:.3e} "
+          f"pos {pos_err:.3e}")
+    assert psi_err <= 1e-5
+    assert rho_err <= 1e-5
+    assert abs(drift) <= 1e-6
+    assert pos_err <= 1e-4
+    assert f[3][0] == pytest.approx(d[3][0], rel=1e-12)  # t
+    assert f[3][1] == pytest.approx(d[3][1], rel=1e-4)   # a_max
+
+
+def test_config2_plain_f64_vs_oracle(ic):
+    import qj
+
+    psi, pos, vel, g, p, dt = ic
+    O.WORKERS = os.cpu_count() or 1
+    k = O.kgrid(g)
+    ref = (psi, pos, vel, 0.0, 0.0, dt)
+    for _ in range(2):
+        ref = O.stars_compute_step(*ref, g, p, dt, k)
+    plan = plan_of(g, p, qj.PLAIN_F64)
+    ps, po, ve, dg = state(psi, pos, vel, dt, True)
+    plan.kdk_step(ps, po, ve, dg, dt, 2, p.m_s)
+    plan.status()
+    assert O.rel_l2(ps.cpu().numpy(), ref[0]) <= 1e-11
+    assert O.rel_l2(po.cpu().numpy(), ref[1]) <= 1e-12
+    assert O.rel_l2(ve.cpu().numpy(), ref[2]) <= 1e-10
+    plan.close()
+
+
+def test_config2_bin_stars_bit_exact_and_repeatable(ic):
+    import qj
+
+    psi, pos, vel, g, p, dt = ic
+    pos32 = pos.astype(np.float32)
+    ref = O.bin_stars_f32_vec(pos32, g, p.m_s)
+    plan = plan_of(g, p, qj.FUSED_F32)
+    d_pos = torch.as_tensor(pos32, device="cuda")
+    runs = [plan.bin_stars(d_pos, m_s=p.m_s).cpu().numpy() for _ in range(3)]
+    for r in runs:
+        assert np.array_equal(r.view(np.uint32), ref.view(np.uint32))
+    plan.close()
+
+
+def test_config2_fused_repeat_runs_bit_identical(ic):
+    import qj
+
+    psi, pos, vel, g, p, dt = ic
+    plan = plan_of(g, p, qj.FUSED_F32)
+    res = []
+    for _ in range(2):
+        ps, po, ve, dg = state(psi, pos, vel, dt, False)
+        plan.kdk_step(ps, po, ve, dg, dt, 20, p.m_s)
+        plan.status()
+        res.append((ps.cpu(), po.cpu(), ve.cpu(), dg.cpu()))
+    for x, y in zip(*res):
+        assert torch.equal(x.view(torch.float32) if x.is_complex() else x,
+                           y.view(torch.float32) if y.is_complex() else y)
+    plan.close()

@@ -6,7 +6,8 @@ synchronise its stream schedule); this entry point keeps its scratch in a
 fixed device array instead.  It is checked through the C ABI against the
 plan-based qj_get_potential (single precision, same tolerance as the other
 float32 Poisson tests), on two calls in a row with different inputs, since
-the scratch array is shared and keeps the previous call's contents.
+the scratch array is shared and keeps the previous call's contents, and on
+its own against the float64 oracle.
 
 The file name makes pytest collect it last.
 """
@@ -16,6 +17,8 @@ import ctypes
 import numpy as np
 import pytest
 import torch
+
+from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
@@ -51,6 +54,11 @@ def test_noalloc_matches_plan_two_calls(shape, L):
             torch.cuda.synchronize()
             assert torch.isfinite(V).all()
             assert rel(V, ref) < TOL, (call, si)
+            # and on its own against the float64 oracle of quantum-stars.py:189-193
+            og = O.Grid(*shape, *L)
+            op = O.Phys(m_per_hbar=1.0, G=phys.G, rho_bar=phys.rho_bar, b_coeff=phys.b_coeff)
+            want = O.get_potential(rho.double().cpu().numpy(), og, op, self_interaction=bool(si))
+            assert O.rel_l2(V.double().cpu().numpy(), want) < TOL, (call, si)
     plan.close()
 
 
