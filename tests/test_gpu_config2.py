@@ -5,7 +5,7 @@ the seeded IC family (psi = sqrt(1 + 0.1 delta), uniform stars at rest with
 
 - fused float32 path against the plain float64 GPU path after 1000 steps:
   psi and rho = |psi|^2 rel-L2 <= 1e-5 (the stated target), total-mass drift
-  |M / M0 - 1| <= 1e-6, star positions rel-L2 <= 1e-4;
+  |M / M0 - 1| <= 1e-6, star positions rel-L2 <= 1e-6 (measured 3.9e-8);
 - the plain float64 path against the float64 oracle at 256^3 for 2 steps
   (<= 1e-11), which ties the comparator of the first test to the oracle at
   this size;
@@ -77,7 +77,7 @@ def test_config2_fused_vs_plain_f64_1000_steps(ic):
     assert psi_err <= 1e-5
     assert rho_err <= 1e-5
     assert abs(drift) <= 1e-6
-    assert pos_err <= 1e-4
+    assert pos_err <= 1e-6
     assert f[3][0] == pytest.approx(d[3][0], rel=1e-12)  # t
     assert f[3][1] == pytest.approx(d[3][1], rel=1e-4)   # a_max
 
