@@ -282,6 +282,7 @@ void set_stars(FusedArgs &a, const qj_plan *P) {
   a.sw1 = P->sb.sw1;
   a.perm = P->sb.perm;
   a.bstart = P->sb.bstart;
+  a.pmask = P->sb.pmask;
   a.A = P->sb.A;
 }
 
@@ -310,6 +311,9 @@ int ensure_prop(qj_plan *P, double dtk, cudaStream_t st) {
 }
 
 int n_pencils(const qj_plan *P, int q) { return (int)(P->ncell / P->n[q]); }
+// Star buckets of orientation q form rows of bucket_nv pencils (b = cu nv + cv):
+// v is y for z pencils, z otherwise.
+int bucket_nv(const qj_plan *P, int q) { return q == 2 ? P->n[1] : P->n[2]; }
 
 // Particle data of a single box, sorted by bucket (pencil of the lower corner
 // along q): one launch for a few particles (black holes), else prepare + sort.
@@ -317,7 +321,7 @@ int stars_prepare_sort(qj_plan *P, const void *pos, int n, const void *masses, d
                        cudaStream_t st) {
   if (n <= 32) return launch_stars_small(pos, n, masses, m_s, geom(P), q, n_pencils(P, q), P->sb, st);
   QJ_TRY(launch_stars_prepare(pos, n, masses, m_s, geom(P), q, P->sb, st));
-  return launch_bucket_sort(n, n_pencils(P, q), P->sb, st);
+  return launch_bucket_sort(n, n_pencils(P, q), bucket_nv(P, q), P->sb, st);
 }
 
 
@@ -365,7 +369,8 @@ int fused_kdk(qj_plan *P, float2 *psi, float *pos, float *vel, int n_s, double m
   if (parts) {
     if (prof_on()) prof_mark_begin(st);
     QJ_TRY(launch_stars_prepare(pos, n_s * nb, nullptr, m_s, geom(P), q, P->sb, st));
-    QJ_TRY(launch_bucket_sort(n_s, n_pencils(P, q), P->sb, st, nb, P->bstart_stride));
+    QJ_TRY(launch_bucket_sort(n_s, n_pencils(P, q), bucket_nv(P, q), P->sb, st, nb,
+                              P->bstart_stride));
     if (prof_on()) prof_mark_end(7, st);
   }
   {
@@ -438,7 +443,8 @@ int fused_kdk(qj_plan *P, float2 *psi, float *pos, float *vel, int n_s, double m
       u.m_s = m_s;
       QJ_TRY(launch_update_fused(pos, vel, geom(P), u, P->sb, pst));
       if (!last)
-        QJ_TRY(launch_bucket_sort(n_s, n_pencils(P, r), P->sb, pst, nb, P->bstart_stride));
+        QJ_TRY(launch_bucket_sort(n_s, n_pencils(P, r), bucket_nv(P, r), P->sb, pst, nb,
+                                  P->bstart_stride));
       if (prof_on()) prof_mark_end(8, pst);
       QJ_CK(cudaEventRecord(P->ev_parts, pst));
     }
@@ -960,6 +966,8 @@ int qj_plan_create_batched(qj_plan **plan, const qj_grid *grid, const qj_phys *p
     if ((rc = dev_alloc_t(P, &b.skey, np))) return fail(rc);
     if ((rc = dev_alloc_t(P, &b.sortbuf, 4 * np))) return fail(rc);
     if ((rc = dev_alloc_t(P, &b.bstart, (size_t)(npen + 1) * nbox))) return fail(rc);
+    b.mstride = (int)((npen + 1 + 31) / 32);
+    if ((rc = dev_alloc_t(P, &b.pmask, (size_t)b.mstride * nbox))) return fail(rc);
     b.A = (float *)P->A;
     int lo = 0, hi = 0;
     cudaError_t e0 = cudaDeviceGetStreamPriorityRange(&lo, &hi);
@@ -1483,7 +1491,7 @@ int qj_bin_stars(qj_plan *P, const void *pos, int n, double m_s, const void *mas
   a.rho_out = (float *)rho_s;
   if (n > 0) {
     QJ_TRY(launch_stars_prepare(pos, n, masses, m_s, geom(P), 2, P->sb, st));
-    QJ_TRY(launch_bucket_sort(n, n_pencils(P, 2), P->sb, st));
+    QJ_TRY(launch_bucket_sort(n, n_pencils(P, 2), bucket_nv(P, 2), P->sb, st));
     set_stars(a, P);
   }
   return launch_fused(M_DEPOSIT, P->n[2], a, st);

@@ -129,15 +129,21 @@ struct StarBufs {
   unsigned *perm;    // [n] stars sorted by (bucket, star)
   unsigned *skey;    // [n] sorted bucket keys
   int *bstart;       // [n_buckets + 1]
+  // pencil mask, [ceil(n_buckets / 32)] words per box at stride mstride: bit
+  // p is set when some star's corners lie on pencil p; the kick skips the
+  // star lookups of the other pencils
+  unsigned *pmask;
+  int mstride;
   unsigned *sortbuf; // [4 n] global sort scratch (large n)
   float *A;          // [8 n][3] accelerations at the 8 corners of each star
 };
 int launch_stars_prepare(const void *pos, int n, const void *masses, double m_s,
                          const CicGeomD &g, int q, const StarBufs &b, cudaStream_t st);
-// n stars per box, nbox boxes (one sort CTA each), bucket starts per box at
-// stride bstride.
-int launch_bucket_sort(int n, int n_buckets, const StarBufs &b, cudaStream_t st, int nbox = 1,
-                       int bstride = 0);
+// n stars per box, nbox boxes (one sort CTA each): permutation, sorted keys,
+// pencil mask, and bucket starts per box at stride bstride; buckets form
+// rows of nv (the extent of the faster cross axis of the orientation).
+int launch_bucket_sort(int n, int n_buckets, int nv, const StarBufs &b, cudaStream_t st,
+                       int nbox = 1, int bstride = 0);
 // n <= 32 particles, one box: launch_stars_prepare + launch_bucket_sort in one launch
 int launch_stars_small(const void *pos, int n, const void *masses, double m_s, const CicGeomD &g,
                        int q, int n_buckets, const StarBufs &b, cudaStream_t st);

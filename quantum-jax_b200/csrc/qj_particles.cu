@@ -489,13 +489,13 @@ int launch_stars_prepare(const void *pos, int n, const void *masses, double m_s,
 // index) and the bucket starts in one launch.  Every block works out the n
 // keys; block 0 also stores the particle data, the permutation and the sorted
 // keys (each particle's rank by counting, the order of the stable sort); every
-// block fills its share of bstart[b] = the number of keys below b, the lower
-// bound k_bucket_starts finds.
+// block fills its share of the bucket runs and the bucket mask, as
+// k_bucket_sort leaves them.
 constexpr int kSmallStars = 32;
 __global__ void __launch_bounds__(256)
     k_stars_small(const float *pos, int n, const float *masses, float fac_all, CicGeom<float> g,
                   int q, int4 *sidx, float4 *sw0, float4 *sw1, unsigned *bkey, unsigned *perm,
-                  unsigned *skey, int *bstart, int n_buckets) {
+                  unsigned *skey, int *bstart, unsigned *pmask, int n_buckets) {
   __shared__ unsigned keys[kSmallStars];
   const int s = threadIdx.x;
   if (s < kSmallStars) {
@@ -523,10 +523,24 @@ __global__ void __launch_bounds__(256)
     perm[rank] = (unsigned)s;
     skey[rank] = key;
   }
+  // bstart[b] = the keys below b (the lower bound k_bucket_starts finds), and
+  // the pencil mask
   for (int b = blockIdx.x * blockDim.x + threadIdx.x; b <= n_buckets; b += gridDim.x * blockDim.x) {
     int c = 0;
     for (int j = 0; j < n; ++j) c += keys[j] < (unsigned)b ? 1 : 0;
     bstart[b] = c;
+    if (b == n_buckets) continue;
+    // pencil b has particles when any of its four touching buckets does
+    const int nv = q == 2 ? g.n[1] : g.n[2], nu = n_buckets / nv;
+    const int cu = b / nv, cv = b - cu * nv;
+    const int cum = cu == 0 ? nu - 1 : cu - 1, cvm = cv == 0 ? nv - 1 : cv - 1;
+    const unsigned nb[4] = {(unsigned)b, (unsigned)(cum * nv + cv), (unsigned)(cu * nv + cvm),
+                            (unsigned)(cum * nv + cvm)};
+    int touch = 0;
+    for (int j = 0; j < n; ++j)
+      touch |= (keys[j] == nb[0]) | (keys[j] == nb[1]) | (keys[j] == nb[2]) | (keys[j] == nb[3]);
+    const unsigned pword = __ballot_sync(__activemask(), touch != 0);
+    if ((b & 31) == 0) pmask[b >> 5] = pword;
   }
 }
 
@@ -540,7 +554,7 @@ int launch_stars_small(const void *pos, int n, const void *masses, double m_s, c
   const int T = 256, B = (n_buckets + 1 + T - 1) / T;
   k_stars_small<<<B, T, 0, st>>>((const float *)pos, n, (const float *)masses, (float)fac,
                                  cast_geom<float>(g), q, b.sidx, b.sw0, b.sw1, b.bkey, b.perm, b.skey,
-                                 b.bstart, n_buckets);
+                                 b.bstart, b.pmask, n_buckets);
   QJ_CK_LAUNCH();
   return 0;
 }
@@ -551,19 +565,26 @@ constexpr int kSortSmemMax = 8192;
 
 __global__ void __launch_bounds__(1024)
     k_bucket_sort(const unsigned *bkey, int n, unsigned nbits, unsigned *gbuf, int use_smem,
-                  unsigned *perm, unsigned *skey) {
+                  unsigned *perm, unsigned *skey, int n_buckets, int nv, unsigned *pmask,
+                  int mstride) {
+  // dynamic shared memory: the mask of non-empty buckets (one bit per
+  // bucket), then the sort buffers when they fit
   extern __shared__ unsigned dyn[];
   __shared__ unsigned hist[32 * 256];
   __shared__ unsigned dbase[256];
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const int mwords = (n_buckets + 31) / 32;
+  unsigned *mask = dyn;
   {  // one CTA per box of a batched plan
     const long long box = blockIdx.x;
     bkey += box * n;
     gbuf += box * 4 * n;
     perm += box * n;
     skey += box * n;
+    pmask += box * mstride;
   }
-  unsigned *buf = use_smem ? dyn : gbuf;
+  for (int i = tid; i < mwords; i += 1024) mask[i] = 0u;  // (the passes below sync)
+  unsigned *buf = use_smem ? dyn + mwords : gbuf;
   unsigned *kA = buf, *iA = buf + n, *kB = buf + 2 * n, *iB = buf + 3 * n;
   const int chunk = (n + 31) / 32;
   const int beg = min(n, w * chunk), end = min(n, beg + chunk);
@@ -636,9 +657,47 @@ __global__ void __launch_bounds__(1024)
     kout = (kout == kA) ? kB : kA;
     iout = (iout == iA) ? iB : iA;
   }
+  // the permutation, the sorted keys and the mask of non-empty buckets (in
+  // shared memory)
   for (int i = tid; i < n; i += 1024) {
+    const unsigned k = kin[i];
     perm[i] = iin ? iin[i] : (unsigned)i;
-    skey[i] = kin[i];
+    skey[i] = k;
+    if (i == 0 || kin[i - 1] != k) atomicOr(&mask[k >> 5], 1u << (k & 31));
+  }
+  __syncthreads();
+  // pencil mask: pencil (u, v) has stars when any of the buckets (u, v),
+  // (u, v - 1), (u - 1, v), (u - 1, v - 1) (wrapped) does.  With rows of a
+  // whole number of words this is word arithmetic: the bucket mask, its
+  // one-bit shift along v within each row, and the same of the row above.
+  const int nu = n_buckets / nv;
+  if (nv % 32 == 0) {
+    const int rw = nv / 32;  // words per row
+    auto vshift = [&](int wd) {  // bits of (u, v - 1) for the pencils of word wd
+      const int row0 = wd - wd % rw;
+      const int prev = wd == row0 ? row0 + rw - 1 : wd - 1;
+      return (mask[wd] << 1) | (mask[prev] >> 31);
+    };
+    for (int i = tid; i < mwords; i += 1024) {
+      const int up = i >= rw ? i - rw : i + (nu - 1) * rw;
+      pmask[i] = mask[i] | vshift(i) | mask[up] | vshift(up);
+    }
+  } else {
+    for (int i = tid; i < mwords; i += 1024) {
+      unsigned word = 0u;
+      for (int j = 0; j < 32; ++j) {
+        const int p = 32 * i + j;
+        if (p >= n_buckets) break;
+        const int cu = p / nv, cv = p - cu * nv;
+        const int cum = cu == 0 ? nu - 1 : cu - 1, cvm = cv == 0 ? nv - 1 : cv - 1;
+        const int nb[4] = {p, cum * nv + cv, cu * nv + cvm, cum * nv + cvm};
+        unsigned on = 0u;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) on |= (mask[nb[k] >> 5] >> (nb[k] & 31)) & 1u;
+        word |= on << j;
+      }
+      pmask[i] = word;
+    }
   }
 }
 
@@ -660,22 +719,30 @@ __global__ void k_bucket_starts(const unsigned *skey, int n, int n_buckets, int 
   bstart[b] = lo;
 }
 
-int launch_bucket_sort(int n, int n_buckets, const StarBufs &b, cudaStream_t st, int nbox,
+// Largest bucket mask of a sort (512 x 512 pencils), in 32-bit words.
+constexpr int kMaskWordsMax = 512 * 512 / 32;
+
+int launch_bucket_sort(int n, int n_buckets, int nv, const StarBufs &b, cudaStream_t st, int nbox,
                        int bstride) {
   if (n <= 0) return 0;
+  const int mwords = (n_buckets + 31) / 32;
+  if (mwords > kMaskWordsMax || nv <= 0 || n_buckets % nv != 0) {
+    set_error("internal: %d star buckets (rows of %d) do not fit the bucket mask", n_buckets, nv);
+    return QJ_ERR_ARG;
+  }
   const unsigned nbits = cell_bits(n_buckets);
   const int use_smem = n <= kSortSmemMax;
-  const size_t smem = use_smem ? (size_t)16 * n : 0;
+  const size_t smem = (size_t)4 * mwords + (use_smem ? (size_t)16 * n : 0);
   // the attribute belongs to the current device's context: set once per device
   static PerDevice<cudaError_t> attr;
   const cudaError_t *attr_err = nullptr;
   QJ_CK(per_device(attr, attr_err, [](cudaError_t &r) {
     r = cudaFuncSetAttribute(k_bucket_sort, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             16 * kSortSmemMax);
+                             16 * kSortSmemMax + 4 * kMaskWordsMax);
   }));
   QJ_CK(*attr_err);
   k_bucket_sort<<<nbox, 1024, smem, st>>>(b.bkey, n, nbits < 8 ? 8 : nbits, b.sortbuf, use_smem,
-                                          b.perm, b.skey);
+                                          b.perm, b.skey, n_buckets, nv, b.pmask, b.mstride);
   QJ_CK_LAUNCH();
   const int T = 256, B = (n_buckets + 1 + T - 1) / T;
   k_bucket_starts<<<dim3(B, nbox), T, 0, st>>>(b.skey, n, n_buckets, b.bstart, bstride);

@@ -59,6 +59,7 @@ struct FusedArgs {
   const float4 *sw1;
   const unsigned *perm;
   const int *bstart;
+  const unsigned *pmask;  // bit per pencil: some star touches it (clear for most)
   float *A;  // [8 n][3] accelerations at the 8 corners of each star (x, y, z)
   float *rho_out;  // M_DEPOSIT: dense star density
   // float64 density partial sums
@@ -129,6 +130,12 @@ __device__ __forceinline__ void select_box(FusedArgs &a) {
   if (a.perm) a.perm += s;
   if (a.A) a.A += 24 * s;
   if (a.bstart) a.bstart += (long long)b * a.box_bstart;
+  if (a.pmask) a.pmask += (long long)b * ((a.box_bstart + 31) / 32);
+}
+
+// Whether any star touches pencil pid (one bit of the pencil mask).
+__device__ __forceinline__ bool pencil_has_stars(const FusedArgs &a, int pid) {
+  return (a.pmask[pid >> 5] >> (pid & 31)) & 1u;
 }
 
 // Per-thread position of a pencil in the grid.
@@ -260,8 +267,8 @@ struct StarRanges {
   int lo[4], hi[4];
   int u, v, cu, cv;
 };
-__device__ __forceinline__ StarRanges star_ranges(const FusedArgs &a, const PencilPos &pp) {
-  StarRanges r;
+__device__ __forceinline__ void star_buckets(const FusedArgs &a, const PencilPos &pp, StarRanges &r,
+                                             int (&b)[4]) {
   const int q = a.axis;
   r.u = q == 1 ? 0 : (q == 2 ? 0 : 1);
   r.v = q == 2 ? 1 : 2;
@@ -269,7 +276,15 @@ __device__ __forceinline__ StarRanges star_ranges(const FusedArgs &a, const Penc
   r.cu = r.u == 0 ? pp.c[0] : pp.c[1];
   r.cv = r.v == 1 ? pp.c[1] : pp.c[2];
   const int cum = r.cu == 0 ? nu - 1 : r.cu - 1, cvm = r.cv == 0 ? nv - 1 : r.cv - 1;
-  const int b[4] = {r.cu * nv + r.cv, cum * nv + r.cv, r.cu * nv + cvm, cum * nv + cvm};
+  b[0] = r.cu * nv + r.cv;
+  b[1] = cum * nv + r.cv;
+  b[2] = r.cu * nv + cvm;
+  b[3] = cum * nv + cvm;
+}
+__device__ __forceinline__ StarRanges star_ranges(const FusedArgs &a, const PencilPos &pp) {
+  StarRanges r;
+  int b[4];
+  star_buckets(a, pp, r, b);
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
     r.lo[k] = a.bstart[b[k]];
@@ -277,37 +292,48 @@ __device__ __forceinline__ StarRanges star_ranges(const FusedArgs &a, const Penc
   }
   return r;
 }
+// Empty ranges: for_star_corners visits nothing.
+__device__ __forceinline__ StarRanges no_star_ranges() {
+  StarRanges r;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) r.lo[k] = r.hi[k] = 0;
+  r.u = r.v = r.cu = r.cv = 0;
+  return r;
+}
 
 // Visit the stars touching this pencil; with ORDERED, in increasing star
-// index (a 4-way merge of the buckets, each already in star order).  For each
-// star and each of its two corners on the pencil (positions i0_q and
-// i0_q + 1), f(s, corner, m, wx, wy, wz, fac) is called on the thread that
-// owns position m.
+// index (a 4-way merge of the buckets, each already in star order), else
+// bucket by bucket.  For each star and each of its two corners on the pencil
+// (positions i0_q and i0_q + 1), f(s, corner, m, wx, wy, wz, fac) is called on
+// the thread that owns position m.
 template <int N, bool ORDERED, class F>
 __device__ __forceinline__ void for_star_corners(const FusedArgs &a, StarRanges r, int t, int P, F &&f) {
   const int q = a.axis;
   while (true) {
     int kb = -1;
     unsigned s = 0xffffffffu;
+    if constexpr (ORDERED) {
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      if (r.lo[k] < r.hi[k]) {
-        const unsigned sk = a.perm[r.lo[k]];
-        if (!ORDERED) {
-          if (kb < 0) {
-            kb = k;
+      for (int k = 0; k < 4; ++k) {
+        if (r.lo[k] < r.hi[k]) {
+          const unsigned sk = a.perm[r.lo[k]];
+          if (sk < s) {
             s = sk;
+            kb = k;
           }
-        } else if (sk < s) {
-          s = sk;
-          kb = k;
         }
       }
+    } else {
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        if (kb < 0 && r.lo[k] < r.hi[k]) kb = k;
     }
     if (kb < 0) break;
+    int j = 0;
 #pragma unroll
     for (int k = 0; k < 4; ++k)
-      if (k == kb) r.lo[k]++;
+      if (k == kb) j = r.lo[k]++;
+    if constexpr (!ORDERED) s = a.perm[j];
     const int4 id = a.sidx[s];
     const float4 w0 = a.sw0[s], w1 = a.sw1[s];
     const int bu = (r.cu == sel3(id.x, id.y, id.z, r.u)) ? 0 : 1;
@@ -708,7 +734,7 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CO
     // the density passes load the pencil's star buckets before the transforms
     // they would otherwise wait behind (in the kick the extra live registers
     // cost more than the latency they hide)
-    StarRanges sr;
+    StarRanges sr = no_star_ranges();
     if constexpr (MODE == M_DENSITY || MODE == M_DRIFT_DENSITY)
       if (a.has_stars) sr = star_ranges(a, pp);
     float2 c0;
@@ -901,6 +927,8 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CO
       const unsigned gb = (unsigned)base + (unsigned)t * (unsigned)st, gs = (unsigned)P * (unsigned)st;
       float am = 0.0f;
       float V[E];
+      // stars touching this pencil (most pencils have none and skip the lookups)
+      const bool pstars = a.has_stars && pencil_has_stars(a, pp.pid);
       {
         // phase 1: S2 -> a_q + i a_y
         float2 v2[E];
@@ -908,7 +936,7 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CO
         fft_pencil<N, +1, true>(v2, t, smv, tw);
 #pragma unroll
         for (int e = 0; e < E; ++e) am = fmaxf(am, fmaxf(fabsf(v2[e].x), fabsf(v2[e].y)));
-        if (a.has_stars) {
+        if (pstars) {
           // the corner lookups index the thread's save slots (free until the drift)
 #pragma unroll
           for (int e = 0; e < E; ++e) save[e * THREADS + tid] = v2[e];
@@ -943,7 +971,7 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CO
           V[e] = v1[e].x;
           am = fmaxf(am, fabsf(v1[e].y));
         }
-        if (a.has_stars) {
+        if (pstars) {
 #pragma unroll
           for (int e = 0; e < E; ++e) save[e * THREADS + tid].x = v1[e].y;
           for_star_corners<N, false>(a, star_ranges(a, pp), t, P,
@@ -969,7 +997,7 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CO
         float *rs = reinterpret_cast<float *>(save);
 #pragma unroll
         for (int e = 0; e < E; ++e) rs[2 * (e * THREADS + tid)] = 0.0f;
-        if (a.has_stars)
+        if (pstars)
           for_star_corners<N, true>(a, star_ranges(a, pp), t, P,
                                     [&](unsigned, int, int m, float wx, float wy, float wz, float fac) {
                                       const float val = fmul_rn(fmul_rn(fmul_rn(wx, wy), wz), fac);
