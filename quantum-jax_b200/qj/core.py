@@ -481,3 +481,73 @@ class StarsStep:
          state["dt_s"]) = self.compute_step(state["psi"], state["pos"], state["vel"],
                                             state["t"], state["a_max"], state["dt_s"])
         return state
+
+
+class HostPipeline:
+    """Host-resident states stepped on the device with the copies overlapped.
+
+    The reference hands its state back to the host every nt_sub steps
+    (quantum-stars.py:452-459).  For a sequence of states that live in host
+    memory (an ensemble fed from the host, or snapshots written out), each
+    call of ``run`` takes state i from pinned host memory, runs ``nsteps``
+    KDK steps on it and writes the result to pinned host memory.  The device
+    holds ``depth`` state buffers: while state i steps on the caller's current
+    stream, state i + 1 is copied in on one copy stream and state i - 1
+    copied out on another, so a call costs about the larger of the steps and
+    one copy instead of their sum.  Results are the same bits as
+    ``Plan.kdk_step`` on each state alone.
+
+    inputs / outputs: sequences of (psi, pos, vel, diag) pinned CPU tensors
+    (diag float64 [3] = t, a_max, dt_s; pos / vel None without stars).  The
+    outputs are complete when the caller's current stream is (``run``
+    returns once everything is enqueued)."""
+
+    def __init__(self, plan: Plan, dt, nsteps, m_s=0.0, n_s=0, depth=3, self_interaction=False,
+                 v_ext=None, device=None):
+        if depth < 2:
+            raise ValueError("depth must be at least 2")
+        self.plan, self.dt, self.nsteps, self.m_s = plan, float(dt), int(nsteps), float(m_s)
+        self.si, self.v_ext = self_interaction, v_ext
+        dev = torch.device(device) if device is not None else torch.device("cuda")
+        shape = plan.grid.shape
+        self.bufs = []
+        for _ in range(depth):
+            ps = torch.empty(shape, dtype=plan.cdtype, device=dev)
+            po = torch.empty((n_s, 3), dtype=plan.rdtype, device=dev) if n_s else None
+            ve = torch.empty((n_s, 3), dtype=plan.rdtype, device=dev) if n_s else None
+            dg = torch.empty(3, dtype=torch.float64, device=dev)
+            self.bufs.append((ps, po, ve, dg))
+        self.h2d = torch.cuda.Stream(device=dev)
+        self.d2h = torch.cuda.Stream(device=dev)
+        self.free = [None] * depth  # event: buffer b's last copy-out is done
+
+    def run(self, inputs, outputs):
+        cur = torch.cuda.current_stream()
+        depth = len(self.bufs)
+        for i, (hin, hout) in enumerate(zip(inputs, outputs)):
+            b = i % depth
+            buf = self.bufs[b]
+            with torch.cuda.stream(self.h2d):
+                if self.free[b] is not None:
+                    self.h2d.wait_event(self.free[b])
+                for d, h in zip(buf, hin):
+                    if d is not None:
+                        d.copy_(h, non_blocking=True)
+                ev_in = torch.cuda.Event()
+                ev_in.record(self.h2d)
+            cur.wait_event(ev_in)
+            ps, po, ve, dg = buf
+            self.plan.kdk_step(ps, po, ve, dg, self.dt, self.nsteps, self.m_s, self.si,
+                               self.v_ext)
+            ev_done = torch.cuda.Event()
+            ev_done.record(cur)
+            with torch.cuda.stream(self.d2h):
+                self.d2h.wait_event(ev_done)
+                for h, d in zip(hout, buf):
+                    if d is not None:
+                        h.copy_(d, non_blocking=True)
+                ev_free = torch.cuda.Event()
+                ev_free.record(self.d2h)
+                self.free[b] = ev_free
+        cur.wait_stream(self.d2h)
+        return outputs
