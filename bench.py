@@ -512,7 +512,10 @@ def main():
         from qj.autograd import kdk_evolve
 
         na, steps_a, K = a.adj_n, a.adj_steps, a.adj_ckpt
-        psi_a, _, _, ga, pa = O.stars_ic(na, 0, seed=0)
+        # the IC family with its 4096 stars as a fixed source density
+        psi_a, pos_a, _, ga, pa = O.stars_ic(na, 4096, seed=0)
+        rho_sa = torch.as_tensor(O.bin_stars(pos_a, ga, np.full(len(pos_a), pa.m_s)),
+                                 dtype=torch.float32, device=dev)
         dta = O.default_dt(ga, pa)
         plan_a = qj.Plan(qj.Grid(na, na, na), qj.Phys(m_per_hbar=1.0, G=pa.G, rho_bar=pa.rho_bar),
                          qj.FUSED_F32, 1)
@@ -520,10 +523,13 @@ def main():
         th = torch.as_tensor(0.5 * O.delta_field(na, 21), dtype=torch.float32,
                              device=dev).requires_grad_(True)
         psi2, *_ = O.stars_ic(na, 0, seed=1)
-        tgt = torch.as_tensor(np.abs(psi2) ** 2, dtype=torch.float32, device=dev)
+        with torch.no_grad():  # target: a forward run from a second seed
+            s2 = torch.as_tensor(np.abs(psi2), dtype=torch.float32, device=dev)
+            tgt = torch.abs(kdk_evolve(torch.zeros_like(s2), s2, plan_a, dta, steps_a, K,
+                                       rho_s=rho_sa)) ** 2
 
         def fwd():
-            return kdk_evolve(th, s, plan_a, dta, steps_a, K)
+            return kdk_evolve(th, s, plan_a, dta, steps_a, K, rho_s=rho_sa)
 
         def run_bwd(psiT):
             L = torch.mean((torch.abs(psiT) ** 2 - tgt) ** 2)
@@ -550,10 +556,13 @@ def main():
         barrier()
         b_ms = e0.elapsed_time(e1)
         adjoint = {"grid": [na] * 3, "steps": steps_a, "checkpoint_every": K,
-                   "forward_ms": f_ms, "forward_with_checkpoints_ms": fc_ms,
-                   "backward_ms": b_ms, "adjoint_over_forward": b_ms / f_ms,
-                   "note": "backward = chunk recompute from checkpoints + reverse sweep "
-                           "(two Poisson solves per kick); forward = qj_kdk_step, psi only"}
+                   "star_source": "4096 stars' CIC density, held fixed",
+                   "forward_ms": fc_ms, "forward_psi_only_ms": f_ms,
+                   "backward_ms": b_ms, "adjoint_over_forward": b_ms / fc_ms,
+                   "note": "forward = the checkpointed forward with the star source "
+                           "(kdk_evolve); backward = chunk recompute from checkpoints + reverse "
+                           "sweep (two Poisson solves per kick); forward_psi_only = qj_kdk_step "
+                           "without the source"}
         plan_a.close()
 
     # ---------------- ensemble: 16x64^3 + 8x96^3 + 8x128^3, 256 stars each -----

@@ -138,22 +138,25 @@ int qj_kdk_gas_bh_step(qj_plan *plan, void *psi, void *rho, void *vx, void *vy,
                        double dt, int nsteps, double sigma_v, int dm_accretion,
                        double bondi_r_acc_mult, double *t_io, void *stream);
 
-/* Gradient of the psi-only KDK step (no particles; optional self-interaction
- * and static V_ext).  The reference claims differentiability (README.md:7)
- * but has no jax.grad call site; this is the reverse sweep of qj_kdk_step.
+/* Gradient of the KDK step with respect to psi (particles as a fixed source:
+ * optional self-interaction, static V_ext, and rho_s, a given density added to
+ * |psi|^2 wherever the step builds its density -- the star density of
+ * quantum-stars.py:298-299 / :315-316 with the stars held fixed; NULL for
+ * none).  The reference claims differentiability (README.md:7) but has no
+ * jax.grad call site; this is the reverse sweep of qj_kdk_step.
  * qj_kdk_forward_ckpt: advances psi by nsteps in chunks of K steps (one
  * qj_kdk_step call each) and copies psi at the start of chunk j into
  * ckpt + j (ckpt: ceil(nsteps / K) complex [nx][ny][nz] arrays).
  * qj_kdk_adjoint: g holds dL/dRe psi_T + i dL/dIm psi_T on entry and
  * dL/dRe psi_0 + i dL/dIm psi_0 on return; it recomputes each chunk from its
  * checkpoint and runs the adjoint kicks (two Poisson solves each) and drifts
- * backwards. */
+ * backwards.  v_ext and rho_s: real [nx][ny][nz] of the plan's real type. */
 int qj_kdk_forward_ckpt(qj_plan *plan, void *psi, int nsteps, int K, void *ckpt,
                         double dt, int self_interaction, const void *v_ext,
-                        void *stream);
+                        const void *rho_s, void *stream);
 int qj_kdk_adjoint(qj_plan *plan, const void *ckpt, void *g, int nsteps, int K,
                    double dt, int self_interaction, const void *v_ext,
-                   void *stream);
+                   const void *rho_s, void *stream);
 
 /* nsteps x compute_step(psi, a) of the comoving script, quantum-cosmo.py:169-196:
  * per step dt = compute_dt(a, da) (:149-162, evaluated in float64 on the

@@ -352,7 +352,8 @@ struct StepCoefs {
 
 int fused_kdk(qj_plan *P, float2 *psi, float *pos, float *vel, int n_s, double m_s, double dt,
               int nsteps, int si, const float *vext, double *diag, cudaStream_t st,
-              const StepCoefs *sc = nullptr, void *save = nullptr, float *vsave = nullptr) {
+              const StepCoefs *sc = nullptr, void *save = nullptr, float *vsave = nullptr,
+              const float *rho_src = nullptr) {
   const bool parts = n_s > 0;
   const int nb = P->nbox;  // boxes: fields [nb][nx][ny][nz], stars [nb][n_s][3]
   P->cur_stars = n_s;
@@ -377,6 +378,7 @@ int fused_kdk(qj_plan *P, float2 *psi, float *pos, float *vel, int n_s, double m
     FusedArgs a = fused_args(P, q);
     a.psi = psi;
     if (parts) set_stars(a, P);
+    a.rho_src = rho_src;
     a.half = 1;  // the passes after it read k <= n/2 of R
     QJ_TRY(launch_fused(M_DENSITY, P->n[q], a, st));
   }
@@ -418,6 +420,7 @@ int fused_kdk(qj_plan *P, float2 *psi, float *pos, float *vel, int n_s, double m
       }
       a.b_coeff = si ? (float)P->ph.b_coeff : 0.0f;
       a.v_ext = vext;
+      a.rho_src = rho_src;
       a.do_drift = last ? 0 : 1;
       if (vsave) a.v_out = vsave + (size_t)k * P->ncell;  // V of kick k (adjoint)
       if (parts) set_stars(a, P);
@@ -461,6 +464,7 @@ int fused_kdk(qj_plan *P, float2 *psi, float *pos, float *vel, int n_s, double m
           QJ_CK(cudaStreamWaitEvent(st, P->ev_parts, 0));
           set_stars(a, P);
         }
+        a.rho_src = rho_src;
         a.half = 1;  // the passes after it read k <= n/2 of R
         QJ_TRY(launch_fused(M_DRIFT_DENSITY, P->n[r], a, st));
       }
@@ -515,16 +519,17 @@ int plain_bin(qj_plan *P, const void *pos, int n, double m_s, const void *masses
 
 int plain_kdk(qj_plan *P, void *psi, void *pos, void *vel, int n_s, double m_s, double dt,
               int nsteps, int si, const void *vext, double *diag, cudaStream_t st,
-              const StepCoefs *sc = nullptr, void *save = nullptr) {
+              const StepCoefs *sc = nullptr, void *save = nullptr,
+              const void *rho_src = nullptr) {
   QJ_TRY(ensure_plain_ws(P));
   QJ_TRY(launch_diag_load(P->dbl, diag, P->amax, st));
   for (int step = 0; step < nsteps; ++step) {
     const double coef = sc ? sc->kick_half[step] : P->ph.m_per_hbar * dt / 2.0;
     const double dtk = sc ? sc->drift[step] : dt;
     for (int half = 0; half < 2; ++half) {
-      // (1/2) kick
-      QJ_TRY(plain_bin(P, pos, n_s, m_s, nullptr, P->rho_s, st));
-      QJ_TRY(plain_potential(P, psi, P->rho_s, nullptr, P->V, si, vext, st));
+      // (1/2) kick; a fixed source density (no stars) takes the stars' place
+      if (!rho_src) QJ_TRY(plain_bin(P, pos, n_s, m_s, nullptr, P->rho_s, st));
+      QJ_TRY(plain_potential(P, psi, rho_src ? rho_src : P->rho_s, nullptr, P->V, si, vext, st));
       QJ_TRY(launch_kick_plain(P->dbl, psi, P->V, coef, P->ncell, st));
       QJ_TRY(plain_accel(P, nullptr, P->amax, st));
       if (n_s > 0) {
@@ -566,19 +571,19 @@ int plain_kdk(qj_plan *P, void *psi, void *pos, void *vel, int n_s, double m_s, 
 // drift with -dt.  psi is checkpointed at chunk starts; the reverse sweep
 // recomputes each chunk forward, saving the state before every kick.
 // ---------------------------------------------------------------------------
-int kdk_chunk(qj_plan *P, void *psi, int m, double dt, int si, const void *vext, cudaStream_t st,
-              void *save, float *vsave = nullptr) {
+int kdk_chunk(qj_plan *P, void *psi, int m, double dt, int si, const void *vext,
+              const void *rho_src, cudaStream_t st, void *save, float *vsave = nullptr) {
   if (!P->tmp_diag) QJ_TRY(dev_alloc(P, &P->tmp_diag, 3 * sizeof(double)));
   QJ_CK(cudaMemsetAsync(P->tmp_diag, 0, 3 * sizeof(double), st));
   if (P->dbl)
     return plain_kdk(P, psi, nullptr, nullptr, 0, 0.0, dt, m, si, vext, (double *)P->tmp_diag, st,
-                     nullptr, save);
+                     nullptr, save, rho_src);
   return fused_kdk(P, (float2 *)psi, nullptr, nullptr, 0, 0.0, dt, m, si, (const float *)vext,
-                   (double *)P->tmp_diag, st, nullptr, save, vsave);
+                   (double *)P->tmp_diag, st, nullptr, save, vsave, (const float *)rho_src);
 }
 
 int adjoint_sweep(qj_plan *P, const void *ckpt, void *g, int nsteps, int K, double dt, int si,
-                  const void *vext, cudaStream_t st) {
+                  const void *vext, const void *rho_src, cudaStream_t st) {
   QJ_TRY(ensure_plain_ws(P));
   const size_t fb = P->ncell * P->csz;
   if (!P->adj_psi) QJ_TRY(dev_alloc(P, &P->adj_psi, fb));
@@ -596,13 +601,14 @@ int adjoint_sweep(qj_plan *P, const void *ckpt, void *g, int nsteps, int K, doub
     const int m = std::min(K, nsteps - seg * K);
     const void *c0 = (const char *)ckpt + (size_t)seg * fb;
     QJ_CK(cudaMemcpyAsync(P->adj_psi, c0, fb, cudaMemcpyDeviceToDevice, st));
-    QJ_TRY(kdk_chunk(P, P->adj_psi, m, dt, si, vext, st, P->adj_states, (float *)P->adj_V));
+    QJ_TRY(kdk_chunk(P, P->adj_psi, m, dt, si, vext, rho_src, st, P->adj_states,
+                     (float *)P->adj_V));
     for (int j = m; j >= 0; --j) {
       const void *pre = j == 0 ? c0 : (const char *)P->adj_states + (size_t)(j - 1) * fb;
       const double coef = half * ((j == 0 || j == m) ? 1.0 : 2.0);
       const void *Vj = P->V;
       if (P->dbl)
-        QJ_TRY(plain_potential(P, pre, nullptr, nullptr, P->V, si, vext, st));
+        QJ_TRY(plain_potential(P, pre, rho_src, nullptr, P->V, si, vext, st));
       else
         Vj = (const float *)P->adj_V + (size_t)j * P->ncell;
       // W = (L + b) mu: the Poisson operator without the rho_bar shift; mu
@@ -1601,7 +1607,8 @@ int qj_kdk_gas_bh_step(qj_plan *P, void *psi, void *rho, void *vx, void *vy, voi
 }
 
 int qj_kdk_forward_ckpt(qj_plan *P, void *psi, int nsteps, int K, void *ckpt, double dt,
-                        int self_interaction, const void *v_ext, void *stream) {
+                        int self_interaction, const void *v_ext, const void *rho_s,
+                        void *stream) {
   QJ_ONE_BOX(P, "qj_kdk_forward_ckpt");
   if (!P || !psi || !ckpt || nsteps <= 0 || K <= 0 || !(dt > 0)) {
     set_error("qj_kdk_forward_ckpt: bad argument");
@@ -1611,19 +1618,21 @@ int qj_kdk_forward_ckpt(qj_plan *P, void *psi, int nsteps, int K, void *ckpt, do
   const size_t fb = P->ncell * P->csz;
   for (int s0 = 0, seg = 0; s0 < nsteps; s0 += K, ++seg) {
     QJ_CK(cudaMemcpyAsync((char *)ckpt + (size_t)seg * fb, psi, fb, cudaMemcpyDeviceToDevice, st));
-    QJ_TRY(kdk_chunk(P, psi, std::min(K, nsteps - s0), dt, self_interaction, v_ext, st, nullptr));
+    QJ_TRY(kdk_chunk(P, psi, std::min(K, nsteps - s0), dt, self_interaction, v_ext, rho_s, st,
+                     nullptr));
   }
   return QJ_OK;
 }
 
 int qj_kdk_adjoint(qj_plan *P, const void *ckpt, void *g, int nsteps, int K, double dt,
-                   int self_interaction, const void *v_ext, void *stream) {
+                   int self_interaction, const void *v_ext, const void *rho_s, void *stream) {
   QJ_ONE_BOX(P, "qj_kdk_adjoint");
   if (!P || !ckpt || !g || nsteps <= 0 || K <= 0 || !(dt > 0)) {
     set_error("qj_kdk_adjoint: bad argument");
     return QJ_ERR_ARG;
   }
-  return adjoint_sweep(P, ckpt, g, nsteps, K, dt, self_interaction, v_ext, (cudaStream_t)stream);
+  return adjoint_sweep(P, ckpt, g, nsteps, K, dt, self_interaction, v_ext, rho_s,
+                       (cudaStream_t)stream);
 }
 
 int qj_kdk_step(qj_plan *P, void *psi, void *pos, void *vel, int n_s, double m_s, double dt,

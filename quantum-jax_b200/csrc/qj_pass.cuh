@@ -83,6 +83,9 @@ struct FusedArgs {
   double *phi;
   double phi_coef;
   int phi_final;
+  // a fixed density added to |psi|^2 in every density build and in the
+  // self-interaction term (single box; the star density as a given source)
+  const float *rho_src;
   // isothermal gas
   const float *grho;
   float *gv[3];
@@ -380,6 +383,11 @@ __device__ __forceinline__ double build_density(float2 (&v)[E], const FusedArgs 
 #pragma unroll
     for (int e = 0; e < E; ++e)
       v[e].x = v[e].x + a.grho[(unsigned)pp.base + (unsigned)(t + P * e) * (unsigned)a.stride];
+  }
+  if (a.rho_src) {
+#pragma unroll
+    for (int e = 0; e < E; ++e)
+      v[e].x = v[e].x + a.rho_src[(unsigned)pp.base + (unsigned)(t + P * e) * (unsigned)a.stride];
   }
   double s = 0.0;
 #pragma unroll
@@ -1004,6 +1012,10 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CO
                                       float &r = rs[2 * ((m / P) * THREADS + tid)];
                                       r = fadd_rn(r, val);
                                     });
+        if (a.rho_src) {
+#pragma unroll
+          for (int e = 0; e < E; ++e) rs[2 * (e * THREADS + tid)] += a.rho_src[gb + e * gs];
+        }
 #pragma unroll
         for (int e = 0; e < E; ++e)
           V[e] = V[e] + a.b_coeff * (ps[e].x * ps[e].x + ps[e].y * ps[e].y + rs[2 * (e * THREADS + tid)]);

@@ -62,9 +62,9 @@ SIGNATURES = {
                                                                  c_int, c_double,
                                                                  ctypes.POINTER(c_double), c_void_p]),
     "qj_kdk_forward_ckpt": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, c_double, c_int,
-                                    c_void_p, c_void_p]),
+                                    c_void_p, c_void_p, c_void_p]),
     "qj_kdk_adjoint": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_double, c_int,
-                               c_void_p, c_void_p]),
+                               c_void_p, c_void_p, c_void_p]),
     "qj_kdk_cosmo": (c_int, [c_void_p, c_void_p, ctypes.POINTER(c_double), c_double, c_double,
                              c_double, c_double, c_int, c_void_p]),
     "qj_get_potential_f32_noalloc": (c_int, [ctypes.POINTER(QjGrid), ctypes.POINTER(QjPhys),

@@ -1,7 +1,8 @@
 """The adjoint (torch.autograd.Function over qj_kdk_forward_ckpt / qj_kdk_adjoint)
 against the torch float64 autograd mirror of the step and against central finite
 differences.  Loss L = mean((|psi_T|^2 - rho_target)^2) w.r.t. the initial phase
-theta; rho_target comes from a forward run of a second seed.
+theta; rho_target comes from a forward run of a second seed.  The stars enter
+as a fixed source density rho_s (their CIC density, held fixed).
 
 Bars: plain float64 gradient rel-L2 <= 1e-9 vs the mirror; fused float32
 gradient cosine >= 0.9999 vs the mirror; finite differences (16 seeded
@@ -36,7 +37,8 @@ def setup(si=False, shape=None, L=(1.0, 1.0, 1.0)):
     return g, p, sqrt_rho, theta, dt, k_sq, rho_tgt
 
 
-def qj_grad(precision, g, p, sqrt_rho, theta, dt, rho_tgt, si=False):
+def qj_grad(precision, g, p, sqrt_rho, theta, dt, rho_tgt, si=False, rho_s=None, nsteps=NSTEPS,
+            K=K):
     import qj
     from qj.autograd import kdk_evolve
 
@@ -47,9 +49,11 @@ def qj_grad(precision, g, p, sqrt_rho, theta, dt, rho_tgt, si=False):
     th = torch.as_tensor(theta, dtype=rt, device="cuda").requires_grad_(True)
     s = torch.as_tensor(sqrt_rho, dtype=rt, device="cuda")
     tg = torch.as_tensor(rho_tgt, dtype=rt, device="cuda")
-    psiT = kdk_evolve(th, s, plan, dt, NSTEPS, K, self_interaction=si)
+    src = None if rho_s is None else torch.as_tensor(rho_s, dtype=rt, device="cuda")
+    psiT = kdk_evolve(th, s, plan, dt, nsteps, K, self_interaction=si, rho_s=src)
     L = torch.mean((torch.abs(psiT) ** 2 - tg) ** 2)
     L.backward()
+    plan.status()
     return plan, float(L.detach()), th.grad.double().cpu().numpy()
 
 
@@ -121,3 +125,86 @@ def test_adjoint_noncubic_f32():
     assert L32 == pytest.approx(L_ref, rel=1e-4)
     assert cos(g32, g_ref) >= 0.9999
     assert O.rel_l2(g32, g_ref) < 1e-2
+
+
+@pytest.mark.parametrize("si", [False, True])
+def test_adjoint_with_fixed_star_density(si):
+    """The star density as a fixed source in every kick's potential: both
+    precisions against the mirror with the same source."""
+    import qj
+
+    g, p, s, th, dt, k_sq, _ = setup(si)
+    _, pos, _, _, ps = O.stars_ic(N, 64, seed=5)
+    rho_s = O.bin_stars(pos, g, np.full(len(pos), ps.m_s))
+    psi2, *_ = O.stars_ic(N, 0, seed=1)
+    tgt = (torch.abs(TM.kdk(torch.as_tensor(psi2), k_sq, p.G, p.rho_bar, p.m_per_hbar, dt, NSTEPS,
+                            p.b_coeff, rho_s=torch.as_tensor(rho_s))) ** 2).numpy()
+    L_ref, g_ref = TM.loss_and_grad(th, s, tgt, k_sq, p.G, p.rho_bar, p.m_per_hbar, dt, NSTEPS,
+                                    p.b_coeff, rho_s=rho_s)
+    plan, L64, g64 = qj_grad(qj.PLAIN_F64, g, p, s, th, dt, tgt, si, rho_s=rho_s)
+    plan.close()
+    assert L64 == pytest.approx(L_ref, rel=1e-10)
+    assert O.rel_l2(g64, g_ref) < 1e-9
+    plan, L32, g32 = qj_grad(qj.FUSED_F32, g, p, s, th, dt, tgt, si, rho_s=rho_s)
+    plan.close()
+    assert L32 == pytest.approx(L_ref, rel=1e-4)
+    assert cos(g32, g_ref) >= 0.9999
+
+
+def test_adjoint_config3_128cube_200_steps():
+    """The adjoint configuration at its own size: 128^3, 200 KDK steps, psi
+    checkpointed every 20 steps, the IC family with 4096 stars as a fixed
+    source density, target |psi_T|^2 of a forward run from a second seed, loss
+    mean((|psi_T|^2 - rho_target)^2) w.r.t. the initial phase theta (float32
+    128^3).  The single-precision adjoint gradient against the float64 one
+    (cosine >= 0.9999); central finite differences of the float64 forward
+    along 16 seeded directions (eps = 1e-3) against the directional
+    derivatives of both (cosine >= 0.9999)."""
+    import qj
+    from qj.autograd import kdk_evolve
+
+    n, steps, kc = 128, 200, 20
+    psi, pos, _, g, p = O.stars_ic(n, 4096, seed=0)
+    rho_s = O.bin_stars(pos, g, np.full(len(pos), p.m_s))
+    s = np.abs(psi)
+    th = 0.5 * O.delta_field(n, 21)
+    dt = O.default_dt(g, p)
+    phys = qj.Phys(m_per_hbar=p.m_per_hbar, G=p.G, rho_bar=p.rho_bar)
+    plan64 = qj.Plan(qj.Grid(n, n, n), phys, qj.PLAIN_F64, 1)
+    src64 = torch.as_tensor(rho_s, dtype=torch.float64, device="cuda")
+    psi2, *_ = O.stars_ic(n, 0, seed=1)
+    t2 = torch.as_tensor(psi2, dtype=torch.complex128, device="cuda")
+    with torch.no_grad():
+        tgt = torch.abs(kdk_evolve(torch.angle(t2), torch.abs(t2), plan64, dt, steps, kc,
+                                   rho_s=src64)) ** 2
+    tgt = tgt.cpu().numpy()
+    plan64.close()
+    plan, L64, g64 = qj_grad(qj.PLAIN_F64, g, p, s, th, dt, tgt, rho_s=rho_s, nsteps=steps, K=kc)
+    plan32, L32, g32 = qj_grad(qj.FUSED_F32, g, p, s, th, dt, tgt, rho_s=rho_s, nsteps=steps,
+                               K=kc)
+    plan32.close()
+    print(f"config 3: L64 {L64:.6e} L32 {L32:.6e} cos(g32, g64) {cos(g32, g64):.7f}")
+    assert L32 == pytest.approx(L64, rel=1e-4)
+    assert cos(g32, g64) >= 0.9999
+    sd = torch.as_tensor(s, dtype=torch.float64, device="cuda")
+    tg = torch.as_tensor(tgt, dtype=torch.float64, device="cuda")
+
+    def loss(theta):
+        with torch.no_grad():
+            psiT = kdk_evolve(torch.as_tensor(theta, dtype=torch.float64, device="cuda"), sd, plan,
+                              dt, steps, kc, rho_s=src64)
+            return float(torch.mean((torch.abs(psiT) ** 2 - tg) ** 2))
+
+    rng = np.random.default_rng(77)
+    eps = 1e-3
+    fd, a64, a32 = [], [], []
+    for _ in range(16):
+        d = rng.standard_normal(th.shape)
+        fd.append((loss(th + eps * d) - loss(th - eps * d)) / (2 * eps))
+        a64.append(float(np.sum(g64 * d)))
+        a32.append(float(np.sum(g32 * d)))
+    plan.close()
+    fd, a64, a32 = np.array(fd), np.array(a64), np.array(a32)
+    print(f"config 3: cos(fd, a64) {cos(fd, a64):.7f} cos(fd, a32) {cos(fd, a32):.7f}")
+    assert cos(fd, a64) >= 0.9999
+    assert cos(fd, a32) >= 0.9999
