@@ -399,8 +399,16 @@ __device__ __forceinline__ double build_density(float2 (&v)[E], const FusedArgs 
 // float64 to r in [-pi/4, pi/4] with quadrant n = rint(2 theta / pi) and a
 // two-part pi/2 (Cody-Waite); sin r and cos r are their Taylor series to
 // degree 9 and 10 (truncation below 2e-10 for |r| <= pi/4), evaluated in
-// float32 by Horner's rule.
+// float32 by Horner's rule.  For |theta| < 2^-10 (the kick phase of most cells
+// at small dt) no reduction is needed: theta - theta^3/6 and 1 - theta^2/2
+// leave out terms below 2^-46 relative, far under a float32 ulp.
 __device__ __forceinline__ void sincos_reduced(double theta, float &sn, float &cs) {
+  if (fabs(theta) < 0x1p-10) {
+    const float x = (float)theta, x2 = x * x;
+    sn = x * fmaf(x2, -1.6666667163e-01f, 1.0f);
+    cs = fmaf(x2, -0.5f, 1.0f);
+    return;
+  }
   // n = the integer nearest 2 theta / pi, by adding 1.5 * 2^52 (|2 theta / pi|
   // < 2^51): the sum's low word is n in two's complement, so the quadrant
   // needs no conversion.  (A product within an ulp of a half-integer may round

@@ -4,9 +4,11 @@ The fused kick rotates psi by exp(-i theta), theta = (m / hbar)(dt / 2) V in
 float64 (quantum-stars.py:300 takes exp(-1j V dt / 2) of the complex64 field).
 The kernel reduces theta to r in [-pi/4, pi/4] in float64 (quadrant
 n = rint(2 theta / pi), two-part pi / 2) and evaluates the Taylor series of
-sin r and cos r to degree 9 / 10 in float32.  Checked here against float64
-NumPy sin / cos (an independent reference) over a sweep of theta:
-log-spaced magnitudes 1e-3 .. 1e3 of both signs, every multiple of pi / 4 up
+sin r and cos r to degree 9 / 10 in float32; below |theta| = 2^-10 it takes
+sin ~ x (1 - x^2 / 6), cos ~ 1 - x^2 / 2 in float32 without reduction.
+Checked here against float64 NumPy sin / cos (an independent reference) over a
+sweep of theta: log-spaced magnitudes 1e-9 .. 1e3 of both signs, a dense band
+around the 2^-10 switch, every multiple of pi / 4 up
 to |theta| = 1000 with offsets of 0, 1e-12, 1e-7 and 1e-4 (the quadrant
 boundaries), and uniform random values.
 
@@ -26,7 +28,7 @@ pytestmark = pytest.mark.gpu
 
 
 def thetas():
-    mag = np.logspace(-3, 3, 200001)
+    mag = np.concatenate([np.logspace(-9, 3, 300001), 2.0 ** -10 * (1 + np.linspace(-1e-6, 1e-6, 201))])
     k = np.arange(-1273, 1274)
     offs = np.array([0.0, 1e-12, -1e-12, 1e-7, -1e-7, 1e-4, -1e-4])
     near = (k[:, None] * (np.pi / 4) + offs[None, :]).ravel()
