@@ -43,6 +43,25 @@ def max_over_ranks(x: float, dist=None, device=None) -> float:
     return float(t.item())
 
 
+def gather_box_records(records, dist=None):
+    """End-of-run gather of per-box scalar diagnostics.  records: this rank's
+    list of dicts, each with an integer "box" (the box's index in the whole
+    ensemble).  Every rank gets all ranks' records ordered by box; a box
+    reported by two ranks is an error (the partition gives each box to one
+    rank).  One all_gather_object, after the timed region."""
+    mine = [dict(r) for r in records]
+    if dist is None:
+        parts = [mine]
+    else:
+        parts = [None] * dist.get_world_size()
+        dist.all_gather_object(parts, mine)
+    out = sorted((r for p in parts for r in p), key=lambda r: r["box"])
+    boxes = [r["box"] for r in out]
+    if len(set(boxes)) != len(boxes):
+        raise ValueError("gather_box_records: a box was reported by more than one rank")
+    return out
+
+
 def box_cost(n_cells: int) -> float:
     """Relative cost of one box step: C log C (FFT-dominated)."""
     return n_cells * math.log2(max(n_cells, 2))

@@ -1,8 +1,8 @@
 """Multi-process host logic on CPU (gloo, world size 2): the max-over-ranks
-timing, the box partition every rank computes identically, the
-reference arm's rank-0-only output, and a rank that leaves: the other rank's
-next collective ends with an error within the short process-group timeout
-instead of waiting for good."""
+timing, the box partition every rank computes identically, the end-of-run
+gather of per-box diagnostics, the reference arm's rank-0-only output, and a
+rank that leaves: the other rank's next collective ends with an error within
+the short process-group timeout instead of waiting for good."""
 
 import os
 import socket
@@ -46,9 +46,15 @@ def _worker(rank, world, port, out):
     mine = qd.partition_boxes(costs, world)[rank]
     allp = [None] * world
     d.all_gather_object(allp, mine)
+    recs = qd.gather_box_records([{"box": i, "rank": rank, "err": 1e-7 * i} for i in mine], d)
+    dup = None
+    try:  # a box claimed by both ranks is refused on both
+        qd.gather_box_records([{"box": 0, "rank": rank}], d)
+    except ValueError as e:
+        dup = str(e)
     d.barrier()
     d.destroy_process_group()
-    out.put((rank, m, allp))
+    out.put((rank, m, allp, recs, dup))
 
 
 @pytest.mark.timeout(120)
@@ -63,9 +69,13 @@ def test_two_gloo_ranks_agree():
     for p in procs:
         p.join(30)
         assert p.exitcode == 0
-    (r0, m0, a0), (r1, m1, a1) = res
+    (r0, m0, a0, g0, d0), (r1, m1, a1, g1, d1) = res
     assert m0 == m1 == 2.5
     assert a0 == a1 and sorted(a0[0] + a0[1]) == list(range(32))
+    # the per-box diagnostics gather: every box once, in box order, on both ranks
+    assert g0 == g1 and [r["box"] for r in g0] == list(range(32))
+    assert all(r["rank"] == (0 if r["box"] in a0[0] else 1) for r in g0)
+    assert d0 and d1 and "more than one rank" in d0
 
 
 def test_reference_arm_prints_only_on_rank_zero():

@@ -92,6 +92,48 @@ def test_ensemble_graph_matches_eager_and_oracle():
         pl.close()
 
 
+def test_ensemble_every_box_of_the_32_box_mix():
+    """The 32-box mix (16 x 64^3, 8 x 96^3, 8 x 128^3, 256 stars each), 10
+    graph-captured steps: every box against the plain float64 path (itself
+    matched to the oracle), and the first 128^3 box against the float64
+    oracle directly."""
+    import qj
+
+    groups = [boxes(64, range(100, 116), 256), boxes(96, range(116, 124), 256),
+              boxes(128, range(124, 132), 256)]
+    state = [tensors(bx) for bx in groups]
+    plans = [plan_for(bx, len(bx)) for bx in groups]
+    ens = qj.Ensemble(plans)
+    nsteps = 10
+    m_s = [bx[0][4].m_s for bx in groups]
+    ens.step([s[0] for s in state], [s[1] for s in state], [s[2] for s in state],
+             [s[3] for s in state], [s[4] for s in state], m_s, nsteps, chunk=5, graph=True)
+    torch.cuda.synchronize()
+    for bx, s, ms in zip(groups, state, m_s):
+        g, p = bx[0][3], bx[0][4]
+        pl64 = qj.Plan(qj.Grid(g.nx, g.ny, g.nz),
+                       qj.Phys(m_per_hbar=1.0, G=p.G, rho_bar=p.rho_bar), qj.PLAIN_F64, 256)
+        for b, (psi0, pos0, vel0, _, _) in enumerate(bx):
+            ps = torch.as_tensor(psi0, dtype=torch.complex128, device="cuda")
+            po = torch.as_tensor(pos0, dtype=torch.float64, device="cuda")
+            ve = torch.as_tensor(vel0, dtype=torch.float64, device="cuda")
+            d = torch.tensor([0.0, 0.0, s[4]], dtype=torch.float64, device="cuda")
+            pl64.kdk_step(ps, po, ve, d, s[4], nsteps, ms)
+            torch.cuda.synchronize()
+            got = s[0][b].to(torch.complex128)
+            err = float(torch.linalg.vector_norm(got - ps) / torch.linalg.vector_norm(ps))
+            assert err < 1e-5, (g.nx, b, err)
+            assert O.rel_l2(s[1][b].double().cpu().numpy(), po.cpu().numpy()) < 1e-5
+        pl64.close()
+    psi0, pos0, vel0, g, p = groups[2][0]
+    ref = O.stars_run(psi0, pos0, vel0, nsteps, g, p, state[2][4])
+    assert O.rel_l2(state[2][0][0].cpu().numpy(), ref[0]) < 1e-5
+    assert O.rel_l2(state[2][1][0].cpu().numpy(), ref[1]) < 1e-5
+    ens.close()
+    for pl in plans:
+        pl.close()
+
+
 @pytest.mark.parametrize("dbl", [False, True])
 def test_fft_radix3_length_96(dbl):
     import qj
