@@ -266,16 +266,33 @@ int qj_hydro_cfl_dt(qj_plan *plan, const void *vx, const void *vy, const void *v
  *           6 drift + density, 7 deposit); 0 = the occupancy maximum.
  *   [8]     CTA slots the passes leave free for the star stream; -1 = 2.
  *   [9]     threads per block of the hydro kernels; 0 = 256.
- * Tuning changes launch shapes only: results are bit-identical for every
- * setting.  qj_autotune_kdk times qj_kdk_step on a copy of the given state
- * (probe_steps steps per trial; psi/pos/vel are not modified) and keeps the
- * fastest setting of [0..8] in the plan.  No reference counterpart (XLA picks
- * its own launch shapes). */
-#define QJ_TUNE_N 10
+ *   [10]    FFT radix plan of the passes along axes of length 128 and 256,
+ *           a bit mask: bit m = pass m of [0..6] along x or y, bit 8 + m =
+ *           pass m along z (the first density build follows bits 6 and 14):
+ *           0 = 16 elements per thread (radix 16 x 16 for 256, 16 x 8 for
+ *           128), 1 = 8 elements per thread (8 x 8 x 4, and 8 x 4 x 4), twice
+ *           the threads per pencil.
+ *   [11]    pencil tile of those passes, a bit mask like [10]: 0 = a CTA holds
+ *           256 threads' worth of z pencils, or a 16-column tile of x / y
+ *           pencils; 1 = half of that (128 threads' worth, 8 columns).
+ * [0..9] change launch shapes only: results are bit-identical for every
+ * setting.  [10] and [11] change the order of the floating-point work (the
+ * transforms' rounding, the grouping of the density's partial sums): results
+ * stay within the single-precision bars, not bit for bit.
+ * qj_autotune_kdk times qj_kdk_step on a copy of the given state (probe_steps
+ * steps per trial; psi/pos/vel are not modified) and keeps the fastest
+ * setting in the plan: with QJ_AUTOTUNE_SHAPES in flags it first picks, per
+ * pass and orientation, the radix plan and tile ([10], [11]) among the four
+ * combinations, then, as without it, the CTA counts [0..8].  No reference counterpart (XLA
+ * picks its own launch shapes and FFT plans). */
+#define QJ_TUNE_N 12
+#define QJ_TUNE_RADIX 10
+#define QJ_TUNE_TILE 11
+#define QJ_AUTOTUNE_SHAPES 1
 int qj_plan_get_tuning(const qj_plan *plan, int32_t *tune, int n);
 int qj_plan_set_tuning(qj_plan *plan, const int32_t *tune, int n);
 int qj_autotune_kdk(qj_plan *plan, const void *psi, const void *pos, const void *vel, int n_s,
-                    double m_s, double dt, int probe_steps, void *stream);
+                    double m_s, double dt, int probe_steps, int flags, void *stream);
 
 /* qj_plan_status: waits for the device, then returns QJ_ERR_TIMEOUT (and
  * clears the flag) if a fused pass of this plan gave up a bounded wait for

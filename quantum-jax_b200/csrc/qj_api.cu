@@ -119,6 +119,7 @@ struct qj_plan {
   // tables
   void *tw[3] = {nullptr, nullptr, nullptr};  // float2 / double2
   float2 *tws[3] = {nullptr, nullptr, nullptr};  // stage twiddle tables (fused passes)
+  float2 *tws_alt[3] = {nullptr, nullptr, nullptr};  // the same for radix plan 1 (n = 128, 256)
   double *kd[3] = {nullptr, nullptr, nullptr};
   float *kf[3] = {nullptr, nullptr, nullptr};
   float *ktf[3] = {nullptr, nullptr, nullptr};
@@ -150,7 +151,7 @@ struct qj_plan {
   void *facc_bh = nullptr;
   double *facc_scal = nullptr, *facc_part = nullptr;
   long long *facc_pi = nullptr;
-  int tune[QJ_TUNE_N] = {0, 0, 0, 0, 0, 0, 0, 0, -1, 0};  // launch tuning (include/qj.h)
+  int tune[QJ_TUNE_N] = {0, 0, 0, 0, 0, 0, 0, 0, -1, 0, 0, 0};  // launch tuning (include/qj.h)
   void *tmp_scalar = nullptr;
   void *tmp_diag = nullptr;
   void *gas_prim = nullptr;  // hydro: 16 values per cell as 4 quads (predicted primitives, gradients by axis)
@@ -240,7 +241,9 @@ int fft3d(qj_plan *P, void *data, int dir, cudaStream_t st) {
   return 0;
 }
 
-FusedArgs fused_args(const qj_plan *P, int axis) {
+// Arguments of a pass of `mode` along `axis`, in the plan's shape variant of
+// that pass (qj.h QJ_TUNE_RADIX / QJ_TUNE_TILE).
+FusedArgs fused_args(const qj_plan *P, int axis, int mode) {
   FusedArgs a;
   std::memset(&a, 0, sizeof(a));
   a.nx = P->n[0];
@@ -249,12 +252,13 @@ FusedArgs fused_args(const qj_plan *P, int axis) {
   a.axis = axis;
   a.stride = axis == 0 ? (long long)P->n[1] * P->n[2] : (axis == 1 ? P->n[2] : 1);
   a.outer_stride = axis == 0 ? P->n[2] : (long long)P->n[1] * P->n[2];
-  a.ztiles = P->n[2] / 16;
+  a.shape = shape_of(P->n[axis], P->tune, mode, axis == 2);
+  a.ztiles = P->n[2] / strided_tile_width(a.shape);
   a.full_nx = P->n[0];
   a.R = P->R;
   a.S1 = P->S1;
   a.S2 = P->S2;
-  a.tw = P->tws[axis];
+  a.tw = (a.shape & 1) ? P->tws_alt[axis] : P->tws[axis];
   a.prop = P->prop[axis];
   for (int d = 0; d < 3; ++d) {
     a.k[d] = P->kf[d];
@@ -290,13 +294,19 @@ void set_stars(FusedArgs &a, const qj_plan *P) {
 // axis q (0 or 2), the axis its first forward transform ran along: the density
 // is real, so k_q > n_q / 2 follows from k_q < n_q / 2 (the Poisson pass writes
 // those as mirrors).  x: the first n/2 + 1 planes; z: the 16-wide tiles that
-// hold k_z <= n/2.
+// hold k_z <= n/2 (16 or, in the narrow tile variant, 8 wide).
 void half_spectrum(FusedArgs &a, const qj_plan *P, int q) {
   a.hq = q;
-  if (q == 0)
+  if (q == 0) {
     a.nx = P->n[0] / 2 + 1;
-  else
-    a.ztiles = (P->n[2] / 2 + 1 + 15) / 16;
+  } else {
+    const int w = strided_tile_width(a.shape);
+    a.ztiles = (P->n[2] / 2 + 1 + w - 1) / w;
+  }
+}
+// Partial sums the density pass along q wrote (one per tile).
+int density_parts(const qj_plan *P, int q) {
+  return pass_blocks(P->n[q], q, P->n[0], P->n[1], P->n[2], shape_of(P->n[q], P->tune, M_DRIFT_DENSITY, q == 2));
 }
 
 int ensure_prop(qj_plan *P, double dtk, cudaStream_t st) {
@@ -375,7 +385,7 @@ int fused_kdk(qj_plan *P, float2 *psi, float *pos, float *vel, int n_s, double m
     if (prof_on()) prof_mark_end(7, st);
   }
   {
-    FusedArgs a = fused_args(P, q);
+    FusedArgs a = fused_args(P, q, M_DENSITY);
     a.psi = psi;
     if (parts) set_stars(a, P);
     a.rho_src = rho_src;
@@ -387,16 +397,16 @@ int fused_kdk(qj_plan *P, float2 *psi, float *pos, float *vel, int n_s, double m
     const bool last = (k == nsteps);
     if (!last) QJ_TRY(ensure_prop(P, drift_dt(k), st));
     {
-      FusedArgs a = fused_args(P, 1);
+      FusedArgs a = fused_args(P, 1, M_FFT_FWD);
       half_spectrum(a, P, q);
       QJ_TRY(launch_fused(M_FFT_FWD, P->n[1], a, st));
     }
     {
-      FusedArgs a = fused_args(P, r);
+      FusedArgs a = fused_args(P, r, M_POISSON);
       a.half = 1;
       half_spectrum(a, P, q);
       a.part_in = P->part;
-      a.n_part = pass_blocks(P->n[q], q, P->n[0], P->n[1], P->n[2]);
+      a.n_part = density_parts(P, q);
       if (use_phi) {
         a.phi = P->phi;
         a.phi_coef = kick_coef(k, last);
@@ -404,13 +414,13 @@ int fused_kdk(qj_plan *P, float2 *psi, float *pos, float *vel, int n_s, double m
       QJ_TRY(launch_fused(M_POISSON, P->n[r], a, st));
     }
     {
-      FusedArgs a = fused_args(P, 1);
+      FusedArgs a = fused_args(P, 1, M_IFFT2);
       a.half = 1;
       half_spectrum(a, P, q);
       QJ_TRY(launch_fused(M_IFFT2, P->n[1], a, st));
     }
     {
-      FusedArgs a = fused_args(P, q);
+      FusedArgs a = fused_args(P, q, M_KICK);
       a.psi = psi;
       // kick k = second half kick of step k-1 and first half kick of step k
       a.kick_coef = kick_coef(k, last);
@@ -453,12 +463,12 @@ int fused_kdk(qj_plan *P, float2 *psi, float *pos, float *vel, int n_s, double m
     }
     if (!last) {
       {
-        FusedArgs a = fused_args(P, 1);
+        FusedArgs a = fused_args(P, 1, M_DRIFT);
         a.psi = psi;
         QJ_TRY(launch_fused(M_DRIFT, P->n[1], a, st));
       }
       {
-        FusedArgs a = fused_args(P, r);
+        FusedArgs a = fused_args(P, r, M_DRIFT_DENSITY);
         a.psi = psi;
         if (parts) {
           QJ_CK(cudaStreamWaitEvent(st, P->ev_parts, 0));
@@ -629,7 +639,7 @@ int adjoint_sweep(qj_plan *P, const void *ckpt, void *g, int nsteps, int K, doub
           // the separable drift as three fused forward-multiply-inverse passes
           QJ_TRY(ensure_prop(P, -dt, st));
           for (int ax = 0; ax < 3; ++ax) {
-            FusedArgs a = fused_args(P, ax);
+            FusedArgs a = fused_args(P, ax, M_DRIFT);
             a.psi = (float2 *)g;
             QJ_TRY(launch_fused(M_DRIFT, P->n[ax], a, st));
           }
@@ -683,24 +693,24 @@ int fused_gas_step(qj_plan *P, const GasArgs &g, cudaStream_t st, bool first, bo
     }
   };
   auto poisson = [&](int q, int r) -> int {
-    FusedArgs a = fused_args(P, 1);
+    FusedArgs a = fused_args(P, 1, M_FFT_FWD);
     half_spectrum(a, P, q);
     QJ_TRY(launch_fused(M_FFT_FWD, P->n[1], a, st));
-    a = fused_args(P, r);
+    a = fused_args(P, r, M_POISSON);
     a.half = 1;
     half_spectrum(a, P, q);
     a.part_in = P->part;
-    a.n_part = pass_blocks(P->n[q], q, P->n[0], P->n[1], P->n[2]);
+    a.n_part = density_parts(P, q);
     a.phi = P->phi;
     a.phi_coef = half;
     QJ_TRY(launch_fused(M_POISSON, P->n[r], a, st));
-    a = fused_args(P, 1);
+    a = fused_args(P, 1, M_IFFT2);
     a.half = 1;
     half_spectrum(a, P, q);
     return launch_fused(M_IFFT2, P->n[1], a, st);
   };
   auto kick = [&](int q, int drift) -> int {
-    FusedArgs a = fused_args(P, q);
+    FusedArgs a = fused_args(P, q, M_KICK);
     a.psi = (float2 *)g.psi;
     a.kick_coef = half;
     a.do_drift = drift;
@@ -724,7 +734,7 @@ int fused_gas_step(qj_plan *P, const GasArgs &g, cudaStream_t st, bool first, bo
     QJ_TRY(stars_prepare_sort(P, g.pos, g.n_bh, g.m_bh, 0.0, 2, st));
   }
   {
-    FusedArgs a = fused_args(P, 2);
+    FusedArgs a = fused_args(P, 2, M_DENSITY);
     a.psi = (float2 *)g.psi;
     stars(a);
     a.half = 1;  // the passes after it read k <= n/2 of R
@@ -739,7 +749,7 @@ int fused_gas_step(qj_plan *P, const GasArgs &g, cudaStream_t st, bool first, bo
     QJ_TRY(launch_update_fused(g.pos, g.vel, geom(P), u, P->sb, st));
   }
   {
-    FusedArgs a = fused_args(P, 1);
+    FusedArgs a = fused_args(P, 1, M_DRIFT);
     a.psi = (float2 *)g.psi;
     QJ_TRY(launch_fused(M_DRIFT, P->n[1], a, st));
   }
@@ -752,7 +762,7 @@ int fused_gas_step(qj_plan *P, const GasArgs &g, cudaStream_t st, bool first, bo
     QJ_TRY(stars_prepare_sort(P, g.pos, g.n_bh, g.m_bh, 0.0, 0, st));
   }
   {
-    FusedArgs a = fused_args(P, 0);
+    FusedArgs a = fused_args(P, 0, M_DRIFT_DENSITY);
     a.psi = (float2 *)g.psi;
     stars(a);
     a.half = 1;  // the passes after it read k <= n/2 of R
@@ -935,6 +945,13 @@ int qj_plan_create_batched(qj_plan **plan, const qj_grid *grid, const qj_phys *p
       if (e == cudaSuccess && !(rc = dev_alloc_t(P, &P->tws[a], ts.size())))
         e = cudaMemcpy(P->tws[a], ts.data(), ts.size() * sizeof(float2), cudaMemcpyHostToDevice);
       if (rc) break;
+      if (has_radix_variant(N)) {
+        const std::vector<float2> ta = stage_twiddles(N, 1);
+        if (e == cudaSuccess && !(rc = dev_alloc_t(P, &P->tws_alt[a], ta.size())))
+          e = cudaMemcpy(P->tws_alt[a], ta.data(), ta.size() * sizeof(float2),
+                         cudaMemcpyHostToDevice);
+        if (rc) break;
+      }
     }
     if (e != cudaSuccess) rc = cuda_fail(e, "cudaMemcpy(twiddles)", __FILE__, __LINE__);
   }
@@ -944,8 +961,9 @@ int qj_plan_create_batched(qj_plan **plan, const qj_grid *grid, const qj_phys *p
     if ((rc = dev_alloc_t(P, &P->R, P->ncell * nbox))) return fail(rc);
     if ((rc = dev_alloc_t(P, &P->S1, P->ncell * nbox))) return fail(rc);
     if ((rc = dev_alloc_t(P, &P->S2, P->ncell * nbox))) return fail(rc);
-    int nb = 0;
-    for (int a = 0; a < 3; ++a) nb = std::max(nb, pass_blocks(n[a], a, n[0], n[1], n[2]));
+    int nb = 0;  // partial sums of a density pass, over every shape variant
+    for (int a = 0; a < 3; ++a)
+      for (int v = 0; v < 4; ++v) nb = std::max(nb, pass_blocks(n[a], a, n[0], n[1], n[2], v));
     P->part_stride = nb;
     if ((rc = dev_alloc_t(P, &P->part, (size_t)nb * nbox))) return fail(rc);
   } else {
@@ -1280,18 +1298,27 @@ int qj_plan_set_tuning(qj_plan *P, const int32_t *tune, int n) {
     set_error("qj_plan_set_tuning: reserve must be -1..64, hydro block 0/64/128/256");
     return QJ_ERR_ARG;
   }
+  if ((tune[QJ_TUNE_RADIX] & ~0x7f7f) != 0 || (tune[QJ_TUNE_TILE] & ~0x7f7f) != 0) {
+    set_error("qj_plan_set_tuning: radix plan and tile variant are bit masks over passes 0..6 "
+              "(strided) and 8..14 (contiguous)");
+    return QJ_ERR_ARG;
+  }
   for (int i = 0; i < QJ_TUNE_N; ++i) P->tune[i] = tune[i];
   return QJ_OK;
 }
 
-// Coordinate search over the launch tuning of the fused step: per pass, the
-// CTAs per SM (1 .. occupancy maximum); then the reserved CTA slots.  Each
-// trial runs probe_steps steps of qj_kdk_step on a scratch copy of the state
-// (the caller's arrays are only read) and takes the faster of two timings.
+// Coordinate search over the launch tuning of the fused step.  With
+// QJ_AUTOTUNE_SHAPES (and an axis of length 128 or 256): first, per pass and
+// orientation (strided x / y, contiguous z), the radix plan and tile variant
+// (the four combinations).  Then, per pass, the CTAs per SM (1 .. the
+// occupancy maximum of its chosen shapes); then the reserved CTA slots.
+// Each trial runs probe_steps steps of qj_kdk_step on a scratch copy of the
+// state (the caller's arrays are only read) and takes the faster of two
+// timings.
 int qj_autotune_kdk(qj_plan *P, const void *psi, const void *pos, const void *vel, int n_s,
-                    double m_s, double dt, int probe_steps, void *stream) {
+                    double m_s, double dt, int probe_steps, int flags, void *stream) {
   if (!P || !psi || n_s < 0 || (n_s > 0 && (!pos || !vel)) || probe_steps < 1 ||
-      !(dt > 0) || n_s > P->max_particles) {
+      !(dt > 0) || n_s > P->max_particles || (flags & ~QJ_AUTOTUNE_SHAPES) != 0) {
     set_error("qj_autotune_kdk: bad argument");
     return QJ_ERR_ARG;
   }
@@ -1327,9 +1354,9 @@ int qj_autotune_kdk(qj_plan *P, const void *psi, const void *pos, const void *ve
     diag0[3 * b + 1] = 0.0;
     diag0[3 * b + 2] = dt;
   }
-  auto trial = [&](float &ms) -> int {
+  auto trial = [&](float &ms, int reps) -> int {
     float best = 1e30f;
-    for (int rep = 0; rep < 2; ++rep) {
+    for (int rep = 0; rep < reps; ++rep) {
       QJ_CK(cudaMemcpyAsync(s_psi, psi, psi_b, cudaMemcpyDeviceToDevice, st));
       if (n_s > 0) {
         QJ_CK(cudaMemcpyAsync(s_pos, pos, par_b, cudaMemcpyDeviceToDevice, st));
@@ -1349,22 +1376,81 @@ int qj_autotune_kdk(qj_plan *P, const void *psi, const void *pos, const void *ve
     ms = best;
     return 0;
   };
-  const int saved[QJ_TUNE_N] = {P->tune[0], P->tune[1], P->tune[2], P->tune[3], P->tune[4],
-                                P->tune[5], P->tune[6], P->tune[7], P->tune[8], P->tune[9]};
+  int saved[QJ_TUNE_N];
+  for (int i = 0; i < QJ_TUNE_N; ++i) saved[i] = P->tune[i];
   float best_ms = 0.f;
-  if ((rc = trial(best_ms)) == 0 && (rc = trial(best_ms)) == 0) {  // warm-up, then baseline
+  if ((rc = trial(best_ms, 2)) == 0 && (rc = trial(best_ms, 2)) == 0) {  // warm-up, then baseline
+    bool variants = false;
+    for (int ax = 0; ax < 3; ++ax) variants = variants || has_radix_variant(P->n[ax]);
     const int modes[] = {M_FFT_FWD, M_POISSON, M_IFFT2, M_KICK, M_DRIFT, M_DRIFT_DENSITY};
+    if ((flags & QJ_AUTOTUNE_SHAPES) && variants) {
+      // per pass and orientation, each radix plan / tile combination at the
+      // current CTA counts (a combination's first trial also sets up its
+      // kernels: the second one, the best of three runs, counts).  A single
+      // pass changes the step by a fraction of a percent, so a combination
+      // is kept when it is 0.3 % faster.  The y-only passes have no
+      // contiguous form.
+      const int shapes0[2] = {P->tune[QJ_TUNE_RADIX], P->tune[QJ_TUNE_TILE]};
+      float shape_ms = 0.f;
+      rc = trial(shape_ms, 3);
+      for (int mb = 0; mb < 2 * 6 && rc == 0; ++mb) {
+        const int m = modes[mb % 6];
+        const bool contig = mb >= 6;
+        if (contig && (m == M_FFT_FWD || m == M_IFFT2)) continue;
+        const int bit = 1 << (m + (contig ? 8 : 0));
+        auto shape_now = [&] {
+          return ((P->tune[QJ_TUNE_RADIX] & bit) ? 1 : 0) | ((P->tune[QJ_TUNE_TILE] & bit) ? 2 : 0);
+        };
+        auto set_shape = [&](int v) {
+          P->tune[QJ_TUNE_RADIX] = (P->tune[QJ_TUNE_RADIX] & ~bit) | ((v & 1) ? bit : 0);
+          P->tune[QJ_TUNE_TILE] = (P->tune[QJ_TUNE_TILE] & ~bit) | ((v & 2) ? bit : 0);
+        };
+        const int cur = shape_now();
+        int best_v = cur;
+        for (int v = 0; v < 4 && rc == 0; ++v) {
+          if (v == cur) continue;
+          set_shape(v);
+          float t = 0.f;
+          if ((rc = trial(t, 1)) == 0 && (rc = trial(t, 3)) == 0 && t < 0.997f * shape_ms) {
+            shape_ms = t;
+            best_v = v;
+          }
+        }
+        set_shape(best_v);
+      }
+      // the chosen shapes against the starting ones, in alternating longer
+      // runs, so that picks made on noise do not add up
+      const int chosen[2] = {P->tune[QJ_TUNE_RADIX], P->tune[QJ_TUNE_TILE]};
+      if (rc == 0 && (chosen[0] != shapes0[0] || chosen[1] != shapes0[1])) {
+        float t_new = 1e30f, t_old = 1e30f;
+        for (int r = 0; r < 3 && rc == 0; ++r) {
+          float t = 0.f;
+          P->tune[QJ_TUNE_RADIX] = shapes0[0];
+          P->tune[QJ_TUNE_TILE] = shapes0[1];
+          if ((rc = trial(t, 2)) == 0) t_old = std::min(t_old, t);
+          P->tune[QJ_TUNE_RADIX] = chosen[0];
+          P->tune[QJ_TUNE_TILE] = chosen[1];
+          if (rc == 0 && (rc = trial(t, 2)) == 0) t_new = std::min(t_new, t);
+        }
+        const bool keep = t_new < 0.997f * t_old;
+        P->tune[QJ_TUNE_RADIX] = keep ? chosen[0] : shapes0[0];
+        P->tune[QJ_TUNE_TILE] = keep ? chosen[1] : shapes0[1];
+      }
+      if (rc == 0) rc = trial(best_ms, 2);  // the CTA search's baseline
+    }
     for (int m : modes) {
-      // occupancy of the pass over both orientations it runs in
+      // occupancy of the pass, in the chosen shape, over both orientations it runs in
       int kmax = 0;
-      for (int ax = 0; ax < 3; ++ax) kmax = std::max(kmax, fused_max_ctas_per_sm(m, P->n[ax], ax == 2));
+      for (int ax = 0; ax < 3; ++ax)
+        kmax = std::max(kmax, fused_max_ctas_per_sm(m, P->n[ax], ax == 2,
+                                                    shape_of(P->n[ax], P->tune, m, ax == 2)));
       const int cur = P->tune[m];
       int best_k = cur;
       for (int k = 1; k <= kmax && rc == 0; ++k) {
         if (k == cur || (cur == 0 && k == kmax)) continue;
         P->tune[m] = k;
         float t = 0.f;
-        if ((rc = trial(t)) == 0 && t < 0.99f * best_ms) {
+        if ((rc = trial(t, 2)) == 0 && t < 0.99f * best_ms) {
           best_ms = t;
           best_k = k;
         }
@@ -1378,7 +1464,7 @@ int qj_autotune_kdk(qj_plan *P, const void *psi, const void *pos, const void *ve
       if (r == (cur_r < 0 ? 2 : cur_r)) continue;
       P->tune[8] = r;
       float t = 0.f;
-      if ((rc = trial(t)) == 0 && t < 0.99f * best_ms) {
+      if ((rc = trial(t, 2)) == 0 && t < 0.99f * best_ms) {
         best_ms = t;
         best_r = r;
       }
@@ -1493,7 +1579,7 @@ int qj_bin_stars(qj_plan *P, const void *pos, int n, double m_s, const void *mas
   cudaStream_t st = (cudaStream_t)stream;
   if (P->dbl) return plain_bin(P, pos, n, m_s, masses, rho_s, st);
   // single precision: the pencil-bucket deposit of the fused step
-  FusedArgs a = fused_args(P, 2);
+  FusedArgs a = fused_args(P, 2, M_DEPOSIT);
   a.rho_out = (float *)rho_s;
   if (n > 0) {
     QJ_TRY(launch_stars_prepare(pos, n, masses, m_s, geom(P), 2, P->sb, st));

@@ -6,7 +6,7 @@
 // t + P * e, e = 0..E-1, both before and after the transform (natural order),
 // so a forward transform, a pointwise multiply and an inverse transform chain
 // in registers.  The transform is a Stockham autosort decimation in time over
-// the radices of FftPlan<N>; the first stage reads registers, the last stage
+// the radices of FftPlan<N, RV>; the first stage reads registers, the last stage
 // writes registers, and each stage boundary is one exchange through shared
 // memory.  Twiddles come from a table w[m] = exp(-2 pi i m / N) computed in
 // float64 on the host and rounded once to the working precision.
@@ -113,8 +113,10 @@ template <int DIR, typename C> struct Dft<3, DIR, C> {
   }
 };
 
-// Radix plans: E elements per thread, NS stages, radix(s) divides E.
-template <int N> struct FftPlan;
+// Radix plans: E elements per thread, NS stages, radix(s) divides E.  RV = 0
+// is each length's default; RV = 1 (n = 128, 256) holds half as many elements
+// per thread, so twice the threads share a pencil over one more stage.
+template <int N, int RV = 0> struct FftPlan;
 template <> struct FftPlan<16> {
   static constexpr int E = 16, NS = 1;
   __host__ __device__ static constexpr int radix(int) { return 16; }
@@ -145,10 +147,24 @@ template <> struct FftPlan<512> {
   static constexpr int E = 16, NS = 3;
   __host__ __device__ static constexpr int radix(int s) { return s == 0 ? 16 : (s == 1 ? 8 : 4); }
 };
+template <> struct FftPlan<128, 1> {  // 8 * 4 * 4, 16 threads per pencil
+  static constexpr int E = 8, NS = 3;
+  __host__ __device__ static constexpr int radix(int s) { return s == 0 ? 8 : 4; }
+};
+template <> struct FftPlan<256, 1> {  // 8 * 8 * 4, 32 threads per pencil
+  static constexpr int E = 8, NS = 3;
+  __host__ __device__ static constexpr int radix(int s) { return s == 2 ? 4 : 8; }
+};
+// Lengths with a radix variant.
+__host__ __device__ constexpr bool has_radix_variant(int n) { return n == 128 || n == 256; }
+// The radix plan whose thread holds E elements of a length-N pencil.
+template <int N, int E> __host__ __device__ constexpr int radix_variant_of() {
+  return E == FftPlan<N, 0>::E ? 0 : 1;
+}
 
-template <int N> __host__ __device__ constexpr int stage_ns(int s) {
+template <int N, int RV = 0> __host__ __device__ constexpr int stage_ns(int s) {
   int ns = 1;
-  for (int i = 0; i < s; ++i) ns *= FftPlan<N>::radix(i);
+  for (int i = 0; i < s; ++i) ns *= FftPlan<N, RV>::radix(i);
   return ns;
 }
 
@@ -178,26 +194,26 @@ template <typename C> struct SmemContig {
 // stages are concatenated.  A thread reads its row two twiddles at a time
 // (16-byte loads); the row length is 2 mod 4 entries, so eight consecutive
 // rows start on eight different bank quads (conflict-free 16-byte loads).
-template <int N> __host__ __device__ constexpr int tw_row(int s) {
-  int L = FftPlan<N>::radix(s) - 1;
+template <int N, int RV = 0> __host__ __device__ constexpr int tw_row(int s) {
+  int L = FftPlan<N, RV>::radix(s) - 1;
   while (L % 4 != 2) ++L;
   return L;
 }
-template <int N> __host__ __device__ constexpr int stage_tw_off(int s) {
+template <int N, int RV = 0> __host__ __device__ constexpr int stage_tw_off(int s) {
   int off = 0;
-  for (int i = 1; i < s; ++i) off += stage_ns<N>(i) * tw_row<N>(i);
+  for (int i = 1; i < s; ++i) off += stage_ns<N, RV>(i) * tw_row<N, RV>(i);
   return off;
 }
-template <int N> __host__ __device__ constexpr int stage_tw_size() {
-  return stage_tw_off<N>(FftPlan<N>::NS);
+template <int N, int RV = 0> __host__ __device__ constexpr int stage_tw_size() {
+  return stage_tw_off<N, RV>(FftPlan<N, RV>::NS);
 }
 
-template <int N, int DIR, int S, typename C, class SM, bool TWS> struct FftStages {
-  using PL = FftPlan<N>;
+template <int N, int DIR, int S, typename C, class SM, bool TWS, int RV> struct FftStages {
+  using PL = FftPlan<N, RV>;
   static constexpr int E = PL::E, P = N / E;
   static constexpr int r = PL::radix(S);
   static constexpr int B = E / r;
-  static constexpr int Ns = stage_ns<N>(S);
+  static constexpr int Ns = stage_ns<N, RV>(S);
   static_assert(E % r == 0, "radix must divide E");
 
   __device__ __forceinline__ static void run(C (&v)[E], int t, const SM &sm,
@@ -221,7 +237,7 @@ template <int N, int DIR, int S, typename C, class SM, bool TWS> struct FftStage
         if constexpr (TWS) {
           // two twiddles per 16-byte load from the thread's row
           const float4 *row =
-              reinterpret_cast<const float4 *>(tw + stage_tw_off<N>(S) + jm * tw_row<N>(S));
+              reinterpret_cast<const float4 *>(tw + stage_tw_off<N, RV>(S) + jm * tw_row<N, RV>(S));
 #pragma unroll
           for (int h = 0; 2 * h + 1 < r; ++h) {
             const float4 w2 = row[h];
@@ -251,26 +267,34 @@ template <int N, int DIR, int S, typename C, class SM, bool TWS> struct FftStage
         for (int q = 0; q < r; ++q) sm.st(idxD + q * Ns, v[u + q * B]);
       }
       SM::sync();
-      FftStages<N, DIR, S + 1, C, SM, TWS>::run(v, t, sm, tw);
+      FftStages<N, DIR, S + 1, C, SM, TWS, RV>::run(v, t, sm, tw);
     }
   }
 };
 
 // Transform the pencil held by the P threads of a group.  Every thread of the
 // CTA (strided) or warp (contiguous) must call this the same number of times.
-// TWS: tw is the stage twiddle table (usually in shared memory); otherwise the
-// flat table w[m] = exp(-2 pi i m / N) in global memory.
-template <int N, int DIR, bool TWS = false, typename C, class SM>
-__device__ __forceinline__ void fft_pencil(C (&v)[FftPlan<N>::E], int t, const SM &sm,
+// TWS: tw is the stage twiddle table of the radix plan (usually in shared
+// memory); otherwise the flat table w[m] = exp(-2 pi i m / N) in global
+// memory.  The radix plan follows from the thread's element count E.
+template <int N, int DIR, bool TWS = false, typename C, int E, class SM>
+__device__ __forceinline__ void fft_pencil(C (&v)[E], int t, const SM &sm,
                                            const C *__restrict__ tw) {
-  FftStages<N, DIR, 0, C, SM, TWS>::run(v, t, sm, tw);
+  constexpr int RV = radix_variant_of<N, E>();
+  static_assert(FftPlan<N, RV>::E == E, "no radix plan of this length holds E elements");
+  FftStages<N, DIR, 0, C, SM, TWS, RV>::run(v, t, sm, tw);
 }
 
-// Launch shape of a pencil pass over length N.
-template <int N, bool CONTIG> struct PassShape {
-  static constexpr int E = FftPlan<N>::E;
+// Launch shape of a pencil pass over length N.  V selects a shape variant:
+// bit 0 the radix plan (FftPlan<N, 1>), bit 1 half the pencils per CTA (a
+// contiguous tile of 128 instead of 256 threads' pencils, a strided tile 8
+// instead of 16 z columns wide).  Variants exist for has_radix_variant(N).
+template <int N, bool CONTIG, int V = 0> struct PassShape {
+  static constexpr int RV = V & 1, TV = (V >> 1) & 1;
+  static constexpr int E = FftPlan<N, RV>::E;
   static constexpr int P = N / E;
-  static constexpr int TP = CONTIG ? (P >= 256 ? 1 : 256 / P) : 16;
+  static constexpr int CT = TV ? 128 : 256;  // threads' worth of contiguous pencils
+  static constexpr int TP = CONTIG ? (P >= CT ? 1 : CT / P) : (TV ? 8 : 16);
   static constexpr int THREADS = TP * P;
   // resident CTAs per SM requested from the register allocator: enough for
   // a budget of 128 registers per thread (2 x 256, 4 x 128, ... threads)

@@ -1,4 +1,6 @@
-// Instantiations and launchers of the fused single-precision pencil passes.
+// Instantiations and launchers of the fused single-precision pencil passes
+// (default shapes of every length; the shape variants of n = 128 and 256 are
+// instantiated by qj_fused_v{1,2,3}.cu).
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -7,11 +9,7 @@
 #include <mutex>
 #include <vector>
 
-#include <cuda.h>
-#include <cudaTypedefs.h>
-
-#include "../../include/qj.h"
-#include "qj_internal.h"
+#include "qj_fused_run.cuh"
 
 namespace qj {
 
@@ -19,185 +17,69 @@ bool fft_length_supported(int n) {
   return n == 16 || n == 32 || n == 64 || n == 96 || n == 128 || n == 256 || n == 512;
 }
 
-template <int N, bool CONTIG>
-static int grid_of(const FusedArgs &a) {
-  using SH = PassShape<N, CONTIG>;
-  if (CONTIG) {
-    // a reduced range (half spectrum) rounds up to whole tiles, within the
-    // grid; the rows past it are pencils the pass does not store
-    const int full = ((a.full_nx > 0 ? a.full_nx : a.nx) * a.ny) / SH::TP;
-    return std::min(full, (a.nx * a.ny + SH::TP - 1) / SH::TP);
-  }
-  return (a.axis == 0 ? a.ny : a.nx) * a.ztiles;
-}
-
-// Stage twiddle table of length n (see stage_tw_off), long double, rounded once.
-template <int N> static std::vector<float2> stage_table() {
-  std::vector<float2> t(stage_tw_size<N>() > 0 ? stage_tw_size<N>() : 1);
-  for (int s = 1; s < FftPlan<N>::NS; ++s) {
-    const int ns = stage_ns<N>(s), r = FftPlan<N>::radix(s);
+// Stage twiddle table of length n and radix plan RV (see stage_tw_off), long
+// double, rounded once.
+template <int N, int RV> static std::vector<float2> stage_table() {
+  using PL = FftPlan<N, RV>;
+  std::vector<float2> t(stage_tw_size<N, RV>() > 0 ? stage_tw_size<N, RV>() : 1);
+  for (int s = 1; s < PL::NS; ++s) {
+    const int ns = stage_ns<N, RV>(s), r = PL::radix(s);
     for (int q = 1; q < r; ++q)
       for (int jm = 0; jm < ns; ++jm) {
         const long long m = (long long)jm * q * (N / (ns * r));
         const long double th = -2.0L * 3.14159265358979323846264338327950288L * m / N;
-        t[stage_tw_off<N>(s) + jm * tw_row<N>(s) + (q - 1)] = float2{(float)cosl(th), (float)sinl(th)};
+        t[stage_tw_off<N, RV>(s) + jm * tw_row<N, RV>(s) + (q - 1)] =
+            float2{(float)cosl(th), (float)sinl(th)};
       }
   }
   return t;
 }
 
-std::vector<float2> stage_twiddles(int n) {
+std::vector<float2> stage_twiddles(int n, int rv) {
+  if (rv) {
+    switch (n) {
+      case 128: return stage_table<128, 1>();
+      case 256: return stage_table<256, 1>();
+    }
+    return {};
+  }
   switch (n) {
-    case 16: return stage_table<16>();
-    case 32: return stage_table<32>();
-    case 64: return stage_table<64>();
-    case 96: return stage_table<96>();
-    case 128: return stage_table<128>();
-    case 256: return stage_table<256>();
-    case 512: return stage_table<512>();
+    case 16: return stage_table<16, 0>();
+    case 32: return stage_table<32, 0>();
+    case 64: return stage_table<64, 0>();
+    case 96: return stage_table<96, 0>();
+    case 128: return stage_table<128, 0>();
+    case 256: return stage_table<256, 0>();
+    case 512: return stage_table<512, 0>();
   }
   return {};
 }
 
-// Tiles (pencil groups of one CTA) of a pass along `axis` of length n_axis.
-int pass_blocks(int n_axis, int axis, int nx, int ny, int nz) {
+template <int N, int V> static int contig_tp() { return PassShape<N, true, V>::TP; }
+
+int strided_tile_width(int v) {
+  return (v & 2) ? PassShape<256, false, 2>::TP : PassShape<256, false, 0>::TP;
+}
+
+// Tiles (pencil groups of one CTA) of a pass along `axis` of length n_axis in
+// shape variant v (0 for lengths without variants).
+int pass_blocks(int n_axis, int axis, int nx, int ny, int nz, int v) {
   if (axis == 2) {
     int tp = 1;
     switch (n_axis) {
-      case 16: tp = PassShape<16, true>::TP; break;
-      case 32: tp = PassShape<32, true>::TP; break;
-      case 64: tp = PassShape<64, true>::TP; break;
-      case 96: tp = PassShape<96, true>::TP; break;
-      case 128: tp = PassShape<128, true>::TP; break;
-      case 256: tp = PassShape<256, true>::TP; break;
-      case 512: tp = PassShape<512, true>::TP; break;
+      case 16: tp = contig_tp<16, 0>(); break;
+      case 32: tp = contig_tp<32, 0>(); break;
+      case 64: tp = contig_tp<64, 0>(); break;
+      case 96: tp = contig_tp<96, 0>(); break;
+      case 128: tp = v == 1 ? contig_tp<128, 1>() : v == 2 ? contig_tp<128, 2>()
+                   : v == 3 ? contig_tp<128, 3>() : contig_tp<128, 0>(); break;
+      case 256: tp = v == 1 ? contig_tp<256, 1>() : v == 2 ? contig_tp<256, 2>()
+                   : v == 3 ? contig_tp<256, 3>() : contig_tp<256, 0>(); break;
+      case 512: tp = contig_tp<512, 0>(); break;
     }
     return (nx * ny) / tp;
   }
-  return (axis == 0 ? ny : nx) * (nz / 16);
-}
-
-// CTA slots a persistent pass leaves free for concurrent work on other
-// streams, such as the star update and bucket sort that run beside the y
-// drift pass (QJ_PERSIST_RESERVE, default 2).
-static int reserve_ctas() {
-  static int r = -1;
-  if (r < 0) {
-    const char *env = getenv("QJ_PERSIST_RESERVE");
-    r = env ? std::max(0, atoi(env)) : 2;
-  }
-  return r;
-}
-
-// cuTensorMapEncodeTiled from the driver, looked up once.
-static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
-  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-  static std::once_flag once;
-  std::call_once(once, [] {
-    void *p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-  });
-  return fn;
-}
-
-// Tensor maps of a strided pass' streamed fields (see TileMaps).
-template <int N, int MODE>
-static int strided_maps(const FusedArgs &a, TileMaps &maps) {
-  auto enc = tensor_map_encoder();
-  if (!enc) {
-    set_error("cuTensorMapEncodeTiled is not available from the driver");
-    return QJ_ERR_CUDA;
-  }
-  const int nbox = a.nbox > 1 ? a.nbox : 1;
-  const cuuint64_t dims[4] = {(cuuint64_t)a.nz, (cuuint64_t)a.ny, (cuuint64_t)a.nx, (cuuint64_t)nbox};
-  const cuuint64_t strides[3] = {(cuuint64_t)a.nz * 8, (cuuint64_t)a.ny * a.nz * 8,
-                                 (cuuint64_t)a.box_cells * 8};
-  const cuuint32_t rows = (cuuint32_t)std::min(N, 256);
-  const cuuint32_t box[4] = {16, a.axis == 0 ? 1u : rows, a.axis == 0 ? rows : 1u, 1};
-  const cuuint32_t estr[4] = {1, 1, 1, 1};
-  for (int f = 0; f < stream_count<MODE>(); ++f) {
-    const CUresult r = enc(&maps.m[f], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4,
-                           const_cast<float2 *>(stream_field<MODE>(a, f)), dims, strides, box, estr,
-                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS) {
-      set_error("cuTensorMapEncodeTiled failed (%d) for a %dx%dx%d pass along axis %d", (int)r, a.nx,
-                a.ny, a.nz, a.axis);
-      return QJ_ERR_CUDA;
-    }
-  }
-  return 0;
-}
-
-// Resident CTAs per SM of a pass (occupancy) and the SM count, queried once
-// per device (the shared-memory attribute belongs to that device's context).
-struct Occupancy {
-  cudaError_t err = cudaSuccess;
-  int per_sm = 1, sms = 1;
-};
-template <int N, bool CONTIG, int MODE>
-static cudaError_t fused_occupancy(int &per_sm, int &sms) {
-  using SH = PassShape<N, CONTIG>;
-  static PerDevice<Occupancy> cache;
-  const Occupancy *o = nullptr;
-  const cudaError_t e = per_device(cache, o, [](Occupancy &r) {
-    const size_t smem = fused_smem_bytes<N, CONTIG, MODE>();
-    r.err = cudaFuncSetAttribute(k_fused<N, CONTIG, MODE>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    int dev = 0, n_sm = 0, p = 0;
-    if (r.err == cudaSuccess) r.err = cudaGetDevice(&dev);
-    if (r.err == cudaSuccess) r.err = cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-    if (r.err == cudaSuccess)
-      r.err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&p, k_fused<N, CONTIG, MODE>, SH::THREADS,
-                                                            smem);
-    r.per_sm = std::max(1, p);
-    r.sms = std::max(1, n_sm);
-  });
-  if (e != cudaSuccess) return e;
-  per_sm = o->per_sm;
-  sms = o->sms;
-  return o->err;
-}
-
-template <int N, bool CONTIG, int MODE>
-static int run_fused(const FusedArgs &a, cudaStream_t st) {
-  using SH = PassShape<N, CONTIG>;
-  const size_t smem = fused_smem_bytes<N, CONTIG, MODE>();
-  // persistent grid: the CTAs resident at once (occupancy x SMs), shared
-  // between the boxes of a batched launch
-  int per_sm = 0, sms = 0;
-  const cudaError_t occ = fused_occupancy<N, CONTIG, MODE>(per_sm, sms);
-  QJ_CK(occ);
-  const int want = a.tune ? a.tune[MODE] : 0;
-  const int resident = (want > 0 ? std::min(want, per_sm) : per_sm) * sms;
-  const int reserve = (a.tune && a.tune[8] >= 0) ? a.tune[8] : reserve_ctas();
-  // the bulk tile copies need 16-byte aligned fields
-  const void *fields[4] = {a.psi, a.R, a.S1, a.S2};
-  for (const void *f : fields)
-    if ((reinterpret_cast<uintptr_t>(f) & 15) != 0) {
-      set_error("fields of the fused passes must be 16-byte aligned");
-      return QJ_ERR_ARG;
-    }
-  FusedArgs b = a;
-  b.ntiles = grid_of<N, CONTIG>(a);
-  // y passes walk backwards: each follows (and precedes) a pass that walks
-  // forwards over the same slow index x
-  b.rev = (!CONTIG && a.axis == 1) ? 1 : 0;
-  TileMaps maps;
-  std::memset(&maps, 0, sizeof(maps));
-  if (!CONTIG && stream_count<MODE>() > 0) {
-    const int rc = strided_maps<N, MODE>(b, maps);
-    if (rc) return rc;
-  }
-  const int nbox = a.nbox > 1 ? a.nbox : 1;
-  const int gx = std::max(1, std::min(b.ntiles, (resident - reserve) / nbox));
-  const dim3 grid(gx, nbox);
-  k_fused<N, CONTIG, MODE><<<grid, SH::THREADS, smem, st>>>(b, maps);
-  QJ_CK_LAUNCH();
-  return 0;
+  return (axis == 0 ? ny : nx) * (nz / (has_radix_variant(n_axis) ? strided_tile_width(v) : 16));
 }
 
 // The y-only transforms are instantiated strided; the others for both the
@@ -211,10 +93,19 @@ static int dispatch_mode(int n, const FusedArgs &a, cudaStream_t st) {
     set_error("internal: pass mode %d requested along z", MODE);
     return 1;
   }
-#define QJ_CASE(NN)                                                    \
-  case NN:                                                             \
-    if constexpr (ONLY_Y) return run_fused<NN, false, MODE>(a, st);    \
-    else return contig ? run_fused<NN, true, MODE>(a, st) : run_fused<NN, false, MODE>(a, st);
+  if (a.shape != 0 && has_radix_variant(n)) {
+    switch (a.shape) {
+      case 1: return run_shape_variant<1>(MODE, n, a, st);
+      case 2: return run_shape_variant<2>(MODE, n, a, st);
+      case 3: return run_shape_variant<3>(MODE, n, a, st);
+    }
+    set_error("internal: pass shape variant %d", a.shape);
+    return 1;
+  }
+#define QJ_CASE(NN)                                                          \
+  case NN:                                                                   \
+    if constexpr (ONLY_Y) return run_fused<NN, false, MODE, 0>(a, st);       \
+    else return contig ? run_fused<NN, true, MODE, 0>(a, st) : run_fused<NN, false, MODE, 0>(a, st);
   switch (n) {
     QJ_CASE(16)
     QJ_CASE(32)
@@ -236,13 +127,13 @@ static int dispatch_deposit(int n, const FusedArgs &a, cudaStream_t st) {
     return 1;
   }
   switch (n) {
-    case 16: return run_fused<16, true, M_DEPOSIT>(a, st);
-    case 32: return run_fused<32, true, M_DEPOSIT>(a, st);
-    case 64: return run_fused<64, true, M_DEPOSIT>(a, st);
-    case 96: return run_fused<96, true, M_DEPOSIT>(a, st);
-    case 128: return run_fused<128, true, M_DEPOSIT>(a, st);
-    case 256: return run_fused<256, true, M_DEPOSIT>(a, st);
-    case 512: return run_fused<512, true, M_DEPOSIT>(a, st);
+    case 16: return run_fused<16, true, M_DEPOSIT, 0>(a, st);
+    case 32: return run_fused<32, true, M_DEPOSIT, 0>(a, st);
+    case 64: return run_fused<64, true, M_DEPOSIT, 0>(a, st);
+    case 96: return run_fused<96, true, M_DEPOSIT, 0>(a, st);
+    case 128: return run_fused<128, true, M_DEPOSIT, 0>(a, st);
+    case 256: return run_fused<256, true, M_DEPOSIT, 0>(a, st);
+    case 512: return run_fused<512, true, M_DEPOSIT, 0>(a, st);
   }
   set_error("unsupported FFT length %d", n);
   return 1;
@@ -270,10 +161,10 @@ template <int MODE> static int occupancy_of(int n, bool contig) {
   constexpr bool ONLY_Z = (MODE == M_DEPOSIT);
 #define QJ_OCC(NN)                                                                          \
   case NN:                                                                                  \
-    if constexpr (ONLY_Y) e = fused_occupancy<NN, false, MODE>(per_sm, sms);                \
-    else if constexpr (ONLY_Z) e = fused_occupancy<NN, true, MODE>(per_sm, sms);            \
-    else e = contig ? fused_occupancy<NN, true, MODE>(per_sm, sms)                          \
-                    : fused_occupancy<NN, false, MODE>(per_sm, sms);                        \
+    if constexpr (ONLY_Y) e = fused_occupancy<NN, false, MODE, 0>(per_sm, sms);             \
+    else if constexpr (ONLY_Z) e = fused_occupancy<NN, true, MODE, 0>(per_sm, sms);         \
+    else e = contig ? fused_occupancy<NN, true, MODE, 0>(per_sm, sms)                       \
+                    : fused_occupancy<NN, false, MODE, 0>(per_sm, sms);                     \
     break;
   switch (n) {
     QJ_OCC(16)
@@ -289,7 +180,15 @@ template <int MODE> static int occupancy_of(int n, bool contig) {
   return e == cudaSuccess ? per_sm : 0;
 }
 
-int fused_max_ctas_per_sm(int mode, int n, bool contig) {
+int fused_max_ctas_per_sm(int mode, int n, bool contig, int shape) {
+  if (shape != 0 && has_radix_variant(n) && mode != M_DEPOSIT) {
+    switch (shape) {
+      case 1: return shape_variant_ctas_per_sm<1>(mode, n, contig);
+      case 2: return shape_variant_ctas_per_sm<2>(mode, n, contig);
+      case 3: return shape_variant_ctas_per_sm<3>(mode, n, contig);
+    }
+    return 0;
+  }
   switch (mode) {
     case M_DENSITY: return occupancy_of<M_DENSITY>(n, contig);
     case M_FFT_FWD: return occupancy_of<M_FFT_FWD>(n, contig);

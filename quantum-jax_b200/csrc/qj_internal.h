@@ -8,6 +8,7 @@
 #include <mutex>
 #include <vector>
 
+#include "../../include/qj.h"
 #include "qj_pass.cuh"
 
 namespace qj {
@@ -59,8 +60,24 @@ void prof_mark_begin(cudaStream_t st);
 void prof_mark_end(int bucket, cudaStream_t st);
 
 bool fft_length_supported(int n);
-// Stage twiddle table of the fused passes for length n (host, float2).
-std::vector<float2> stage_twiddles(int n);
+// Stage twiddle table of the fused passes for length n and radix plan rv
+// (host, float2; rv = 1 only for has_radix_variant(n)).
+std::vector<float2> stage_twiddles(int n, int rv = 0);
+
+// Launch-shape variant (PassShape's V) of a plan's pass of `mode` along an
+// axis of length n, contiguous (z) or strided (x, y): bit b of
+// tune[QJ_TUNE_RADIX] gives V's bit 0 (radix plan 1), bit b of
+// tune[QJ_TUNE_TILE] its bit 1 (half tile), b = mode for a strided pass and
+// 8 + mode for a contiguous one.  The first density build takes the drift +
+// density pass's bits of its orientation, so that both write the same number
+// of partial sums; the deposit and lengths without variants always take 0.
+inline int shape_of(int n, const int *tune, int mode, bool contig) {
+  if (!tune || !has_radix_variant(n) || mode == M_DEPOSIT) return 0;
+  const int b = (mode == M_DENSITY ? M_DRIFT_DENSITY : mode) + (contig ? 8 : 0);
+  return ((tune[QJ_TUNE_RADIX] >> b) & 1) | (((tune[QJ_TUNE_TILE] >> b) & 1) << 1);
+}
+// z columns of a strided tile in shape variant v (16, or 8 for bit 1).
+int strided_tile_width(int v);
 
 // ----- pencil passes (qj_fused.cu, qj_fftpass.cu) -----
 // Launch one fused single-precision pass of `mode` along `a.axis` (length n).
@@ -68,8 +85,9 @@ int launch_selftest_wait(unsigned *err, long long limit_ns, cudaStream_t st);
 // out[i] = (sin, cos) of theta[i] by the kick pass's own sincos_reduced.
 int launch_selftest_sincos(const double *theta, float2 *out, int n, cudaStream_t st);
 int launch_fused(int mode, int n, const FusedArgs &a, cudaStream_t st);
-// Number of CTAs a pass along `axis` launches (= partial sums written).
-int pass_blocks(int n_axis, int axis, int nx, int ny, int nz);
+// Number of tiles of a pass along `axis` in shape variant v (= the partial
+// sums a density pass writes).
+int pass_blocks(int n_axis, int axis, int nx, int ny, int nz, int v = 0);
 // Generic in-place FFT pass over a complex field (float2 if dbl == 0, else
 // double2) along a.axis.
 int launch_fft(bool dbl, int n, int dir, const FftArgs &a, cudaStream_t st);
@@ -193,8 +211,9 @@ int launch_adj_update(bool dbl, void *g, const void *psi, const void *V, const v
                       const void *mu, double b, double coef, long long ncell, cudaStream_t st);
 
 // ----- gas and black hole (qj_gas.cu) -----
-// CTAs of a fused pass that fit one SM (occupancy), 0 if unknown.
-int fused_max_ctas_per_sm(int mode, int n, bool contig);
+// CTAs of a fused pass in shape variant `shape` that fit one SM (occupancy),
+// 0 if unknown.
+int fused_max_ctas_per_sm(int mode, int n, bool contig, int shape = 0);
 
 int launch_hydro(bool dbl, void *rho, void *vx, void *vy, void *vz, void *prim, int n, double dx,
                  double dt, double cs, int clamp_rho, cudaStream_t st, int block = 256,

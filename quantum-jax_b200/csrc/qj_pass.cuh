@@ -42,7 +42,7 @@ struct FusedArgs {
   int axis;                // 0, 1, 2
   long long stride;        // element stride along the axis
   long long outer_stride;  // strided passes: stride of the outer index
-  int ztiles;              // strided passes: nz / 16
+  int ztiles;              // strided passes: nz / (z columns of a tile)
   float2 *psi;
   float2 *R;
   float2 *S1;
@@ -92,6 +92,9 @@ struct FusedArgs {
   float gas_dt;
   // tiles of this pass per box (the persistent CTAs stride over them)
   int ntiles;
+  // shape variant of the pass (PassShape's V: radix plan, tile width); set
+  // with the fields that follow from it (tw, ztiles)
+  int shape;
   // forward y / Poisson passes over half of the real density's spectrum (the
   // other non-y axis to n/2); the Poisson pass then also writes the mirrors
   int half;
@@ -160,7 +163,7 @@ __device__ __forceinline__ PencilPos pencil_pos(const FusedArgs &a, int tile, in
     pp.c[2] = 0;
   } else {
     const int o = tile / a.ztiles;
-    const int z = (tile % a.ztiles) * 16 + p;
+    const int z = (tile % a.ztiles) * TP + p;
     pp.base = (long long)o * a.outer_stride + z;
     pp.c[2] = z;
     if (a.axis == 0) {  // o = y
@@ -491,29 +494,30 @@ __device__ __forceinline__ float2 phase_rotate(float2 z, double theta) {
 
 // Landing buffer of one tile.  Contiguous tiles (z pencils) land as one row
 // per pencil, padded by P elements when P < 16 so that the lanes of the
-// different pencils in a warp read different banks; strided tiles land as N rows of the 16
-// pencils' elements (128 B each), the dense box of a tensor-map copy.  Every
-// copy is a multiple of 16 bytes and starts on a 16-byte boundary.
-template <int N, bool CONTIG> struct Landing {
-  using SH = PassShape<N, CONTIG>;
+// different pencils in a warp read different banks; strided tiles land as N
+// rows of the TP pencils' elements (TP x 8 B each: 128 B, or 64 B for the
+// narrow tile variant), the dense box of a tensor-map copy.  Every copy is a
+// multiple of 16 bytes and starts on a 16-byte boundary.
+template <int N, bool CONTIG, int V = 0> struct Landing {
+  using SH = PassShape<N, CONTIG, V>;
   static constexpr int PAD = CONTIG ? (SH::P >= 16 ? 0 : (SH::P >= 2 ? SH::P : 2)) : 0;
-  static constexpr int ROWS = CONTIG ? SH::TP : N;   // bulk copies per tile
-  static constexpr int ROW_ELEMS = CONTIG ? N : 16;  // complex64 per copy
-  static constexpr int ROW_STRIDE = CONTIG ? N + PAD : 16;
+  static constexpr int ROWS = CONTIG ? SH::TP : N;       // bulk copies per tile
+  static constexpr int ROW_ELEMS = CONTIG ? N : SH::TP;  // complex64 per copy
+  static constexpr int ROW_STRIDE = CONTIG ? N + PAD : SH::TP;
   static constexpr size_t BYTES = (size_t)ROWS * ROW_STRIDE * sizeof(float2);
   static constexpr unsigned TX = (unsigned)ROWS * ROW_ELEMS * (unsigned)sizeof(float2);
   static_assert((ROW_STRIDE * sizeof(float2)) % 16 == 0, "landing rows must stay 16-byte aligned");
   static_assert(TX < (1u << 20), "tile larger than an mbarrier transaction count");
   __device__ static __forceinline__ int idx(int p, int i) {
-    return CONTIG ? p * ROW_STRIDE + i : i * 16 + p;
+    return CONTIG ? p * ROW_STRIDE + i : i * SH::TP + p;
   }
 };
 
 // Dynamic shared memory of a fused pass: the exchange rows, the stage twiddle
 // table, the pass axis' own tables, THREADS x E per-thread save slots (drift
 // and Poisson passes) and the landing buffer.
-template <int N, bool CONTIG, int MODE> struct FusedSmem {
-  using SH = PassShape<N, CONTIG>;
+template <int N, bool CONTIG, int MODE, int V = 0> struct FusedSmem {
+  using SH = PassShape<N, CONTIG, V>;
   static constexpr bool DRIFTS = MODE == M_KICK || MODE == M_DRIFT || MODE == M_DRIFT_DENSITY;
   static constexpr bool LANDS = MODE != M_DEPOSIT;
   static constexpr bool SAVES = DRIFTS || MODE == M_POISSON || MODE == M_IFFT2;
@@ -523,16 +527,16 @@ template <int N, bool CONTIG, int MODE> struct FusedSmem {
                                       : (MODE == M_POISSON ? 2 * N * sizeof(float)
                                                            : (MODE == M_IFFT2 ? N * sizeof(float) : 0));
   static constexpr size_t TW = a16(SH::template smem_bytes<float2>());
-  static constexpr size_t TAB = a16(TW + (size_t)stage_tw_size<N>() * sizeof(float2));
+  static constexpr size_t TAB = a16(TW + (size_t)stage_tw_size<N, SH::RV>() * sizeof(float2));
   static constexpr size_t SAVE = a16(TAB + TAB_BYTES);
   static constexpr size_t LAND =
       a16(SAVE + (SAVES ? (size_t)SH::THREADS * SH::E * sizeof(float2) : 0));
   // + slack to round the landing buffer up to a 128-byte boundary (tensor copies)
-  static constexpr size_t TOTAL = LAND + (LANDS ? Landing<N, CONTIG>::BYTES + 128 : 0);
+  static constexpr size_t TOTAL = LAND + (LANDS ? Landing<N, CONTIG, V>::BYTES + 128 : 0);
 };
-template <int N, bool CONTIG, int MODE>
+template <int N, bool CONTIG, int MODE, int V = 0>
 __host__ __device__ constexpr size_t fused_smem_bytes() {
-  return FusedSmem<N, CONTIG, MODE>::TOTAL;
+  return FusedSmem<N, CONTIG, MODE, V>::TOTAL;
 }
 
 // The input fields a pass streams, in order of use.
@@ -548,9 +552,9 @@ __host__ __device__ __forceinline__ const float2 *stream_field(const FusedArgs &
 }
 
 // Strided passes: one tiled tensor map per streamed field, over the
-// (z, y, x, box) array of complex64 (8-byte elements), whose box is 16 z by
-// up to 256 rows along the pass axis.  One copy instruction then brings a
-// whole tile (two for n = 512).
+// (z, y, x, box) array of complex64 (8-byte elements), whose box is the
+// tile's z columns (16, or 8) by up to 256 rows along the pass axis.  One copy
+// instruction then brings a whole tile (two for n = 512).
 struct TileMaps {
   CUtensorMap m[3];
 };
@@ -599,18 +603,18 @@ __device__ __forceinline__ bool mbar_wait_bounded(unsigned long long *bar, unsig
 template <bool CONTIG>
 __device__ __forceinline__ long long tile_origin(const FusedArgs &a, int tile, int TP) {
   if (CONTIG) return (long long)tile * TP * a.nz;
-  return (long long)(tile / a.ztiles) * a.outer_stride + (long long)(tile % a.ztiles) * 16;
+  return (long long)(tile / a.ztiles) * a.outer_stride + (long long)(tile % a.ztiles) * TP;
 }
 
 // Start the copies of streamed field f's tile into the landing buffer (warp
 // 0 only).  Contiguous tiles: one bulk copy per pencil row.  Strided tiles:
 // the field's tensor map, coordinates (z0, y, x, box) with the pass axis
 // starting at row h.
-template <int N, bool CONTIG, int MODE>
+template <int N, bool CONTIG, int MODE, int V>
 __device__ __forceinline__ void issue_tile(const FusedArgs &a, const TileMaps &maps, int f, int tile,
                                            float2 *land, unsigned long long *bar) {
-  using L = Landing<N, CONTIG>;
-  constexpr int T = PassShape<N, CONTIG>::THREADS;
+  using L = Landing<N, CONTIG, V>;
+  constexpr int T = PassShape<N, CONTIG, V>::THREADS, TP = PassShape<N, CONTIG, V>::TP;
   constexpr unsigned MASK = T >= 32 ? 0xffffffffu : ((1u << T) - 1u);
   const int lane = threadIdx.x & 31;
   if (lane == 0) {
@@ -621,7 +625,7 @@ __device__ __forceinline__ void issue_tile(const FusedArgs &a, const TileMaps &m
   if constexpr (CONTIG) {
     __syncwarp(MASK);
     const float2 *fld = stream_field<MODE>(a, f);
-    const long long o = tile_origin<CONTIG>(a, tile, PassShape<N, CONTIG>::TP);
+    const long long o = tile_origin<CONTIG>(a, tile, TP);
     for (int r = lane; r < L::ROWS; r += 32) {
       const float2 *src = fld + o + (long long)r * a.nz;
       asm volatile(
@@ -632,14 +636,14 @@ __device__ __forceinline__ void issue_tile(const FusedArgs &a, const TileMaps &m
     }
   } else {
     if (lane == 0) {
-      const int z0 = (tile % a.ztiles) * 16, o = tile / a.ztiles, box = blockIdx.y;
+      const int z0 = (tile % a.ztiles) * TP, o = tile / a.ztiles, box = blockIdx.y;
       const unsigned long long map = reinterpret_cast<unsigned long long>(&maps.m[f]);
 #pragma unroll
       for (int h = 0; h < N; h += 256) {
         const int cy = a.axis == 0 ? o : h, cx = a.axis == 0 ? h : o;
         asm volatile(
             "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-            " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(smem_addr(land + h * 16)),
+            " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(smem_addr(land + h * TP)),
             "l"(map), "r"(z0), "r"(cy), "r"(cx), "r"(box), "r"(smem_addr(bar))
             : "memory");
       }
@@ -651,12 +655,12 @@ __device__ __forceinline__ void issue_tile(const FusedArgs &a, const TileMaps &m
 // this thread's elements (and element 0 of its pencil, c0), release the
 // buffer to the next copy and start that copy.  Returns false on every
 // thread of the CTA if the wait gave up (the error word is set).
-template <int N, bool CONTIG, int MODE, int E>
+template <int N, bool CONTIG, int MODE, int V, int E>
 __device__ __forceinline__ bool take_tile(float2 (&v)[E], float2 &c0, const FusedArgs &a,
                                           const TileMaps &maps, float2 *land,
                                           unsigned long long *bar, unsigned &parity, int &f, int tile,
                                           int p, int t) {
-  using L = Landing<N, CONTIG>;
+  using L = Landing<N, CONTIG, V>;
   constexpr int P = N / E, NF = stream_count<MODE>();
   bool ok = mbar_wait_bounded(bar, parity);
   if (ok) {
@@ -684,16 +688,16 @@ __device__ __forceinline__ bool take_tile(float2 (&v)[E], float2 &c0, const Fuse
   }
   f = nf;
   if (nt < a.ntiles && threadIdx.x < 32)
-    issue_tile<N, CONTIG, MODE>(a, maps, nf, a.rev ? a.ntiles - 1 - nt : nt, land, bar);
+    issue_tile<N, CONTIG, MODE, V>(a, maps, nf, a.rev ? a.ntiles - 1 - nt : nt, land, bar);
   return true;
 }
 
-template <int N, bool CONTIG, int MODE>
-__global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CONTIG>::MINB)
+template <int N, bool CONTIG, int MODE, int SV = 0>
+__global__ void __launch_bounds__(PassShape<N, CONTIG, SV>::THREADS, PassShape<N, CONTIG, SV>::MINB)
     k_fused(FusedArgs a, const __grid_constant__ TileMaps maps) {
   select_box(a);
-  using SH = PassShape<N, CONTIG>;
-  using LAY = FusedSmem<N, CONTIG, MODE>;
+  using SH = PassShape<N, CONTIG, SV>;
+  using LAY = FusedSmem<N, CONTIG, MODE, SV>;
   constexpr int E = SH::E, P = SH::P, TP = SH::TP, THREADS = SH::THREADS;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   float2 *sm = reinterpret_cast<float2 *>(smem_raw);
@@ -722,7 +726,7 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CO
   else
     smv.base = sm + p;
   // the stage twiddle table of this axis, staged after the exchange rows
-  for (int i = tid; i < stage_tw_size<N>(); i += THREADS) tw_s[i] = a.tw[i];
+  for (int i = tid; i < stage_tw_size<N, SH::RV>(); i += THREADS) tw_s[i] = a.tw[i];
   if constexpr (LAY::DRIFTS) {
     for (int i = tid; i < N; i += THREADS) tab2[i] = a.prop[i];
   } else if constexpr (MODE == M_IFFT2) {
@@ -740,7 +744,7 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CO
   int fld = 0;
   if constexpr (LAY::LANDS)
     if ((int)blockIdx.x < a.ntiles && tid < 32)
-      issue_tile<N, CONTIG, MODE>(a, maps, 0, a.rev ? a.ntiles - 1 - (int)blockIdx.x : (int)blockIdx.x,
+      issue_tile<N, CONTIG, MODE, SV>(a, maps, 0, a.rev ? a.ntiles - 1 - (int)blockIdx.x : (int)blockIdx.x,
                                   land, &lbar);
 
   for (int it = blockIdx.x; it < a.ntiles; it += gridDim.x) {
@@ -755,7 +759,7 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS, PassShape<N, CO
       if (a.has_stars) sr = star_ranges(a, pp);
     float2 c0;
 #define QJ_TAKE(v) \
-  if (!take_tile<N, CONTIG, MODE, E>(v, c0, a, maps, land, &lbar, parity, fld, it, p, t)) return
+  if (!take_tile<N, CONTIG, MODE, SV, E>(v, c0, a, maps, land, &lbar, parity, fld, it, p, t)) return
 
     if constexpr (MODE == M_DENSITY) {
       float2 v[E];
@@ -1122,7 +1126,7 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG>::THREADS) k_fft(FftArgs a
     base = (long long)(blockIdx.x * TP + p) * a.nz;
   } else {
     const int o = blockIdx.x / a.ztiles;
-    const int z = (blockIdx.x % a.ztiles) * 16 + p;
+    const int z = (blockIdx.x % a.ztiles) * TP + p;
     base = (long long)o * a.outer_stride + z;
   }
   using SMV = typename std::conditional<CONTIG, SmemContig<C>, SmemStrided<C, TP>>::type;

@@ -21,7 +21,10 @@ QJ_ERR_TIMEOUT = 4
 QJ_ERR_ALLOC = 5
 QJ_PLAIN_F64 = 0
 QJ_FUSED_F32 = 1
-QJ_TUNE_N = 10
+QJ_TUNE_N = 12
+QJ_TUNE_RADIX = 10
+QJ_TUNE_TILE = 11
+QJ_AUTOTUNE_SHAPES = 1
 
 # Every symbol include/qj.h declares, with (restype, argtypes).
 c_void_p, c_int, c_double, c_int64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int64
@@ -83,7 +86,7 @@ SIGNATURES = {
                                 c_double, c_void_p, c_void_p]),
     "qj_plan_set_tuning": (c_int, [c_void_p, c_void_p, c_int]),
     "qj_autotune_kdk": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_double,
-                                c_double, c_int, c_void_p]),
+                                c_double, c_int, c_int, c_void_p]),
     "qj_selftest_sincos": (c_int, [c_void_p, c_void_p, c_int, c_void_p]),
     "qj_xla_kdk_step_f32": (None, [c_void_p, ctypes.POINTER(c_void_p), ctypes.c_char_p,
                                    ctypes.c_size_t, c_void_p]),

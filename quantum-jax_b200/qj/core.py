@@ -169,23 +169,26 @@ class Plan:
         buf = (ctypes.c_int32 * _lib.QJ_TUNE_N)(*[int(v) for v in values])
         check(lib().qj_plan_set_tuning(self._h, buf, _lib.QJ_TUNE_N))
 
-    def autotune(self, psi, pos, vel, m_s, dt, probe_steps=10, cache_file=None):
-        """Pick the fused passes' CTAs per SM and the reserved CTA slots by
-        timing qj_kdk_step on a copy of (psi, pos, vel); the arrays are only
-        read.  Results are cached in a JSON file (QJ_TUNING_CACHE, default
-        ~/.cache/qj/tuning.json) keyed by device, grid, boxes, stars and
-        precision; a cached entry is applied without timing.  Returns the
-        tuning list."""
+    def autotune(self, psi, pos, vel, m_s, dt, probe_steps=10, cache_file=None, shapes=True):
+        """Pick the fused passes' launch tuning by timing qj_kdk_step on a
+        copy of (psi, pos, vel); the arrays are only read.  shapes=True also
+        picks the FFT radix plan and pencil tile of the 128- and 256-long
+        axes (which change the rounding, within the single-precision bars);
+        shapes=False keeps them and tunes only what is bit-identical (CTAs per
+        SM, reserved slots).  Results are cached in a JSON file
+        (QJ_TUNING_CACHE, default ~/.cache/qj/tuning.json) keyed by device,
+        grid, boxes, stars, precision and the shapes flag; a cached entry is
+        applied without timing.  Returns the tuning list."""
         import os
 
         n_s = 0 if pos is None else int(pos.shape[-2])
         key = "|".join(str(x) for x in (
             torch.cuda.get_device_name(psi.device), self.grid.nx, self.grid.ny, self.grid.nz,
-            self.nbox, n_s, self.precision))
+            self.nbox, n_s, self.precision, "shapes" if shapes else "ctas"))
         path = cache_file or os.environ.get(
             "QJ_TUNING_CACHE", os.path.join(os.path.expanduser("~"), ".cache", "qj", "tuning.json"))
         cache = read_tuning_cache(path)
-        if key in cache:
+        if key in cache and len(cache[key]) == _lib.QJ_TUNE_N:
             self.tuning = cache[key]
             return self.tuning
         ncell = self.grid.nx * self.grid.ny * self.grid.nz
@@ -200,7 +203,8 @@ class Plan:
                                  f"[nbox, n_s, 3] (or [n_s, 3] for one box)")
         check(lib().qj_autotune_kdk(self._h, _ptr(psi), _ptr(pos) if n_s else None,
                                     _ptr(vel) if n_s else None, n_s, float(m_s), float(dt),
-                                    int(probe_steps), _stream()))
+                                    int(probe_steps), _lib.QJ_AUTOTUNE_SHAPES if shapes else 0,
+                                    _stream()))
         tuning = self.tuning
         cache = read_tuning_cache(path)  # entries other processes added meanwhile
         cache[key] = tuning
