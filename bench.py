@@ -603,14 +603,17 @@ def main():
                                    qj.FUSED_F32, 256))
         if not a.no_autotune:
             # each batched plan, and each single-box plan of the one-by-one
-            # comparison, on its own state (the first box for the latter)
+            # comparison, on its own state (the first box for the latter); the
+            # batched plans keep the default radix plan and tile, which the
+            # ensemble's one launch per pass requires
             for pl, sg, stt in zip(plans, singles, state):
                 pl.autotune(stt[0], stt[1], stt[2], stt[5], stt[4], probe_steps=5,
-                            cache_file=os.path.join(a.tune_dir, "tuning.json"))
+                            cache_file=os.path.join(a.tune_dir, "tuning.json"), shapes=False)
                 sg.autotune(stt[0][0].contiguous(), stt[1][0].contiguous(),
                             stt[2][0].contiguous(), stt[5], stt[4], probe_steps=5,
                             cache_file=os.path.join(a.tune_dir, "tuning.json"))
         ens = qj.Ensemble(plans)
+        merged = ens.merged
         init = [[t.clone() if isinstance(t, torch.Tensor) else t for t in s] for s in state]
 
         def ens_run(m):
@@ -625,6 +628,26 @@ def main():
         e1.record(stream)
         barrier()
         ens_ms = max_over_ranks(e0.elapsed_time(e1))
+        # the same steps as one launch per fused pass for all sizes (same
+        # bits), on a copy of the state, for comparison
+        ens_m = qj.Ensemble(plans, merge=True)
+        merged_ms = None
+        if ens_m.merged:
+            sm = [[t.clone() if isinstance(t, torch.Tensor) else t for t in x] for x in init]
+
+            def ens_m_run(m):
+                ens_m.step([x[0] for x in sm], [x[1] for x in sm], [x[2] for x in sm],
+                           [x[3] for x in sm], [x[4] for x in sm], [x[5] for x in sm], m,
+                           chunk=a.ens_chunk, graph=True)
+
+            ens_m_run(a.ens_chunk)
+            barrier()
+            e0.record(stream)
+            ens_m_run(ens_steps)
+            e1.record(stream)
+            barrier()
+            merged_ms = max_over_ranks(e0.elapsed_time(e1))
+        ens_m.close()
         cells = sum(n_e**3 * nb for n_e, nb in all_groups)  # all ranks' boxes
         # one by one: each box alone through a single-box plan, same steps
         views, first = [], []
@@ -672,11 +695,15 @@ def main():
             k = f"{r['n']}^3"
             worst[k] = max(worst.get(k, 0.0), r["psi_rel_l2_vs_f64"])
         ensemble = {"boxes": "16x64^3 + 8x96^3 + 8x128^3, 256 stars each",
+                    "launches": ("one persistent launch per fused pass for all sizes"
+                                 if merged else "one stream per size class"),
                     "sharding": f"{world} rank(s), greedy by C log C; this rank: "
                                 + ", ".join(f"{nb}x{n_e}^3" for n_e, nb, _ in groups),
                     "tuning": {f"{n_e}^3": pl.tuning for (n_e, _, _), pl in zip(groups, plans)},
                     "cells": cells, "steps": ens_steps, "graph_chunk": a.ens_chunk,
                     "ensemble_cell_steps_per_s": cells * ens_steps / (ens_ms * 1e-3),
+                    "one_launch_per_pass_cell_steps_per_s": (
+                        cells * ens_steps / (merged_ms * 1e-3) if merged_ms else None),
                     "one_by_one_cell_steps_per_s": cells * ens_steps / (seq_ms * 1e-3),
                     "speedup": seq_ms / ens_ms,
                     "psi_rel_l2_vs_f64_max": worst,

@@ -195,15 +195,24 @@ int qj_get_potential_f32_noalloc(const qj_grid *grid, const qj_phys *phys,
 
 /* Ensembles of uneven boxes (no reference counterpart: the reference runs one
  * box per process).  One batched plan per box size; qj_ensemble_step advances
- * every plan's boxes by nsteps, each plan on its own stream, joined on
- * `stream`.  With use_graph, the `chunk`-step body is captured once into a
- * CUDA graph (recaptured when pointers or sizes change) and replayed
- * nsteps / chunk times; a remainder runs directly.  Arrays are indexed by
- * plan: psi[i], pos[i], vel[i] (device), n_s[i], m_s[i], dt[i] (host),
- * diag[i] (device, nbox records). */
+ * every plan's boxes by nsteps, joined on `stream`, each plan on its own
+ * stream.  With use_graph, the `chunk`-step body is captured once into a CUDA
+ * graph (recaptured when pointers, sizes or the launch form change) and
+ * replayed nsteps / chunk times; a remainder runs directly.  Arrays are
+ * indexed by plan: psi[i], pos[i], vel[i] (device), n_s[i], m_s[i], dt[i]
+ * (host), diag[i] (device, nbox records).
+ * qj_ensemble_set_merge(ens, 1) runs each fused pass of the step as one
+ * persistent launch over all plans' boxes instead, its CTAs split between
+ * the sizes in proportion to their work, when the plans are cubes of distinct
+ * sizes among 64, 96 and 128 with the default radix plan and tile (tuning
+ * fields 10, 11 zero).  The bits are the same; the per-plan streams measured
+ * faster, so they are the default (merge 0).  qj_ensemble_merged returns 1
+ * when steps use the single launches, else 0. */
 typedef struct qj_ensemble qj_ensemble;
 int qj_ensemble_create(qj_ensemble **ens, qj_plan *const *plans, int nplans);
 int qj_ensemble_destroy(qj_ensemble *ens);
+int qj_ensemble_set_merge(qj_ensemble *ens, int on);
+int qj_ensemble_merged(const qj_ensemble *ens);
 int qj_ensemble_step(qj_ensemble *ens, void *const *psi, void *const *pos,
                      void *const *vel, const int *n_s, const double *m_s,
                      const double *dt, qj_diag *const *diag, int nsteps,

@@ -346,12 +346,7 @@ int deposit_list(qj_plan *P, const void *pos, int n, double m_s, const void *mas
 }
 
 // ---------------------------------------------------------------------------
-// Fused single-precision KDK (complex64 psi).  Consecutive half kicks of
-// adjacent steps share their potential (the density |psi|^2 and the star
-// positions do not change between them), so nsteps steps take nsteps + 1
-// Poisson solves; each kick still advances the star velocities by two
-// separate dt/2 half kicks and records dt_s between them, as the reference's
-// step boundary does.
+// Fused single-precision KDK (complex64 psi).
 // ---------------------------------------------------------------------------
 // Per-step coefficients of a variable-step run (quantum-cosmo.py:173-181):
 // kick_half[n] = m_per_hbar dt_n pot_fac_n / 2, drift[n] = dt_n kin_fac_n.
@@ -360,132 +355,202 @@ struct StepCoefs {
   std::vector<double> kick_half, drift;
 };
 
-int fused_kdk(qj_plan *P, float2 *psi, float *pos, float *vel, int n_s, double m_s, double dt,
-              int nsteps, int si, const float *vext, double *diag, cudaStream_t st,
-              const StepCoefs *sc = nullptr, void *save = nullptr, float *vsave = nullptr,
-              const float *rho_src = nullptr) {
-  const bool parts = n_s > 0;
-  const int nb = P->nbox;  // boxes: fields [nb][nx][ny][nz], stars [nb][n_s][3]
-  P->cur_stars = n_s;
-  auto half = [&](int n) { return sc ? sc->kick_half[n] : P->ph.m_per_hbar * dt / 2.0; };
-  auto drift_dt = [&](int n) { return sc ? sc->drift[n] : dt; };
-  auto kick_coef = [&](int k, bool last) { return (k > 0 ? half(k - 1) : 0.0) + (last ? 0.0 : half(k)); };
-  // the uniform potential's phase is carried in float64 (FusedArgs::phi), except
-  // on the adjoint's recompute path, whose saved potentials include it
-  const bool use_phi = save == nullptr && vsave == nullptr;
-  if (use_phi) QJ_CK(cudaMemsetAsync(P->phi, 0, (size_t)nb * sizeof(double), st));
-  QJ_TRY(launch_diag_load(false, diag, P->amax, st, nb));
-  if (parts) QJ_TRY(launch_set_scalar(false, P->dts, INFINITY, st, nb));
-  int q = 2;
-  if (parts) {
-    if (prof_on()) prof_mark_begin(st);
-    QJ_TRY(launch_stars_prepare(pos, n_s * nb, nullptr, m_s, geom(P), q, P->sb, st));
-    QJ_TRY(launch_bucket_sort(n_s, n_pencils(P, q), bucket_nv(P, q), P->sb, st, nb,
-                              P->bstart_stride));
-    if (prof_on()) prof_mark_end(7, st);
+// One fused pass of a run: its mode, axis and arguments.
+struct Phase {
+  int mode, axis;
+  FusedArgs a;
+};
+int run_phase(const qj_plan *P, const Phase &ph, cudaStream_t st) {
+  return launch_fused(ph.mode, P->n[ph.axis], ph.a, st);
+}
+
+// A fused KDK run of one plan, phase by phase.  fused_kdk runs the phases in
+// order; an ensemble runs each phase for all its plans (as one launch per
+// fused pass where the plans' sizes allow) with the same sequence:
+//   begin, density, then for k = 0..nsteps: step_begin, fft_fwd, poisson,
+//   ifft2, kick, stars; unless k == nsteps: drift, join, drift_density,
+//   step_end; finally end.
+// Consecutive half kicks of adjacent steps share their potential (the density
+// |psi|^2 and the star positions do not change between them), so nsteps
+// steps take nsteps + 1 Poisson solves; each kick still advances the star
+// velocities by two separate dt/2 half kicks and records dt_s between them,
+// as the reference's step boundary does.
+struct KdkRun {
+  qj_plan *P;
+  float2 *psi;
+  float *pos, *vel;
+  int n_s;
+  double m_s, dt;
+  int nsteps, si;
+  const float *vext;
+  double *diag;
+  const StepCoefs *sc;
+  void *save;
+  float *vsave;
+  const float *rho_src;
+  bool parts = false, use_phi = false;
+  int q = 2;  // the axis of the density build before kick k (and of kick k)
+
+  double half(int n) const { return sc ? sc->kick_half[n] : P->ph.m_per_hbar * dt / 2.0; }
+  double drift_dt(int n) const { return sc ? sc->drift[n] : dt; }
+  double kick_coef(int k, bool last) const {
+    return (k > 0 ? half(k - 1) : 0.0) + (last ? 0.0 : half(k));
   }
-  {
+  int r() const { return 2 - q; }
+
+  int begin(cudaStream_t st) {
+    parts = n_s > 0;
+    const int nb = P->nbox;  // boxes: fields [nb][nx][ny][nz], stars [nb][n_s][3]
+    P->cur_stars = n_s;
+    // the uniform potential's phase is carried in float64 (FusedArgs::phi),
+    // except on the adjoint's recompute path, whose saved potentials include it
+    use_phi = save == nullptr && vsave == nullptr;
+    q = 2;
+    if (use_phi) QJ_CK(cudaMemsetAsync(P->phi, 0, (size_t)nb * sizeof(double), st));
+    QJ_TRY(launch_diag_load(false, diag, P->amax, st, nb));
+    if (parts) QJ_TRY(launch_set_scalar(false, P->dts, INFINITY, st, nb));
+    if (parts) {
+      if (prof_on()) prof_mark_begin(st);
+      QJ_TRY(launch_stars_prepare(pos, n_s * nb, nullptr, m_s, geom(P), q, P->sb, st));
+      QJ_TRY(launch_bucket_sort(n_s, n_pencils(P, q), bucket_nv(P, q), P->sb, st, nb,
+                                P->bstart_stride));
+      if (prof_on()) prof_mark_end(7, st);
+    }
+    return 0;
+  }
+  Phase density() const {
     FusedArgs a = fused_args(P, q, M_DENSITY);
     a.psi = psi;
     if (parts) set_stars(a, P);
     a.rho_src = rho_src;
     a.half = 1;  // the passes after it read k <= n/2 of R
-    QJ_TRY(launch_fused(M_DENSITY, P->n[q], a, st));
+    return {M_DENSITY, q, a};
   }
+  int step_begin(int k, cudaStream_t st) {
+    if (k < nsteps) QJ_TRY(ensure_prop(P, drift_dt(k), st));
+    return 0;
+  }
+  Phase fft_fwd() const {
+    FusedArgs a = fused_args(P, 1, M_FFT_FWD);
+    half_spectrum(a, P, q);
+    return {M_FFT_FWD, 1, a};
+  }
+  Phase poisson(int k) const {
+    FusedArgs a = fused_args(P, r(), M_POISSON);
+    a.half = 1;
+    half_spectrum(a, P, q);
+    a.part_in = P->part;
+    a.n_part = density_parts(P, q);
+    if (use_phi) {
+      a.phi = P->phi;
+      a.phi_coef = kick_coef(k, k == nsteps);
+    }
+    return {M_POISSON, r(), a};
+  }
+  Phase ifft2() const {
+    FusedArgs a = fused_args(P, 1, M_IFFT2);
+    a.half = 1;
+    half_spectrum(a, P, q);
+    return {M_IFFT2, 1, a};
+  }
+  Phase kick(int k) const {
+    const bool last = k == nsteps;
+    FusedArgs a = fused_args(P, q, M_KICK);
+    a.psi = psi;
+    // kick k = second half kick of step k-1 and first half kick of step k
+    a.kick_coef = kick_coef(k, last);
+    if (use_phi) {
+      a.phi = P->phi;
+      a.phi_final = last ? 1 : 0;
+    }
+    a.b_coeff = si ? (float)P->ph.b_coeff : 0.0f;
+    a.v_ext = vext;
+    a.rho_src = rho_src;
+    a.do_drift = last ? 0 : 1;
+    if (vsave) a.v_out = vsave + (size_t)k * P->ncell;  // V of kick k (adjoint)
+    if (parts) set_stars(a, P);
+    return {M_KICK, q, a};
+  }
+  // fork: the star update and bucket sort run on the side stream while the y
+  // drift pass runs on st; joined before the next density build
+  int stars(int k, cudaStream_t st) {
+    if (!parts) return 0;
+    const bool last = k == nsteps;
+    QJ_CK(cudaEventRecord(P->ev_kick, st));
+    QJ_CK(cudaStreamWaitEvent(P->side, P->ev_kick, 0));
+    cudaStream_t pst = P->side;
+    if (prof_on()) prof_mark_begin(pst);
+    UpdateArgs u;
+    std::memset(&u, 0, sizeof(u));
+    u.n = n_s * P->nbox;
+    u.box_stars = n_s;
+    u.dt = dt;
+    u.k2 = k > 0;
+    u.k1 = !last;
+    u.drift = !last;
+    u.dts_bits = P->dts;
+    u.q_next = last ? -1 : r();
+    u.m_s = m_s;
+    QJ_TRY(launch_update_fused(pos, vel, geom(P), u, P->sb, pst));
+    if (!last)
+      QJ_TRY(launch_bucket_sort(n_s, n_pencils(P, r()), bucket_nv(P, r()), P->sb, pst, P->nbox,
+                                P->bstart_stride));
+    if (prof_on()) prof_mark_end(8, pst);
+    QJ_CK(cudaEventRecord(P->ev_parts, pst));
+    return 0;
+  }
+  Phase drift() const {
+    FusedArgs a = fused_args(P, 1, M_DRIFT);
+    a.psi = psi;
+    return {M_DRIFT, 1, a};
+  }
+  int join(cudaStream_t st) {
+    if (parts) QJ_CK(cudaStreamWaitEvent(st, P->ev_parts, 0));
+    return 0;
+  }
+  Phase drift_density() const {
+    FusedArgs a = fused_args(P, r(), M_DRIFT_DENSITY);
+    a.psi = psi;
+    if (parts) set_stars(a, P);
+    a.rho_src = rho_src;
+    a.half = 1;  // the passes after it read k <= n/2 of R
+    return {M_DRIFT_DENSITY, r(), a};
+  }
+  int step_end(int k, cudaStream_t st) {
+    if (save)  // the state after drift k (before kick k + 1), for the adjoint
+      QJ_CK(cudaMemcpyAsync((char *)save + (size_t)k * P->ncell * P->csz, psi,
+                            P->ncell * P->csz, cudaMemcpyDeviceToDevice, st));
+    q = r();
+    return 0;
+  }
+  int end(cudaStream_t st) {
+    QJ_TRY(join(st));
+    return launch_diag_store(false, diag, P->amax, P->dts, parts ? 1 : 0, nsteps * dt, st,
+                             P->nbox);
+  }
+};
+
+int fused_kdk(qj_plan *P, float2 *psi, float *pos, float *vel, int n_s, double m_s, double dt,
+              int nsteps, int si, const float *vext, double *diag, cudaStream_t st,
+              const StepCoefs *sc = nullptr, void *save = nullptr, float *vsave = nullptr,
+              const float *rho_src = nullptr) {
+  KdkRun R{P, psi, pos, vel, n_s, m_s, dt, nsteps, si, vext, diag, sc, save, vsave, rho_src};
+  QJ_TRY(R.begin(st));
+  QJ_TRY(run_phase(P, R.density(), st));
   for (int k = 0; k <= nsteps; ++k) {
-    const int r = 2 - q;
-    const bool last = (k == nsteps);
-    if (!last) QJ_TRY(ensure_prop(P, drift_dt(k), st));
-    {
-      FusedArgs a = fused_args(P, 1, M_FFT_FWD);
-      half_spectrum(a, P, q);
-      QJ_TRY(launch_fused(M_FFT_FWD, P->n[1], a, st));
-    }
-    {
-      FusedArgs a = fused_args(P, r, M_POISSON);
-      a.half = 1;
-      half_spectrum(a, P, q);
-      a.part_in = P->part;
-      a.n_part = density_parts(P, q);
-      if (use_phi) {
-        a.phi = P->phi;
-        a.phi_coef = kick_coef(k, last);
-      }
-      QJ_TRY(launch_fused(M_POISSON, P->n[r], a, st));
-    }
-    {
-      FusedArgs a = fused_args(P, 1, M_IFFT2);
-      a.half = 1;
-      half_spectrum(a, P, q);
-      QJ_TRY(launch_fused(M_IFFT2, P->n[1], a, st));
-    }
-    {
-      FusedArgs a = fused_args(P, q, M_KICK);
-      a.psi = psi;
-      // kick k = second half kick of step k-1 and first half kick of step k
-      a.kick_coef = kick_coef(k, last);
-      if (use_phi) {
-        a.phi = P->phi;
-        a.phi_final = last ? 1 : 0;
-      }
-      a.b_coeff = si ? (float)P->ph.b_coeff : 0.0f;
-      a.v_ext = vext;
-      a.rho_src = rho_src;
-      a.do_drift = last ? 0 : 1;
-      if (vsave) a.v_out = vsave + (size_t)k * P->ncell;  // V of kick k (adjoint)
-      if (parts) set_stars(a, P);
-      QJ_TRY(launch_fused(M_KICK, P->n[q], a, st));
-    }
-    if (parts) {
-      // fork: the star update and bucket sort run on the side stream while
-      // the y drift pass runs on st; joined before the next density build
-      QJ_CK(cudaEventRecord(P->ev_kick, st));
-      QJ_CK(cudaStreamWaitEvent(P->side, P->ev_kick, 0));
-      cudaStream_t pst = P->side;
-      if (prof_on()) prof_mark_begin(pst);
-      UpdateArgs u;
-      std::memset(&u, 0, sizeof(u));
-      u.n = n_s * nb;
-      u.box_stars = n_s;
-      u.dt = dt;
-      u.k2 = k > 0;
-      u.k1 = !last;
-      u.drift = !last;
-      u.dts_bits = P->dts;
-      u.q_next = last ? -1 : r;
-      u.m_s = m_s;
-      QJ_TRY(launch_update_fused(pos, vel, geom(P), u, P->sb, pst));
-      if (!last)
-        QJ_TRY(launch_bucket_sort(n_s, n_pencils(P, r), bucket_nv(P, r), P->sb, pst, nb,
-                                  P->bstart_stride));
-      if (prof_on()) prof_mark_end(8, pst);
-      QJ_CK(cudaEventRecord(P->ev_parts, pst));
-    }
-    if (!last) {
-      {
-        FusedArgs a = fused_args(P, 1, M_DRIFT);
-        a.psi = psi;
-        QJ_TRY(launch_fused(M_DRIFT, P->n[1], a, st));
-      }
-      {
-        FusedArgs a = fused_args(P, r, M_DRIFT_DENSITY);
-        a.psi = psi;
-        if (parts) {
-          QJ_CK(cudaStreamWaitEvent(st, P->ev_parts, 0));
-          set_stars(a, P);
-        }
-        a.rho_src = rho_src;
-        a.half = 1;  // the passes after it read k <= n/2 of R
-        QJ_TRY(launch_fused(M_DRIFT_DENSITY, P->n[r], a, st));
-      }
-      if (save)  // the state after drift k (before kick k + 1), for the adjoint
-        QJ_CK(cudaMemcpyAsync((char *)save + (size_t)k * P->ncell * P->csz, psi,
-                              P->ncell * P->csz, cudaMemcpyDeviceToDevice, st));
-    }
-    q = r;
+    QJ_TRY(R.step_begin(k, st));
+    QJ_TRY(run_phase(P, R.fft_fwd(), st));
+    QJ_TRY(run_phase(P, R.poisson(k), st));
+    QJ_TRY(run_phase(P, R.ifft2(), st));
+    QJ_TRY(run_phase(P, R.kick(k), st));
+    QJ_TRY(R.stars(k, st));
+    if (k == nsteps) break;
+    QJ_TRY(run_phase(P, R.drift(), st));
+    QJ_TRY(R.join(st));
+    QJ_TRY(run_phase(P, R.drift_density(), st));
+    QJ_TRY(R.step_end(k, st));
   }
-  if (parts) QJ_CK(cudaStreamWaitEvent(st, P->ev_parts, 0));
-  return launch_diag_store(false, diag, P->amax, P->dts, parts ? 1 : 0, nsteps * dt, st, nb);
+  return R.end(st);
 }
 
 // ---------------------------------------------------------------------------
@@ -1748,12 +1813,18 @@ int qj_kdk_step(qj_plan *P, void *psi, void *pos, void *vel, int n_s, double m_s
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
-// Ensembles: several batched plans (one per box size) stepped concurrently,
-// one stream each, with the fork/join step body captured once into a CUDA
-// graph and replayed.
+// Ensembles: several batched plans (one per box size) stepped together, with
+// the step body captured once into a CUDA graph and replayed.  By default each
+// plan steps on its own stream.  With merge on and the plans' sizes distinct
+// cubes of 64, 96 and 128 (the sizes that share a CTA shape), every fused pass
+// is instead one launch for all plans' boxes (launch_fused_ens); that gives
+// the same bits but measured slower on the 32-box mix (1.07 vs 0.95 ms per
+// step): each pass then ends for all sizes together, while the streams let one
+// size's pass overlap another size's next one.
 // ---------------------------------------------------------------------------
 struct qj_ensemble {
   std::vector<qj_plan *> plans;
+  bool merge = false;  // use ensemble launches when the plans allow them
   std::vector<cudaStream_t> streams;
   cudaStream_t origin = nullptr;
   cudaEvent_t fork = nullptr, done = nullptr, caller = nullptr;
@@ -1774,7 +1845,71 @@ struct EnsArgs {
   qj_diag *const *diag;
 };
 
+// The plans fit ensemble launches: at most one plan per size class, each a
+// cube of a class size, no shape variants in their tuning.
+bool ens_mergeable(const qj_ensemble *E) {
+  if (!E->merge || E->plans.empty() || (int)E->plans.size() > kEnsClasses) return false;
+  bool used[kEnsClasses] = {false, false, false};
+  for (const qj_plan *P : E->plans) {
+    const int s = ens_slot(P->n[0]);
+    if (s < 0 || used[s] || P->n[1] != P->n[0] || P->n[2] != P->n[0] ||
+        P->tune[QJ_TUNE_RADIX] != 0 || P->tune[QJ_TUNE_TILE] != 0)
+      return false;
+    used[s] = true;
+  }
+  return true;
+}
+
+// m steps of every plan with one launch per fused pass for all of them: the
+// phases of fused_kdk (KdkRun), each run for all plans before the next.  The
+// plans' star updates and sorts run on their own side streams, forked after
+// the kick and joined before the drift + density pass, as in fused_kdk.
+int ensemble_merged_body(qj_ensemble *E, const EnsArgs &a, int m) {
+  const int np = (int)E->plans.size();
+  cudaStream_t st = E->origin;
+  std::vector<KdkRun> runs;
+  int reserve = 0;
+  for (int i = 0; i < np; ++i) {
+    qj_plan *P = E->plans[i];
+    runs.push_back(KdkRun{P, (float2 *)a.psi[i], (float *)(a.n_s[i] ? a.pos[i] : nullptr),
+                          (float *)(a.n_s[i] ? a.vel[i] : nullptr), a.n_s[i], a.m_s[i], a.dt[i], m,
+                          0, nullptr, (double *)a.diag[i], nullptr, nullptr, nullptr, nullptr});
+    // each plan with stars keeps its own free CTA slots for its side stream
+    if (a.n_s[i] > 0) reserve += P->tune[8] >= 0 ? P->tune[8] : 2;
+  }
+  FusedArgs fa[kEnsClasses];
+  int fn[kEnsClasses];
+  auto phase = [&](auto &&get) -> int {
+    int mode = 0;
+    for (int i = 0; i < np; ++i) {
+      const Phase ph = get(runs[i]);
+      mode = ph.mode;
+      fa[i] = ph.a;
+      fn[i] = runs[i].P->n[ph.axis];
+    }
+    return launch_fused_ens(mode, np, fa, fn, reserve, st);
+  };
+  for (KdkRun &R : runs) QJ_TRY(R.begin(st));
+  QJ_TRY(phase([](KdkRun &R) { return R.density(); }));
+  for (int k = 0; k <= m; ++k) {
+    for (KdkRun &R : runs) QJ_TRY(R.step_begin(k, st));
+    QJ_TRY(phase([](KdkRun &R) { return R.fft_fwd(); }));
+    QJ_TRY(phase([k](KdkRun &R) { return R.poisson(k); }));
+    QJ_TRY(phase([](KdkRun &R) { return R.ifft2(); }));
+    QJ_TRY(phase([k](KdkRun &R) { return R.kick(k); }));
+    for (KdkRun &R : runs) QJ_TRY(R.stars(k, st));
+    if (k == m) break;
+    QJ_TRY(phase([](KdkRun &R) { return R.drift(); }));
+    for (KdkRun &R : runs) QJ_TRY(R.join(st));
+    QJ_TRY(phase([](KdkRun &R) { return R.drift_density(); }));
+    for (KdkRun &R : runs) QJ_TRY(R.step_end(k, st));
+  }
+  for (KdkRun &R : runs) QJ_TRY(R.end(st));
+  return 0;
+}
+
 int ensemble_body(qj_ensemble *E, const EnsArgs &a, int m) {
+  if (ens_mergeable(E)) return ensemble_merged_body(E, a, m);
   QJ_CK(cudaEventRecord(E->fork, E->origin));
   for (size_t i = 0; i < E->plans.size(); ++i) {
     QJ_CK(cudaStreamWaitEvent(E->streams[i], E->fork, 0));
@@ -1841,6 +1976,23 @@ int qj_ensemble_destroy(qj_ensemble *E) {
   return QJ_OK;
 }
 
+int qj_ensemble_set_merge(qj_ensemble *E, int on) {
+  if (!E) {
+    set_error("qj_ensemble_set_merge: bad argument");
+    return QJ_ERR_ARG;
+  }
+  E->merge = on != 0;
+  return QJ_OK;
+}
+
+int qj_ensemble_merged(const qj_ensemble *E) {
+  if (!E) {
+    set_error("qj_ensemble_merged: bad argument");
+    return QJ_ERR_ARG;
+  }
+  return ens_mergeable(E) ? 1 : 0;
+}
+
 int qj_ensemble_step(qj_ensemble *E, void *const *psi, void *const *pos, void *const *vel,
                      const int *n_s, const double *m_s, const double *dt, qj_diag *const *diag,
                      int nsteps, int chunk, int use_graph, void *stream) {
@@ -1864,6 +2016,7 @@ int qj_ensemble_step(qj_ensemble *E, void *const *psi, void *const *pos, void *c
   const int full = nsteps / chunk, rem = nsteps % chunk;
   if (use_graph && full > 0) {
     std::vector<const void *> key;
+    key.push_back((const void *)(intptr_t)(ens_mergeable(E) ? 1 : 0));
     for (size_t i = 0; i < np; ++i) {
       key.push_back(psi[i]);
       key.push_back(n_s[i] ? pos[i] : nullptr);

@@ -107,7 +107,7 @@ struct FusedArgs {
   const int *tune;
   // set to nonzero when a pass gave up waiting for a tile copy
   unsigned *err;
-  // batched boxes (blockIdx.y = box): per-box strides of the fields (cells),
+  // batched boxes (CtaPos::box): per-box strides of the fields (cells),
   // stars, bucket starts, partial sums; a_max is per box
   int nbox;  // launch grid.y (0 or 1 = one box)
   long long box_cells;
@@ -116,9 +116,25 @@ struct FusedArgs {
   int box_part;
 };
 
-// Offset a pass' pointers to box blockIdx.y of a batched plan.
-__device__ __forceinline__ void select_box(FusedArgs &a) {
-  const int b = blockIdx.y;
+// A CTA's place in its pass: box box(), slot bx() of the gx() persistent
+// CTAs that stride over that box's tiles.  k_fused reads them from its grid
+// (GridCta: blockIdx.y, blockIdx.x, gridDim.x, re-read where used, as the
+// special registers they are); an ensemble launch assigns them from the size
+// class's CTA range (CtaPos).
+struct GridCta {
+  __device__ __forceinline__ int bx() const { return (int)blockIdx.x; }
+  __device__ __forceinline__ int box() const { return (int)blockIdx.y; }
+  __device__ __forceinline__ int gx() const { return (int)gridDim.x; }
+};
+struct CtaPos {
+  int bx_, box_, gx_;
+  __device__ __forceinline__ int bx() const { return bx_; }
+  __device__ __forceinline__ int box() const { return box_; }
+  __device__ __forceinline__ int gx() const { return gx_; }
+};
+
+// Offset a pass' pointers to box b of a batched plan.
+__device__ __forceinline__ void select_box(FusedArgs &a, int b) {
   if (b == 0) return;
   const long long c = (long long)b * a.box_cells;
   if (a.psi) a.psi += c;
@@ -484,7 +500,7 @@ __device__ __forceinline__ float2 phase_rotate(float2 z, double theta) {
 // ---------------------------------------------------------------------------
 // Streaming tiles through shared memory.
 //
-// The CTAs of a pass are persistent (tile = blockIdx.x + k gridDim.x).  A
+// The CTAs of a pass are persistent (tile = bx + k gx, see GridCta).  A
 // pass reads its input fields tile by tile through one landing buffer: while
 // the CTA transforms one field of one tile, bulk copies (cp.async.bulk into
 // this CTA's own shared memory, completion counted in bytes on an mbarrier)
@@ -612,7 +628,7 @@ __device__ __forceinline__ long long tile_origin(const FusedArgs &a, int tile, i
 // starting at row h.
 template <int N, bool CONTIG, int MODE, int V>
 __device__ __forceinline__ void issue_tile(const FusedArgs &a, const TileMaps &maps, int f, int tile,
-                                           float2 *land, unsigned long long *bar) {
+                                           int box, float2 *land, unsigned long long *bar) {
   using L = Landing<N, CONTIG, V>;
   constexpr int T = PassShape<N, CONTIG, V>::THREADS, TP = PassShape<N, CONTIG, V>::TP;
   constexpr unsigned MASK = T >= 32 ? 0xffffffffu : ((1u << T) - 1u);
@@ -636,7 +652,7 @@ __device__ __forceinline__ void issue_tile(const FusedArgs &a, const TileMaps &m
     }
   } else {
     if (lane == 0) {
-      const int z0 = (tile % a.ztiles) * TP, o = tile / a.ztiles, box = blockIdx.y;
+      const int z0 = (tile % a.ztiles) * TP, o = tile / a.ztiles;
       const unsigned long long map = reinterpret_cast<unsigned long long>(&maps.m[f]);
 #pragma unroll
       for (int h = 0; h < N; h += 256) {
@@ -655,11 +671,11 @@ __device__ __forceinline__ void issue_tile(const FusedArgs &a, const TileMaps &m
 // this thread's elements (and element 0 of its pencil, c0), release the
 // buffer to the next copy and start that copy.  Returns false on every
 // thread of the CTA if the wait gave up (the error word is set).
-template <int N, bool CONTIG, int MODE, int V, int E>
+template <int N, bool CONTIG, int MODE, int V, int E, class CTA>
 __device__ __forceinline__ bool take_tile(float2 (&v)[E], float2 &c0, const FusedArgs &a,
                                           const TileMaps &maps, float2 *land,
                                           unsigned long long *bar, unsigned &parity, int &f, int tile,
-                                          int p, int t) {
+                                          int p, int t, const CTA &cta) {
   using L = Landing<N, CONTIG, V>;
   constexpr int P = N / E, NF = stream_count<MODE>();
   bool ok = mbar_wait_bounded(bar, parity);
@@ -684,18 +700,21 @@ __device__ __forceinline__ bool take_tile(float2 (&v)[E], float2 &c0, const Fuse
   int nf = f + 1, nt = tile;
   if (nf == NF) {
     nf = 0;
-    nt = tile + gridDim.x;
+    nt = tile + cta.gx();
   }
   f = nf;
   if (nt < a.ntiles && threadIdx.x < 32)
-    issue_tile<N, CONTIG, MODE, V>(a, maps, nf, a.rev ? a.ntiles - 1 - nt : nt, land, bar);
+    issue_tile<N, CONTIG, MODE, V>(a, maps, nf, a.rev ? a.ntiles - 1 - nt : nt, cta.box(), land, bar);
   return true;
 }
 
-template <int N, bool CONTIG, int MODE, int SV = 0>
-__global__ void __launch_bounds__(PassShape<N, CONTIG, SV>::THREADS, PassShape<N, CONTIG, SV>::MINB)
-    k_fused(FusedArgs a, const __grid_constant__ TileMaps maps) {
-  select_box(a);
+// The body of a fused pass for one CTA: k_fused runs it with the CTA's own
+// grid position; an ensemble launch runs the body of each CTA's size class.
+// maps must live in parameter space (__grid_constant__) or global memory:
+// the tile copies take its address.
+template <int N, bool CONTIG, int MODE, int SV, class CTA>
+__device__ __forceinline__ void fused_body(FusedArgs &a, const TileMaps &maps, const CTA cta) {
+  select_box(a, cta.box());
   using SH = PassShape<N, CONTIG, SV>;
   using LAY = FusedSmem<N, CONTIG, MODE, SV>;
   constexpr int E = SH::E, P = SH::P, TP = SH::TP, THREADS = SH::THREADS;
@@ -743,11 +762,11 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG, SV>::THREADS, PassShape<N
   unsigned parity = 0;
   int fld = 0;
   if constexpr (LAY::LANDS)
-    if ((int)blockIdx.x < a.ntiles && tid < 32)
-      issue_tile<N, CONTIG, MODE, SV>(a, maps, 0, a.rev ? a.ntiles - 1 - (int)blockIdx.x : (int)blockIdx.x,
-                                  land, &lbar);
+    if (cta.bx() < a.ntiles && tid < 32)
+      issue_tile<N, CONTIG, MODE, SV>(a, maps, 0, a.rev ? a.ntiles - 1 - cta.bx() : cta.bx(),
+                                      cta.box(), land, &lbar);
 
-  for (int it = blockIdx.x; it < a.ntiles; it += gridDim.x) {
+  for (int it = cta.bx(); it < a.ntiles; it += cta.gx()) {
     const int tile = a.rev ? a.ntiles - 1 - it : it;  // logical tile
     const PencilPos pp = pencil_pos<CONTIG>(a, tile, p, TP);
     const long long base = pp.base, st = a.stride;
@@ -759,7 +778,8 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG, SV>::THREADS, PassShape<N
       if (a.has_stars) sr = star_ranges(a, pp);
     float2 c0;
 #define QJ_TAKE(v) \
-  if (!take_tile<N, CONTIG, MODE, SV, E>(v, c0, a, maps, land, &lbar, parity, fld, it, p, t)) return
+  if (!take_tile<N, CONTIG, MODE, SV, E, CTA>(v, c0, a, maps, land, &lbar, parity, fld, it, p, t, cta)) \
+  return
 
     if constexpr (MODE == M_DENSITY) {
       float2 v[E];
@@ -1091,6 +1111,12 @@ __global__ void __launch_bounds__(PassShape<N, CONTIG, SV>::THREADS, PassShape<N
     }
 #undef QJ_TAKE
   }
+}
+
+template <int N, bool CONTIG, int MODE, int SV = 0>
+__global__ void __launch_bounds__(PassShape<N, CONTIG, SV>::THREADS, PassShape<N, CONTIG, SV>::MINB)
+    k_fused(FusedArgs a, const __grid_constant__ TileMaps maps) {
+  fused_body<N, CONTIG, MODE, SV>(a, maps, GridCta{});
 }
 
 // Generic in-place FFT pass over a complex field (plain path and qj_fft3d).

@@ -48,6 +48,8 @@ SIGNATURES = {
                                        ctypes.POINTER(QjPhys), c_int, c_int, c_int]),
     "qj_ensemble_create": (c_int, [ctypes.POINTER(c_void_p), ctypes.POINTER(c_void_p), c_int]),
     "qj_ensemble_destroy": (c_int, [c_void_p]),
+    "qj_ensemble_set_merge": (c_int, [c_void_p, c_int]),
+    "qj_ensemble_merged": (c_int, [c_void_p]),
     "qj_ensemble_step": (c_int, [c_void_p, ctypes.POINTER(c_void_p), ctypes.POINTER(c_void_p),
                                  ctypes.POINTER(c_void_p), ctypes.POINTER(c_int),
                                  ctypes.POINTER(c_double), ctypes.POINTER(c_double),

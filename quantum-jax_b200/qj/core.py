@@ -419,13 +419,34 @@ class Plan:
 class Ensemble:
     """Independent boxes of uneven size stepped together: one batched plan per
     size, each on its own stream, with the step body captured once in a CUDA
-    graph and replayed (qj_ensemble_step)."""
+    graph and replayed (qj_ensemble_step).  ``merge=True`` runs each fused
+    pass as one persistent launch for all plans instead, when they are cubes
+    of distinct sizes among 64, 96 and 128 (``merged`` tells); same bits,
+    measured slower than the streams."""
 
-    def __init__(self, plans):
+    def __init__(self, plans, merge=False):
         self.plans = list(plans)
         self._h = ctypes.c_void_p()
         arr = (ctypes.c_void_p * len(self.plans))(*[p._h.value for p in self.plans])
         check(lib().qj_ensemble_create(ctypes.byref(self._h), arr, len(self.plans)))
+        self.merge = merge
+
+    @property
+    def merge(self):
+        return self._merge
+
+    @merge.setter
+    def merge(self, on):
+        check(lib().qj_ensemble_set_merge(self._h, int(bool(on))))
+        self._merge = bool(on)
+
+    @property
+    def merged(self):
+        """True when a step runs one launch per fused pass for all plans."""
+        rc = lib().qj_ensemble_merged(self._h)
+        if rc < 0:
+            check(rc)
+        return rc == 1
 
     def step(self, psi, pos, vel, diag, dt, m_s, nsteps, chunk=10, graph=True):
         """psi / pos / vel / diag: per-plan tensors as for a batched

@@ -92,18 +92,57 @@ def test_ensemble_graph_matches_eager_and_oracle():
         pl.close()
 
 
+def test_single_launch_per_pass_equals_per_plan_streams():
+    """Plans of 64^3, 96^3 and 128^3 share one launch per fused pass; that
+    gives the same bits as stepping each plan on its own stream, eager and
+    graph-captured, with stars on some plans and none on another."""
+    import qj
+
+    groups = [boxes(64, [140, 141, 142], 64), boxes(96, [143, 144], 32), boxes(128, [145], 0)]
+    plans = [plan_for(bx, len(bx)) for bx in groups]
+    results = []
+    for merge, graph in ((True, True), (True, False), (False, True)):
+        state = [tensors(bx) for bx in groups]
+        ens = qj.Ensemble(plans, merge=merge)
+        assert ens.merged == merge
+        m_s = [bx[0][4].m_s for bx in groups]
+        pos = [s[1] if bx[0][1].shape[0] else None for s, bx in zip(state, groups)]
+        vel = [s[2] if bx[0][1].shape[0] else None for s, bx in zip(state, groups)]
+        ens.step([s[0] for s in state], pos, vel, [s[3] for s in state], [s[4] for s in state],
+                 m_s, 7, chunk=3, graph=graph)
+        torch.cuda.synchronize()
+        for pl in plans:
+            pl.status()
+        results.append(state)
+        ens.close()
+    for other in results[1:]:
+        for sa, sb in zip(results[0], other):
+            for x, y in zip(sa[:4], sb[:4]):
+                assert torch.equal(x, y)
+    # and a plan with a shape variant in its tuning keeps the per-plan streams
+    t = plans[2].tuning
+    t[11] = 1 << 2
+    plans[2].tuning = t
+    ens = qj.Ensemble(plans, merge=True)
+    assert not ens.merged
+    ens.close()
+    for pl in plans:
+        pl.close()
+
+
 def test_ensemble_every_box_of_the_32_box_mix():
     """The 32-box mix (16 x 64^3, 8 x 96^3, 8 x 128^3, 256 stars each), 10
-    graph-captured steps: every box against the plain float64 path (itself
-    matched to the oracle), and the first 128^3 box against the float64
-    oracle directly."""
+    graph-captured steps as one launch per fused pass for all sizes: every box
+    against the plain float64 path (itself matched to the oracle), and the
+    first 128^3 box against the float64 oracle directly."""
     import qj
 
     groups = [boxes(64, range(100, 116), 256), boxes(96, range(116, 124), 256),
               boxes(128, range(124, 132), 256)]
     state = [tensors(bx) for bx in groups]
     plans = [plan_for(bx, len(bx)) for bx in groups]
-    ens = qj.Ensemble(plans)
+    ens = qj.Ensemble(plans, merge=True)
+    assert ens.merged
     nsteps = 10
     m_s = [bx[0][4].m_s for bx in groups]
     ens.step([s[0] for s in state], [s[1] for s in state], [s[2] for s in state],
