@@ -722,7 +722,10 @@ __device__ __forceinline__ void fused_body(FusedArgs &a, const TileMaps &maps, c
   float2 *sm = reinterpret_cast<float2 *>(smem_raw);
   float2 *tw_s = reinterpret_cast<float2 *>(smem_raw + LAY::TW);
   float2 *save = reinterpret_cast<float2 *>(smem_raw + LAY::SAVE);  // per-thread slots
-  float2 *tab2 = reinterpret_cast<float2 *>(smem_raw + LAY::TAB);  // drift propagator
+  // the drift propagator, staged once per CTA: read from shared memory by
+  // every pencil (from global memory, through L1 beside the spill traffic, it
+  // cost the kick 6 us and the y drift 4.5 us at 256^3)
+  float2 *tab2 = reinterpret_cast<float2 *>(smem_raw + LAY::TAB);
   float *tabk = reinterpret_cast<float *>(smem_raw + LAY::TAB);    // Poisson: k, then k~
   float2 *land = reinterpret_cast<float2 *>(
       smem_raw + ((LAY::LAND + smem_addr(smem_raw) + 127) & ~(size_t)127) - smem_addr(smem_raw));
@@ -1063,7 +1066,7 @@ __device__ __forceinline__ void fused_body(FusedArgs &a, const TileMaps &maps, c
 #pragma unroll
         for (int e = 0; e < E; ++e) a.v_out[gb + e * gs] = V[e];
       }
-      if (a.do_drift) drift_pencil<N, E, P, THREADS>(ps, c0, a.prop, t, smv, tw, save);
+      if (a.do_drift) drift_pencil<N, E, P, THREADS>(ps, c0, tab2, t, smv, tw, save);
       store_pencil<E>(ps, a.psi, base, st, t, P);
       if constexpr (THREADS >= 32) {
 #pragma unroll
@@ -1096,7 +1099,7 @@ __device__ __forceinline__ void fused_body(FusedArgs &a, const TileMaps &maps, c
     } else if constexpr (MODE == M_DRIFT || MODE == M_DRIFT_DENSITY) {
       float2 v[E];
       QJ_TAKE(v);
-      drift_pencil<N, E, P, THREADS>(v, c0, a.prop, t, smv, tw, save);
+      drift_pencil<N, E, P, THREADS>(v, c0, tab2, t, smv, tw, save);
       store_pencil<E>(v, a.psi, base, st, t, P);
       if constexpr (MODE == M_DRIFT_DENSITY) {
         double s = build_density<N, E>(v, a, pp, sr, t, P);
