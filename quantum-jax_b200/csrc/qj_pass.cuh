@@ -375,6 +375,53 @@ __device__ __forceinline__ void for_star_corners(const FusedArgs &a, StarRanges 
   }
 }
 
+// The kick's star corners: f(s, corner, slot) for each corner of each star
+// on this pencil, where slot indexes the save slots ([E][THREADS], written by
+// the corners' owners) at the corner's cell.  The writes f makes do not
+// depend on their order (each star corner and axis has one writer).  Along z
+// (CONTIG) a pencil's P threads sit in one warp and split its stars between
+// them, one lookup per star instead of one per thread; the caller syncs the
+// pencil's lanes around the call (pencil_lanes).  Along x / y the pencil's
+// threads span several warps, and each corner's owner visits it.
+__device__ __forceinline__ unsigned pencil_lanes(int P) {
+  const int lane = threadIdx.x & 31;
+  return P >= 32 ? 0xffffffffu : (((1u << P) - 1u) << ((lane / P) * P));
+}
+template <int N, bool CONTIG, int THREADS, class F>
+__device__ __forceinline__ void kick_star_corners(const FusedArgs &a, const StarRanges &r, int t,
+                                                  int P, F &&f) {
+  const int tid = threadIdx.x;
+  if constexpr (!CONTIG) {
+    for_star_corners<N, false>(a, r, t, P, [&](unsigned s, int cbits, int m, float, float, float, float) {
+      f(s, cbits, (m / P) * THREADS + tid);
+    });
+  } else {
+    const int q = a.axis, base = tid - t;
+    const int n0 = r.hi[0] - r.lo[0], n1 = r.hi[1] - r.lo[1], n2 = r.hi[2] - r.lo[2];
+    const int total = n0 + n1 + n2 + (r.hi[3] - r.lo[3]);
+    for (int j = t; j < total; j += P) {
+      const int idx = j < n0               ? r.lo[0] + j
+                      : j < n0 + n1        ? r.lo[1] + (j - n0)
+                      : j < n0 + n1 + n2   ? r.lo[2] + (j - n0 - n1)
+                                           : r.lo[3] + (j - n0 - n1 - n2);
+      const unsigned s = a.perm[idx];
+      const int4 id = a.sidx[s];
+      const int bu = (r.cu == sel3(id.x, id.y, id.z, r.u)) ? 0 : 1;
+      const int bv = (r.cv == sel3(id.x, id.y, id.z, r.v)) ? 0 : 1;
+      const int q0 = sel3(id.x, id.y, id.z, q);
+#pragma unroll
+      for (int cq = 0; cq < 2; ++cq) {
+        int m = q0 + cq;
+        if (m >= N) m -= N;
+        const int bx = q == 0 ? cq : (r.u == 0 ? bu : bv);
+        const int by = q == 1 ? cq : (r.u == 1 ? bu : bv);
+        const int bz = q == 2 ? cq : bv;
+        f(s, bx + 2 * by + 4 * bz, (m / P) * THREADS + base + (m % P));
+      }
+    }
+  }
+}
+
 // rho = |psi|^2 + rho_stars (+ rho_gas), element by element (float32 order
 // of quantum-stars.py:299 / quantum-gas-bh.py:542).  The star density of a
 // cell is summed from zero in star order in the (still zero) imaginary slot,
@@ -980,16 +1027,18 @@ __device__ __forceinline__ void fused_body(FusedArgs &a, const TileMaps &maps, c
 #pragma unroll
         for (int e = 0; e < E; ++e) am = fmaxf(am, fmaxf(fabsf(v2[e].x), fabsf(v2[e].y)));
         if (pstars) {
-          // the corner lookups index the thread's save slots (free until the drift)
+          // the corner lookups index the pencil's save slots (free until the drift)
 #pragma unroll
           for (int e = 0; e < E; ++e) save[e * THREADS + tid] = v2[e];
-          for_star_corners<N, false>(a, star_ranges(a, pp), t, P,
-                                     [&](unsigned s, int cbits, int m, float, float, float, float) {
-                                       const float2 w = save[(m / P) * THREADS + tid];
-                                       float *dst = a.A + 3 * (8 * s + c_corner_of_bits_dev(cbits));
-                                       dst[aq] = w.x;
-                                       dst[1] = w.y;
-                                     });
+          if constexpr (CONTIG) __syncwarp(pencil_lanes(P));
+          kick_star_corners<N, CONTIG, THREADS>(a, star_ranges(a, pp), t, P,
+                                                [&](unsigned s, int cbits, int slot) {
+                                                  const float2 w = save[slot];
+                                                  float *dst = a.A + 3 * (8 * s + c_corner_of_bits_dev(cbits));
+                                                  dst[aq] = w.x;
+                                                  dst[1] = w.y;
+                                                });
+          if constexpr (CONTIG) __syncwarp(pencil_lanes(P));
         }
         if (a.gv[0]) {
           // v += a dt/2 as fire-and-forget adds at L2: each element has one
@@ -1017,11 +1066,13 @@ __device__ __forceinline__ void fused_body(FusedArgs &a, const TileMaps &maps, c
         if (pstars) {
 #pragma unroll
           for (int e = 0; e < E; ++e) save[e * THREADS + tid].x = v1[e].y;
-          for_star_corners<N, false>(a, star_ranges(a, pp), t, P,
-                                     [&](unsigned s, int cbits, int m, float, float, float, float) {
-                                       a.A[3 * (8 * s + c_corner_of_bits_dev(cbits)) + (aq == 0 ? 2 : 0)] =
-                                           save[(m / P) * THREADS + tid].x;
-                                     });
+          if constexpr (CONTIG) __syncwarp(pencil_lanes(P));
+          kick_star_corners<N, CONTIG, THREADS>(a, star_ranges(a, pp), t, P,
+                                                [&](unsigned s, int cbits, int slot) {
+                                                  a.A[3 * (8 * s + c_corner_of_bits_dev(cbits)) +
+                                                      (aq == 0 ? 2 : 0)] = save[slot].x;
+                                                });
+          if constexpr (CONTIG) __syncwarp(pencil_lanes(P));
         }
         if (a.gv[0]) {  // gas half kick, quantum-gas-bh.py:255-266 (adds as above)
           float *g = aq == 0 ? a.gv[2] : a.gv[0];
