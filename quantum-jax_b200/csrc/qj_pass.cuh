@@ -375,9 +375,9 @@ __device__ __forceinline__ void for_star_corners(const FusedArgs &a, StarRanges 
   }
 }
 
-// The kick's star corners: f(s, corner, slot) for each corner of each star
-// on this pencil, where slot indexes the save slots ([E][THREADS], written by
-// the corners' owners) at the corner's cell.  The writes f makes do not
+// The kick's star corners: f(s, corner, slot, m) for each corner of each
+// star on this pencil, at element m of the pencil, where slot indexes the
+// save slots ([E][THREADS], written by the corners' owners) at that cell.  The writes f makes do not
 // depend on their order (each star corner and axis has one writer).  Along z
 // (CONTIG) a pencil's P threads sit in one warp and split its stars between
 // them, one lookup per star instead of one per thread; the caller syncs the
@@ -393,7 +393,7 @@ __device__ __forceinline__ void kick_star_corners(const FusedArgs &a, const Star
   const int tid = threadIdx.x;
   if constexpr (!CONTIG) {
     for_star_corners<N, false>(a, r, t, P, [&](unsigned s, int cbits, int m, float, float, float, float) {
-      f(s, cbits, (m / P) * THREADS + tid);
+      f(s, cbits, (m / P) * THREADS + tid, m);
     });
   } else {
     const int q = a.axis, base = tid - t;
@@ -416,7 +416,7 @@ __device__ __forceinline__ void kick_star_corners(const FusedArgs &a, const Star
         const int bx = q == 0 ? cq : (r.u == 0 ? bu : bv);
         const int by = q == 1 ? cq : (r.u == 1 ? bu : bv);
         const int bz = q == 2 ? cq : bv;
-        f(s, bx + 2 * by + 4 * bz, (m / P) * THREADS + base + (m % P));
+        f(s, bx + 2 * by + 4 * bz, (m / P) * THREADS + base + (m % P), m);
       }
     }
   }
@@ -1026,19 +1026,11 @@ __device__ __forceinline__ void fused_body(FusedArgs &a, const TileMaps &maps, c
         fft_pencil<N, +1, true>(v2, t, smv, tw);
 #pragma unroll
         for (int e = 0; e < E; ++e) am = fmaxf(am, fmaxf(fabsf(v2[e].x), fabsf(v2[e].y)));
+        // a_q + i a_y wait in the thread's save slots (free until the drift)
+        // for the star corners, looked up once after phase 2
         if (pstars) {
-          // the corner lookups index the pencil's save slots (free until the drift)
 #pragma unroll
           for (int e = 0; e < E; ++e) save[e * THREADS + tid] = v2[e];
-          if constexpr (CONTIG) __syncwarp(pencil_lanes(P));
-          kick_star_corners<N, CONTIG, THREADS>(a, star_ranges(a, pp), t, P,
-                                                [&](unsigned s, int cbits, int slot) {
-                                                  const float2 w = save[slot];
-                                                  float *dst = a.A + 3 * (8 * s + c_corner_of_bits_dev(cbits));
-                                                  dst[aq] = w.x;
-                                                  dst[1] = w.y;
-                                                });
-          if constexpr (CONTIG) __syncwarp(pencil_lanes(P));
         }
         if (a.gv[0]) {
           // v += a dt/2 as fire-and-forget adds at L2: each element has one
@@ -1064,13 +1056,20 @@ __device__ __forceinline__ void fused_body(FusedArgs &a, const TileMaps &maps, c
           am = fmaxf(am, fabsf(v1[e].y));
         }
         if (pstars) {
+          // a_r into the pencil's exchange row, free until the drift's first
+          // exchange: in a transform's last stage each thread reads only the
+          // elements of its own residue t mod P, so no thread still reads the
+          // ones this thread writes
 #pragma unroll
-          for (int e = 0; e < E; ++e) save[e * THREADS + tid].x = v1[e].y;
+          for (int e = 0; e < E; ++e) smv.st(t + P * e, float2{v1[e].y, 0.0f});
           if constexpr (CONTIG) __syncwarp(pencil_lanes(P));
           kick_star_corners<N, CONTIG, THREADS>(a, star_ranges(a, pp), t, P,
-                                                [&](unsigned s, int cbits, int slot) {
-                                                  a.A[3 * (8 * s + c_corner_of_bits_dev(cbits)) +
-                                                      (aq == 0 ? 2 : 0)] = save[slot].x;
+                                                [&](unsigned s, int cbits, int slot, int m) {
+                                                  const float2 w = save[slot];
+                                                  float *dst = a.A + 3 * (8 * s + c_corner_of_bits_dev(cbits));
+                                                  dst[aq] = w.x;
+                                                  dst[1] = w.y;
+                                                  dst[aq == 0 ? 2 : 0] = smv.ld(m).x;
                                                 });
           if constexpr (CONTIG) __syncwarp(pencil_lanes(P));
         }
