@@ -405,7 +405,6 @@ def main():
     clocks = Clocks(local)
     clocks.start()
     time.sleep(0.3)
-    lib.qj_profile_enable(1)
     l0 = lib.qj_launch_count()
     barrier()
     e0 = torch.cuda.Event(enable_timing=True)
@@ -417,14 +416,21 @@ def main():
     launches = int(lib.qj_launch_count() - l0)
     ms = e0.elapsed_time(e1)
     clk = clocks.stop()
+    ms_max = max_over_ranks(ms)
+    value = world * C * a.steps / (ms_max * 1e-3)
+    # the per-pass split: CUDA events around every pass on the launching
+    # stream, in a separate run (events between the passes would also stand
+    # between a pass and its programmatic dependent in the timed run)
     import ctypes
 
+    prof_steps = min(a.steps, 200)
+    lib.qj_profile_enable(1)
+    fused.kdk_step(ps, po, ve, diag, dt, prof_steps, p.m_s)
+    torch.cuda.synchronize()
     pms = (ctypes.c_double * 9)()
     pcnt = (ctypes.c_int64 * 9)()
     lib.qj_profile_read(pms, pcnt, 9)
     lib.qj_profile_enable(0)
-    ms_max = max_over_ranks(ms)
-    value = world * C * a.steps / (ms_max * 1e-3)
 
     # roofline of the dominant pass
     hbm, hbm_kind = peaks()
@@ -741,6 +747,7 @@ def main():
                              "pos_rel_l2_vs_f64": pos_err,
                              "f64_path": "plain float64 GPU path (matches the oracle to 1e-11)"},
                 "roofline": roofline, "step_roofline": step_roof, "passes": per_pass,
+                "passes_note": f"CUDA events around each pass, a separate {prof_steps}-step run",
                 "tuning": tuning,
                 "gpu_launches": launches, "clocks": clk, "e2e": e2e, "cpu_baseline": cb,
                 "adjoint": adjoint, "ensemble": ensemble, "gas_bh": gas_bh}

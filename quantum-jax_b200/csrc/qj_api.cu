@@ -430,9 +430,14 @@ struct KdkRun {
     if (k < nsteps) QJ_TRY(ensure_prop(P, drift_dt(k), st));
     return 0;
   }
+  // The potential's passes (forward y, Poisson, inverse y, kick) each follow
+  // another fused pass directly on the stream, so each launches as its
+  // programmatic dependent (pdl); forward y follows the drift + density pass,
+  // or on the first step the density build or the drift table.
   Phase fft_fwd() const {
     FusedArgs a = fused_args(P, 1, M_FFT_FWD);
     half_spectrum(a, P, q);
+    a.pdl = 1;
     return {M_FFT_FWD, 1, a};
   }
   Phase poisson(int k) const {
@@ -445,12 +450,14 @@ struct KdkRun {
       a.phi = P->phi;
       a.phi_coef = kick_coef(k, k == nsteps);
     }
+    a.pdl = 1;
     return {M_POISSON, r(), a};
   }
   Phase ifft2() const {
     FusedArgs a = fused_args(P, 1, M_IFFT2);
     a.half = 1;
     half_spectrum(a, P, q);
+    a.pdl = 1;
     return {M_IFFT2, 1, a};
   }
   Phase kick(int k) const {
@@ -469,6 +476,7 @@ struct KdkRun {
     a.do_drift = last ? 0 : 1;
     if (vsave) a.v_out = vsave + (size_t)k * P->ncell;  // V of kick k (adjoint)
     if (parts) set_stars(a, P);
+    a.pdl = 1;
     return {M_KICK, q, a};
   }
   // fork: the star update and bucket sort run on the side stream while the y

@@ -155,8 +155,20 @@ int run_fused(const FusedArgs &a, cudaStream_t st) {
   }
   const int nbox = a.nbox > 1 ? a.nbox : 1;
   const int gx = std::max(1, std::min(b.ntiles, (resident - reserve) / nbox));
-  const dim3 grid(gx, nbox);
-  k_fused<N, CONTIG, MODE, V><<<grid, SH::THREADS, smem, st>>>(b, maps);
+  cudaLaunchConfig_t cfg;
+  std::memset(&cfg, 0, sizeof(cfg));
+  cfg.gridDim = dim3(gx, nbox);
+  cfg.blockDim = dim3(SH::THREADS);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  // programmatic dependent launch: the CTAs may start during the previous
+  // pass's last tiles and wait for it (griddepcontrol.wait) before reading
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = a.pdl ? 1 : 0;
+  QJ_CK(cudaLaunchKernelEx(&cfg, k_fused<N, CONTIG, MODE, V>, b, maps));
   QJ_CK_LAUNCH();
   return 0;
 }

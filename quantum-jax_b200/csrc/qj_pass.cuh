@@ -95,6 +95,9 @@ struct FusedArgs {
   // shape variant of the pass (PassShape's V: radix plan, tile width); set
   // with the fields that follow from it (tw, ztiles)
   int shape;
+  // host side only: launch the pass as a programmatic dependent of the kernel
+  // before it on the stream (that kernel must be a fused pass of this step)
+  int pdl;
   // forward y / Poisson passes over half of the real density's spectrum (the
   // other non-y axis to n/2); the Poisson pass then also writes the mirrors
   int half;
@@ -808,6 +811,11 @@ __device__ __forceinline__ void fused_body(FusedArgs &a, const TileMaps &maps, c
   }
   if (tid == 0) mbar_init(&lbar, 1);
   __syncthreads();
+  // The tables above are the plan's own; the previous pass's results are read
+  // from here on.  Launched as a programmatic dependent of that pass, this
+  // CTA may have started (and staged its tables) during the pass's last
+  // tiles: wait until it has completed.  A no-op for a plain launch.
+  asm volatile("griddepcontrol.wait;" ::: "memory");
   const float2 *tw = tw_s;
   unsigned parity = 0;
   int fld = 0;
@@ -817,6 +825,9 @@ __device__ __forceinline__ void fused_body(FusedArgs &a, const TileMaps &maps, c
                                       cta.box(), land, &lbar);
 
   for (int it = cta.bx(); it < a.ntiles; it += cta.gx()) {
+    // this CTA's last tile: a next pass launched as a programmatic dependent
+    // may start its CTAs in the slots that free up from now on
+    if (it + cta.gx() >= a.ntiles) asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     const int tile = a.rev ? a.ntiles - 1 - it : it;  // logical tile
     const PencilPos pp = pencil_pos<CONTIG>(a, tile, p, TP);
     const long long base = pp.base, st = a.stride;
