@@ -507,9 +507,14 @@ struct KdkRun {
     QJ_CK(cudaEventRecord(P->ev_parts, pst));
     return 0;
   }
+  // the y drift follows the kick on the stream (the star fork between them
+  // is an event record, no wait), so it too launches as the kick's
+  // programmatic dependent; the drift + density pass waits for the star
+  // stream's event, and launches plainly
   Phase drift() const {
     FusedArgs a = fused_args(P, 1, M_DRIFT);
     a.psi = psi;
+    a.pdl = 1;
     return {M_DRIFT, 1, a};
   }
   int join(cudaStream_t st) {
