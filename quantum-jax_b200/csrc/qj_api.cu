@@ -701,27 +701,65 @@ int adjoint_sweep(qj_plan *P, const void *ckpt, void *g, int nsteps, int K, doub
         Vj = (const float *)P->adj_V + (size_t)j * P->ncell;
       // W = (L + b) mu: the Poisson operator without the rho_bar shift; mu
       // itself is kept only for the self-interaction term
-      QJ_TRY(launch_adj_mu(P->dbl, g, pre, Vj, coef, si ? mu : nullptr, 4.0 * M_PI * P->ph.G, P->c0,
-                           P->ncell, st));
-      QJ_TRY(fft3d(P, P->c0, -1, st));
-      QJ_TRY(launch_poisson_div(P->dbl, P->c0, ktabs(P), P->ncell, st));
-      QJ_TRY(fft3d(P, P->c0, +1, st));
-      QJ_TRY(launch_adj_update(P->dbl, g, pre, Vj, P->c0, si ? mu : nullptr, P->ph.b_coeff, coef,
-                               P->ncell, st));
-      if (j > 0) {  // adjoint of drift j - 1: the drift with -dt
-        if (P->dbl) {
+      if (P->dbl) {
+        QJ_TRY(launch_adj_mu(P->dbl, g, pre, Vj, coef, si ? mu : nullptr, 4.0 * M_PI * P->ph.G,
+                             P->c0, P->ncell, st));
+        QJ_TRY(fft3d(P, P->c0, -1, st));
+        QJ_TRY(launch_poisson_div(P->dbl, P->c0, ktabs(P), P->ncell, st));
+        QJ_TRY(fft3d(P, P->c0, +1, st));
+        QJ_TRY(launch_adj_update(P->dbl, g, pre, Vj, P->c0, si ? mu : nullptr, P->ph.b_coeff,
+                                 coef, P->ncell, st));
+        if (j > 0) {  // adjoint of drift j - 1: the drift with -dt
           QJ_TRY(fft3d(P, g, -1, st));
           QJ_TRY(launch_drift_mul(P->dbl, g, ktabs(P), -dt, P->ph.m_per_hbar, P->ncell, st));
           QJ_TRY(fft3d(P, g, +1, st));
-        } else {
-          // the separable drift as three fused forward-multiply-inverse passes
-          QJ_TRY(ensure_prop(P, -dt, st));
-          for (int ax = 0; ax < 3; ++ax) {
-            FusedArgs a = fused_args(P, ax, M_DRIFT);
-            a.psi = (float2 *)g;
-            QJ_TRY(launch_fused(M_DRIFT, P->n[ax], a, st));
-          }
         }
+      } else {
+        // the forward step's potential passes with mu as the density: mu,
+        // its partial sums and the z transform (ADJ_SOURCE); forward y;
+        // Poisson along x with no rho_bar shift and the k = 0 term kept in W;
+        // inverse y; then the inverse z transform to W, the g update and the
+        // z part of the drift adjoint (ADJ_UPDATE); the drift adjoint along y
+        // and x (the drift with -dt)
+        const int q = 2, r = 0;
+        if (j > 0) QJ_TRY(ensure_prop(P, -dt, st));
+        FusedArgs a = fused_args(P, q, M_ADJ_SOURCE);
+        a.psi = (float2 *)g;
+        a.adj_pre = (const float2 *)pre;
+        a.adj_V = (const float *)Vj;
+        a.adj_mu = si ? (float *)mu : nullptr;
+        a.kick_coef = coef;
+        a.half = 1;
+        QJ_TRY(launch_fused(M_ADJ_SOURCE, P->n[q], a, st));
+        a = fused_args(P, 1, M_FFT_FWD);
+        half_spectrum(a, P, q);
+        QJ_TRY(launch_fused(M_FFT_FWD, P->n[1], a, st));
+        a = fused_args(P, r, M_POISSON);
+        a.half = 1;
+        half_spectrum(a, P, q);
+        a.part_in = P->part;
+        a.n_part = pass_blocks(P->n[q], q, P->n[0], P->n[1], P->n[2], 0);  // ADJ_SOURCE's tiles
+        a.rho_bar = 0.0;
+        QJ_TRY(launch_fused(M_POISSON, P->n[r], a, st));
+        a = fused_args(P, 1, M_IFFT2);
+        a.half = 1;
+        half_spectrum(a, P, q);
+        QJ_TRY(launch_fused(M_IFFT2, P->n[1], a, st));
+        a = fused_args(P, q, M_ADJ_UPDATE);
+        a.psi = (float2 *)g;
+        a.adj_pre = (const float2 *)pre;
+        a.adj_V = (const float *)Vj;
+        a.adj_mu = si ? (float *)mu : nullptr;
+        a.kick_coef = coef;
+        a.b_coeff = si ? (float)P->ph.b_coeff : 0.0f;
+        a.do_drift = j > 0 ? 1 : 0;
+        QJ_TRY(launch_fused(M_ADJ_UPDATE, P->n[q], a, st));
+        if (j > 0)
+          for (int ax = 1; ax >= 0; --ax) {
+            FusedArgs d = fused_args(P, ax, M_DRIFT);
+            d.psi = (float2 *)g;
+            QJ_TRY(launch_fused(M_DRIFT, P->n[ax], d, st));
+          }
       }
     }
   }

@@ -120,20 +120,22 @@ static int dispatch_mode(int n, const FusedArgs &a, cudaStream_t st) {
   return 1;
 }
 
-// The dense deposit runs along z only.
-static int dispatch_deposit(int n, const FusedArgs &a, cudaStream_t st) {
+// The dense deposit and the adjoint passes run along z only, in the default
+// shape.
+template <int MODE>
+static int dispatch_z_only(int n, const FusedArgs &a, cudaStream_t st) {
   if (a.axis != 2) {
-    set_error("internal: deposit pass must run along z");
+    set_error("internal: pass mode %d must run along z", MODE);
     return 1;
   }
   switch (n) {
-    case 16: return run_fused<16, true, M_DEPOSIT, 0>(a, st);
-    case 32: return run_fused<32, true, M_DEPOSIT, 0>(a, st);
-    case 64: return run_fused<64, true, M_DEPOSIT, 0>(a, st);
-    case 96: return run_fused<96, true, M_DEPOSIT, 0>(a, st);
-    case 128: return run_fused<128, true, M_DEPOSIT, 0>(a, st);
-    case 256: return run_fused<256, true, M_DEPOSIT, 0>(a, st);
-    case 512: return run_fused<512, true, M_DEPOSIT, 0>(a, st);
+    case 16: return run_fused<16, true, MODE, 0>(a, st);
+    case 32: return run_fused<32, true, MODE, 0>(a, st);
+    case 64: return run_fused<64, true, MODE, 0>(a, st);
+    case 96: return run_fused<96, true, MODE, 0>(a, st);
+    case 128: return run_fused<128, true, MODE, 0>(a, st);
+    case 256: return run_fused<256, true, MODE, 0>(a, st);
+    case 512: return run_fused<512, true, MODE, 0>(a, st);
   }
   set_error("unsupported FFT length %d", n);
   return 1;
@@ -148,7 +150,9 @@ static int launch_fused_impl(int mode, int n, const FusedArgs &a, cudaStream_t s
     case M_KICK: return dispatch_mode<M_KICK>(n, a, st);
     case M_DRIFT: return dispatch_mode<M_DRIFT>(n, a, st);
     case M_DRIFT_DENSITY: return dispatch_mode<M_DRIFT_DENSITY>(n, a, st);
-    case M_DEPOSIT: return dispatch_deposit(n, a, st);
+    case M_DEPOSIT: return dispatch_z_only<M_DEPOSIT>(n, a, st);
+    case M_ADJ_SOURCE: return dispatch_z_only<M_ADJ_SOURCE>(n, a, st);
+    case M_ADJ_UPDATE: return dispatch_z_only<M_ADJ_UPDATE>(n, a, st);
   }
   set_error("internal: bad pass mode %d", mode);
   return 1;
@@ -244,7 +248,9 @@ int launch_fused(int mode, int n, const FusedArgs &a, cudaStream_t st) {
   const bool prof = prof_on();
   if (prof) prof_mark_begin(st);
   const int rc = launch_fused_impl(mode, n, a, st);
-  if (prof && rc == 0) prof_mark_end(mode, st);
+  // buckets 0..7 are the passes of the step; the adjoint's passes count as
+  // other kernels (8)
+  if (prof && rc == 0) prof_mark_end(mode <= M_DEPOSIT ? mode : 8, st);
   return rc;
 }
 

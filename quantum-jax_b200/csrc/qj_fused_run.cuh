@@ -128,7 +128,7 @@ int run_fused(const FusedArgs &a, cudaStream_t st) {
   int per_sm = 0, sms = 0;
   const cudaError_t occ = fused_occupancy<N, CONTIG, MODE, V>(per_sm, sms);
   QJ_CK(occ);
-  const int want = a.tune ? a.tune[MODE] : 0;
+  const int want = (a.tune && MODE <= M_DEPOSIT) ? a.tune[MODE] : 0;  // [0..7]: passes
   const int resident = (want > 0 ? std::min(want, per_sm) : per_sm) * sms;
   const int reserve = (a.tune && a.tune[8] >= 0) ? a.tune[8] : reserve_ctas();
   // the bulk tile copies need 16-byte aligned fields

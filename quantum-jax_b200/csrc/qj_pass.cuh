@@ -18,6 +18,11 @@
 //                  optional drift along q: psi <- IFFT_q(P_q FFT_q psi)
 //   DRIFT          psi -> IFFT_y(P_y FFT_y psi)
 //   DRIFT_DENSITY  DRIFT along r, then DENSITY along r
+// Adjoint of the kick (reverse sweep), along z, around FFT_FWD / POISSON /
+// IFFT2 of the same source:
+//   ADJ_SOURCE     g, psi, V -> mu = c Im(conj(g) e^{-icV} psi) -> FFT_z -> R
+//   ADJ_UPDATE     S1 -> IFFT_z -> W; g <- e^{icV} g + 2 (W + b mu) psi; the
+//                  drift adjoint along z (the propagator of -dt)
 #pragma once
 
 #include <cuda.h>
@@ -35,6 +40,8 @@ enum PassMode : int {
   M_DRIFT = 5,
   M_DRIFT_DENSITY = 6,
   M_DEPOSIT = 7,  // dense star density along z (bin_stars), no transform
+  M_ADJ_SOURCE = 8,
+  M_ADJ_UPDATE = 9,
 };
 
 struct FusedArgs {
@@ -86,6 +93,12 @@ struct FusedArgs {
   // a fixed density added to |psi|^2 in every density build and in the
   // self-interaction term (single box; the star density as a given source)
   const float *rho_src;
+  // adjoint passes: the state before the kick (psi is the adjoint g), the
+  // kick's potential, and mu (written by ADJ_SOURCE, read by ADJ_UPDATE;
+  // only with self-interaction)
+  const float2 *adj_pre;
+  const float *adj_V;
+  float *adj_mu;
   // isothermal gas
   const float *grho;
   float *gv[3];
@@ -584,7 +597,8 @@ template <int N, bool CONTIG, int V = 0> struct Landing {
 // and Poisson passes) and the landing buffer.
 template <int N, bool CONTIG, int MODE, int V = 0> struct FusedSmem {
   using SH = PassShape<N, CONTIG, V>;
-  static constexpr bool DRIFTS = MODE == M_KICK || MODE == M_DRIFT || MODE == M_DRIFT_DENSITY;
+  static constexpr bool DRIFTS =
+      MODE == M_KICK || MODE == M_DRIFT || MODE == M_DRIFT_DENSITY || MODE == M_ADJ_UPDATE;
   static constexpr bool LANDS = MODE != M_DEPOSIT;
   static constexpr bool SAVES = DRIFTS || MODE == M_POISSON || MODE == M_IFFT2;
   static constexpr size_t a16(size_t x) { return (x + 15) & ~(size_t)15; }
@@ -607,11 +621,15 @@ __host__ __device__ constexpr size_t fused_smem_bytes() {
 
 // The input fields a pass streams, in order of use.
 template <int MODE> __host__ __device__ constexpr int stream_count() {
-  return MODE == M_KICK ? 3 : (MODE == M_IFFT2 ? 2 : (MODE == M_DEPOSIT ? 0 : 1));
+  return (MODE == M_KICK || MODE == M_ADJ_UPDATE) ? 3
+         : (MODE == M_IFFT2 || MODE == M_ADJ_SOURCE) ? 2
+         : (MODE == M_DEPOSIT ? 0 : 1);
 }
 template <int MODE>
 __host__ __device__ __forceinline__ const float2 *stream_field(const FusedArgs &a, int f) {
   if constexpr (MODE == M_KICK) return f == 0 ? a.S2 : (f == 1 ? a.S1 : a.psi);
+  if constexpr (MODE == M_ADJ_SOURCE) return f == 0 ? a.psi : a.adj_pre;
+  if constexpr (MODE == M_ADJ_UPDATE) return f == 0 ? a.S1 : (f == 1 ? a.psi : a.adj_pre);
   if constexpr (MODE == M_IFFT2) return f == 0 ? a.S1 : a.S2;
   if constexpr (MODE == M_FFT_FWD || MODE == M_POISSON) return a.R;
   return a.psi;
@@ -1136,6 +1154,64 @@ __device__ __forceinline__ void fused_body(FusedArgs &a, const TileMaps &maps, c
       } else {
         atomic_max_nonneg(a.amax_bits, am);
       }
+    } else if constexpr (MODE == M_ADJ_SOURCE) {
+      // mu = c Im(conj(g) psi') with psi' = e^{-icV} psi (the kick adjoint's
+      // Poisson source, quantum-stars.py:300 differentiated), its float64
+      // partial sum, and its forward transform along z (half of R)
+      const unsigned gb = (unsigned)base + (unsigned)t * (unsigned)st, gs = (unsigned)P * (unsigned)st;
+      float2 v[E];
+      QJ_TAKE(v);  // g
+      {
+        float2 z[E];
+        QJ_TAKE(z);  // psi before the kick
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+          float sn, cs;
+          sincos_reduced(a.kick_coef * (double)a.adj_V[gb + e * gs], sn, cs);
+          const float2 zp = float2{z[e].x * cs + z[e].y * sn, z[e].y * cs - z[e].x * sn};
+          const float m = (float)a.kick_coef * (v[e].x * zp.y - v[e].y * zp.x);
+          if (a.adj_mu) a.adj_mu[gb + e * gs] = m;
+          v[e] = float2{m, 0.0f};
+        }
+      }
+      double sm = 0.0;
+#pragma unroll
+      for (int e = 0; e < E; ++e) sm += (double)v[e].x;
+      sm = block_sum<THREADS>(sm, red);
+      if (tid == 0) a.part[tile] = sm;
+      fft_pencil<N, -1, true>(v, t, smv, tw);
+      store_pencil_half<N, E>(v, a.R, base, st, t, P);
+    } else if constexpr (MODE == M_ADJ_UPDATE) {
+      // W = L mu along z from S1 (its real part), then
+      // g <- e^{icV} g + 2 (W + b mu) psi and the drift adjoint along z
+      const unsigned gb = (unsigned)base + (unsigned)t * (unsigned)st, gs = (unsigned)P * (unsigned)st;
+      float W[E];
+      {
+        float2 v1[E];
+        QJ_TAKE(v1);
+        fft_pencil<N, +1, true>(v1, t, smv, tw);
+#pragma unroll
+        for (int e = 0; e < E; ++e) W[e] = v1[e].x;
+      }
+      float2 g[E];
+      QJ_TAKE(g);
+      const float2 gc = c0;  // the drift's increment constant: g's element 0
+      {
+        float2 z[E];
+        QJ_TAKE(z);  // psi before the kick
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+          float w = W[e];
+          if (a.adj_mu) w = w + a.b_coeff * a.adj_mu[gb + e * gs];
+          float sn, cs;
+          sincos_reduced(a.kick_coef * (double)a.adj_V[gb + e * gs], sn, cs);
+          const float two_w = 2.0f * w;
+          g[e] = float2{g[e].x * cs - g[e].y * sn + two_w * z[e].x,
+                        g[e].y * cs + g[e].x * sn + two_w * z[e].y};
+        }
+      }
+      if (a.do_drift) drift_pencil<N, E, P, THREADS>(g, gc, tab2, t, smv, tw, save);
+      store_pencil<E>(g, a.psi, base, st, t, P);
     } else if constexpr (MODE == M_DEPOSIT) {
       // bin_stars (quantum-stars.py:212-247): every cell sums its star
       // contributions from zero in star order
