@@ -731,8 +731,11 @@ int adjoint_sweep(qj_plan *P, const void *ckpt, void *g, int nsteps, int K, doub
         a.kick_coef = coef;
         a.half = 1;
         QJ_TRY(launch_fused(M_ADJ_SOURCE, P->n[q], a, st));
+        // each pass from here follows another fused pass directly: launched
+        // as its programmatic dependent
         a = fused_args(P, 1, M_FFT_FWD);
         half_spectrum(a, P, q);
+        a.pdl = 1;
         QJ_TRY(launch_fused(M_FFT_FWD, P->n[1], a, st));
         a = fused_args(P, r, M_POISSON);
         a.half = 1;
@@ -740,10 +743,12 @@ int adjoint_sweep(qj_plan *P, const void *ckpt, void *g, int nsteps, int K, doub
         a.part_in = P->part;
         a.n_part = pass_blocks(P->n[q], q, P->n[0], P->n[1], P->n[2], 0);  // ADJ_SOURCE's tiles
         a.rho_bar = 0.0;
+        a.pdl = 1;
         QJ_TRY(launch_fused(M_POISSON, P->n[r], a, st));
         a = fused_args(P, 1, M_IFFT2);
         a.half = 1;
         half_spectrum(a, P, q);
+        a.pdl = 1;
         QJ_TRY(launch_fused(M_IFFT2, P->n[1], a, st));
         a = fused_args(P, q, M_ADJ_UPDATE);
         a.psi = (float2 *)g;
@@ -753,11 +758,13 @@ int adjoint_sweep(qj_plan *P, const void *ckpt, void *g, int nsteps, int K, doub
         a.kick_coef = coef;
         a.b_coeff = si ? (float)P->ph.b_coeff : 0.0f;
         a.do_drift = j > 0 ? 1 : 0;
+        a.pdl = 1;
         QJ_TRY(launch_fused(M_ADJ_UPDATE, P->n[q], a, st));
         if (j > 0)
           for (int ax = 1; ax >= 0; --ax) {
             FusedArgs d = fused_args(P, ax, M_DRIFT);
             d.psi = (float2 *)g;
+            d.pdl = 1;
             QJ_TRY(launch_fused(M_DRIFT, P->n[ax], d, st));
           }
       }
