@@ -202,12 +202,13 @@ int qj_get_potential_f32_noalloc(const qj_grid *grid, const qj_phys *phys,
  * indexed by plan: psi[i], pos[i], vel[i] (device), n_s[i], m_s[i], dt[i]
  * (host), diag[i] (device, nbox records).
  * qj_ensemble_set_merge(ens, 1) runs each fused pass of the step as one
- * persistent launch over all plans' boxes instead, its CTAs split between
- * the sizes in proportion to their work, when the plans are cubes of distinct
- * sizes among 64, 96 and 128 with the default radix plan and tile (tuning
- * fields 10, 11 zero).  The bits are the same; the per-plan streams measured
- * faster, so they are the default (merge 0).  qj_ensemble_merged returns 1
- * when steps use the single launches, else 0. */
+ * launch over all plans' boxes instead, whose CTAs claim each box's tiles
+ * from a device counter (a small buffer of the ensemble, sized before any
+ * capture), when the plans are cubes of distinct sizes among 64, 96 and 128
+ * with the default radix plan and tile (tuning fields 10, 11 zero).  The
+ * bits are the same; the per-plan streams measured faster, so they are the
+ * default (merge 0).  qj_ensemble_merged returns 1 when steps use the single
+ * launches, else 0. */
 typedef struct qj_ensemble qj_ensemble;
 int qj_ensemble_create(qj_ensemble **ens, qj_plan *const *plans, int nplans);
 int qj_ensemble_destroy(qj_ensemble *ens);

@@ -1889,6 +1889,10 @@ struct qj_ensemble {
   std::vector<cudaEvent_t> joins;
   cudaGraphExec_t exec = nullptr;
   std::vector<const void *> key;  // pointers and sizes the graph was captured with
+  // tile counters of the ensemble launches: one per box for each launch of a
+  // merged body (ens_counters)
+  unsigned *ctr = nullptr;
+  size_t ctr_n = 0;
 };
 
 namespace {
@@ -1918,13 +1922,47 @@ bool ens_mergeable(const qj_ensemble *E) {
   return true;
 }
 
+// Boxes of all plans, and the fused launches of an m-step merged body: the
+// first density build, four potential passes for each of the m + 1 kicks and
+// two drift passes for each step.
+int ens_boxes(const qj_ensemble *E) {
+  int b = 0;
+  for (const qj_plan *P : E->plans) b += P->nbox;
+  return b;
+}
+size_t ens_launches(int m) { return 6 * (size_t)m + 5; }
+
+// Tile counters for merged bodies of up to m steps (allocated here, never
+// during a stream capture: qj_ensemble_step calls this before it captures).
+int ens_counters(qj_ensemble *E, int m) {
+  const size_t need = ens_launches(m) * (size_t)ens_boxes(E);
+  if (E->ctr_n >= need) return 0;
+  if (E->ctr) {
+    QJ_CK(cudaFree(E->ctr));
+    E->ctr = nullptr;
+    E->ctr_n = 0;
+  }
+  QJ_CK(cudaMalloc(&E->ctr, need * sizeof(unsigned)));
+  E->ctr_n = need;
+  return 0;
+}
+
 // m steps of every plan with one launch per fused pass for all of them: the
 // phases of fused_kdk (KdkRun), each run for all plans before the next.  The
 // plans' star updates and sorts run on their own side streams, forked after
 // the kick and joined before the drift + density pass, as in fused_kdk.
+// Each launch claims tiles from its own counters, all zeroed by one memset.
 int ensemble_merged_body(qj_ensemble *E, const EnsArgs &a, int m) {
   const int np = (int)E->plans.size();
   cudaStream_t st = E->origin;
+  const int boxes = ens_boxes(E);
+  const size_t nctr = ens_launches(m) * (size_t)boxes;
+  if (E->ctr_n < nctr) {
+    set_error("internal: %zu ensemble tile counters for %zu", E->ctr_n, nctr);
+    return QJ_ERR_ARG;
+  }
+  QJ_CK(cudaMemsetAsync(E->ctr, 0, nctr * sizeof(unsigned), st));
+  size_t launch = 0;
   std::vector<KdkRun> runs;
   int reserve = 0;
   for (int i = 0; i < np; ++i) {
@@ -1945,7 +1983,12 @@ int ensemble_merged_body(qj_ensemble *E, const EnsArgs &a, int m) {
       fa[i] = ph.a;
       fn[i] = runs[i].P->n[ph.axis];
     }
-    return launch_fused_ens(mode, np, fa, fn, reserve, st);
+    if (launch >= ens_launches(m)) {
+      set_error("internal: more ensemble launches than counted");
+      return QJ_ERR_ARG;
+    }
+    unsigned *ctr = E->ctr + launch++ * (size_t)boxes;
+    return launch_fused_ens(mode, np, fa, fn, reserve, ctr, boxes, st);
   };
   for (KdkRun &R : runs) QJ_TRY(R.begin(st));
   QJ_TRY(phase([](KdkRun &R) { return R.density(); }));
@@ -2022,6 +2065,7 @@ int qj_ensemble_destroy(qj_ensemble *E) {
   if (!E) return QJ_OK;
   if (E->origin) cudaStreamSynchronize(E->origin);
   if (E->exec) cudaGraphExecDestroy(E->exec);
+  if (E->ctr) cudaFree(E->ctr);
   for (cudaStream_t s : E->streams)
     if (s) cudaStreamDestroy(s);
   for (cudaEvent_t j : E->joins)
@@ -2072,9 +2116,11 @@ int qj_ensemble_step(qj_ensemble *E, void *const *psi, void *const *pos, void *c
   QJ_CK(cudaEventRecord(E->caller, st));
   QJ_CK(cudaStreamWaitEvent(E->origin, E->caller, 0));
   const int full = nsteps / chunk, rem = nsteps % chunk;
+  if (ens_mergeable(E)) QJ_TRY(ens_counters(E, std::max(full > 0 ? chunk : 0, rem)));
   if (use_graph && full > 0) {
     std::vector<const void *> key;
     key.push_back((const void *)(intptr_t)(ens_mergeable(E) ? 1 : 0));
+    key.push_back(E->ctr);  // a graph of merged launches holds its counters
     for (size_t i = 0; i < np; ++i) {
       key.push_back(psi[i]);
       key.push_back(n_s[i] ? pos[i] : nullptr);

@@ -1,32 +1,34 @@
 // Ensemble launches of the fused passes: one persistent launch per pass for
 // the boxes of up to three batched plans of sizes 64, 96 and 128 (one plan
 // per size).  Those lengths share a CTA shape (128 threads on a strided pass,
-// 256 on a contiguous one), so each CTA runs the pass body of its size class:
-// the classes split the launch's resident CTAs in proportion to their work,
-// and within a class the CTAs stride over its boxes' tiles exactly as a
-// k_fused launch of that plan would.  Results are bit-identical to stepping
-// each plan on its own (no tile's arithmetic depends on which CTA runs it).
+// 256 on a contiguous one), so a CTA can run the pass body of any size class.
+// Each CTA works on one box and claims its tiles from the box's counter
+// (DynCta) until none are left, copying its next tile in while it transforms
+// the current one; each class has enough CTAs to fill the GPU, and the
+// classes follow one another in the launch (k_fused_ens).  Results are
+// bit-identical to stepping each plan on its own (no tile's arithmetic
+// depends on which CTA runs it).
 #include <cmath>
 
 #include "qj_fused_run.cuh"
 
 namespace qj {
 
-// Size classes, by slot: the largest first, so that its CTAs (the bulk of
-// the work) start first and the smaller classes' fill the tail.
+// Size classes, by slot: the largest first, so that the smaller classes'
+// shorter tiles fill the launch's tail.
 constexpr int kEnsSizes[kEnsClasses] = {128, 96, 64};
-
-double ens_oversubscription();
 
 struct EnsClass {
   FusedArgs a;
   TileMaps maps;
-  int cta0;  // first CTA of the class in the launch
-  int gx;    // persistent CTAs per box (the class has gx * nbox CTAs)
-  int ctas;  // gx * nbox, 0 for an empty slot
+  int nbox;  // boxes of the class (0 for an empty slot)
+  int ctr0;  // the first box's tile counter in the launch's counters
+  int cta0;  // the class's CTA range in the launch: the CTAs that start on it
+  int ctas;
 };
 struct EnsLaunch {
   EnsClass c[kEnsClasses];
+  unsigned *ctr;  // one tile counter per box of the launch, zeroed before it
 };
 static_assert(sizeof(EnsLaunch) <= 4096, "ensemble launch parameters exceed 4 KB");
 
@@ -46,22 +48,32 @@ template <int MODE, bool CONTIG> constexpr size_t ens_smem_bytes() {
   return a > b ? (a > c ? a : c) : (b > c ? b : c);
 }
 
-template <int N, bool CONTIG, int MODE>
-__device__ __forceinline__ void ens_class_body(const EnsClass &c, int local) {
+// One CTA of class S: its box is its place in the class's CTA range modulo
+// the class's box count, and it claims that box's tiles until none are left.
+template <int S, int MODE, bool CONTIG>
+__device__ __forceinline__ void ens_class_body(const EnsLaunch &L, int local, int *slot) {
+  const EnsClass &c = L.c[S];
+  const int b = local % c.nbox;
   FusedArgs a = c.a;
-  fused_body<N, CONTIG, MODE, 0>(a, c.maps, CtaPos{local % c.gx, local / c.gx, c.gx});
+  fused_body<kEnsSizes[S], CONTIG, MODE, 0>(a, c.maps, DynCta{b, L.ctr + c.ctr0 + b, slot});
 }
 
+// The classes' CTA ranges follow one another in slot order, the largest
+// class first; each range holds enough CTAs to fill the GPU on its own.  The
+// hardware starts the CTAs in order, so the largest class's boxes take the
+// GPU first, and as its CTAs find no tiles left and leave, the next class's
+// CTAs take their slots: the classes overlap only at their ends.
 template <int MODE, bool CONTIG>
 __global__ void __launch_bounds__(EnsShape<CONTIG>::THREADS, EnsShape<CONTIG>::MINB)
     k_fused_ens(const __grid_constant__ EnsLaunch L) {
-  const int b = (int)blockIdx.x;
-  if (b < L.c[0].cta0 + L.c[0].ctas) {
-    ens_class_body<kEnsSizes[0], CONTIG, MODE>(L.c[0], b - L.c[0].cta0);
-  } else if (b < L.c[1].cta0 + L.c[1].ctas) {
-    ens_class_body<kEnsSizes[1], CONTIG, MODE>(L.c[1], b - L.c[1].cta0);
-  } else if (b < L.c[2].cta0 + L.c[2].ctas) {
-    ens_class_body<kEnsSizes[2], CONTIG, MODE>(L.c[2], b - L.c[2].cta0);
+  __shared__ int slot;
+  const int bid = (int)blockIdx.x;
+  if (bid < L.c[0].cta0 + L.c[0].ctas) {
+    ens_class_body<0, MODE, CONTIG>(L, bid - L.c[0].cta0, &slot);
+  } else if (bid < L.c[1].cta0 + L.c[1].ctas) {
+    ens_class_body<1, MODE, CONTIG>(L, bid - L.c[1].cta0, &slot);
+  } else if (bid < L.c[2].cta0 + L.c[2].ctas) {
+    ens_class_body<2, MODE, CONTIG>(L, bid - L.c[2].cta0, &slot);
   }
 }
 
@@ -89,7 +101,7 @@ template <int MODE, bool CONTIG> static cudaError_t ens_occupancy(int &per_sm, i
 }
 
 template <int N, int MODE, bool CONTIG>
-static int ens_class_setup(const FusedArgs &a, EnsClass &c, double &work) {
+static int ens_class_setup(const FusedArgs &a, EnsClass &c) {
   c.a = a;
   c.a.ntiles = grid_of<N, CONTIG, 0>(a);
   c.a.rev = (!CONTIG && a.axis == 1) ? 1 : 0;
@@ -98,19 +110,16 @@ static int ens_class_setup(const FusedArgs &a, EnsClass &c, double &work) {
     const int rc = strided_maps<N, MODE, 0>(c.a, c.maps);
     if (rc) return rc;
   }
-  const int nbox = a.nbox > 1 ? a.nbox : 1;
-  // a tile holds the same number of pencils in every class; its cost grows
-  // as N log N
-  work = (double)c.a.ntiles * nbox * N * std::log2((double)N);
+  c.nbox = a.nbox > 1 ? a.nbox : 1;
   return 0;
 }
 
 template <int MODE, bool CONTIG>
-static int run_ens(int np, const FusedArgs *a, const int *n, int reserve, cudaStream_t st) {
+static int run_ens(int np, const FusedArgs *a, const int *n, int reserve, unsigned *ctr,
+                   int nctr, cudaStream_t st) {
   EnsLaunch L;
   std::memset(&L, 0, sizeof(L));
-  double work[kEnsClasses] = {0.0, 0.0, 0.0}, total = 0.0;
-  int nboxes[kEnsClasses] = {0, 0, 0};
+  L.ctr = ctr;
   for (int i = 0; i < np; ++i) {
     const void *fields[4] = {a[i].psi, a[i].R, a[i].S1, a[i].S2};
     for (const void *f : fields)
@@ -120,47 +129,36 @@ static int run_ens(int np, const FusedArgs *a, const int *n, int reserve, cudaSt
       }
     const int slot = ens_slot(n[i]);
     EnsClass &c = L.c[slot];
-    const int rc = slot == 0   ? ens_class_setup<kEnsSizes[0], MODE, CONTIG>(a[i], c, work[0])
-                   : slot == 1 ? ens_class_setup<kEnsSizes[1], MODE, CONTIG>(a[i], c, work[1])
-                               : ens_class_setup<kEnsSizes[2], MODE, CONTIG>(a[i], c, work[2]);
+    const int rc = slot == 0   ? ens_class_setup<kEnsSizes[0], MODE, CONTIG>(a[i], c)
+                   : slot == 1 ? ens_class_setup<kEnsSizes[1], MODE, CONTIG>(a[i], c)
+                               : ens_class_setup<kEnsSizes[2], MODE, CONTIG>(a[i], c);
     if (rc) return rc;
-    nboxes[slot] = a[i].nbox > 1 ? a[i].nbox : 1;
-    total += work[slot];
+  }
+  // the classes' box counters follow one another in slot order
+  int boxes = 0;
+  for (int s = 0; s < kEnsClasses; ++s) {
+    L.c[s].ctr0 = boxes;
+    boxes += L.c[s].nbox;
+  }
+  if (boxes > nctr) {
+    set_error("internal: ensemble launch of %d boxes with %d tile counters", boxes, nctr);
+    return QJ_ERR_ARG;
   }
   int per_sm = 0, sms = 0;
   QJ_CK((ens_occupancy<MODE, CONTIG>(per_sm, sms)));
+  // each class's range: a multiple of its box count, at least the CTAs that
+  // fit at once (less the reserved slots)
   const int resident = std::max(1, per_sm * sms - reserve);
-  // CTAs of equal work, ens_oversubscription() times as many as fit at once:
-  // the hardware starts each next CTA where one finishes, which balances the
-  // classes as their passes run.  The classes' CTA ranges follow one another
-  // in slot order (an empty slot has an empty range at its place), the order
-  // k_fused_ens tests.
-  const double per_cta = total / (ens_oversubscription() * resident);
   int next = 0;
   for (int s = 0; s < kEnsClasses; ++s) {
     EnsClass &c = L.c[s];
     c.cta0 = next;
-    if (nboxes[s] == 0) continue;
-    const int want = (int)std::lround(work[s] / nboxes[s] / per_cta);
-    c.gx = std::max(1, std::min(c.a.ntiles, want));
-    c.ctas = c.gx * nboxes[s];
+    c.ctas = c.nbox > 0 ? ((resident + c.nbox - 1) / c.nbox) * c.nbox : 0;
     next += c.ctas;
   }
   k_fused_ens<MODE, CONTIG><<<next, EnsShape<CONTIG>::THREADS, ens_smem_bytes<MODE, CONTIG>(), st>>>(L);
   QJ_CK_LAUNCH();
   return 0;
-}
-
-// CTAs of an ensemble launch per resident slot (QJ_ENS_OVERSUB, default 6;
-// measured on the 32-box mix: 1, 2, 3, 6 gave 1363, 1171, 1131, 1073 us per
-// step).
-double ens_oversubscription() {
-  static double f = -1.0;
-  if (f < 0) {
-    const char *env = getenv("QJ_ENS_OVERSUB");
-    f = env ? std::max(1.0, atof(env)) : 6.0;
-  }
-  return f;
 }
 
 int ens_slot(int n) {
@@ -170,7 +168,7 @@ int ens_slot(int n) {
 }
 
 int launch_fused_ens(int mode, int np, const FusedArgs *a, const int *n, int reserve,
-                     cudaStream_t st) {
+                     unsigned *ctr, int nctr, cudaStream_t st) {
   if (np < 1 || np > kEnsClasses) {
     set_error("internal: ensemble launch of %d plans", np);
     return QJ_ERR_ARG;
@@ -194,7 +192,8 @@ int launch_fused_ens(int mode, int np, const FusedArgs *a, const int *n, int res
   int rc;
 #define QJ_ENS(M)                                                                        \
   case M:                                                                                \
-    rc = contig ? run_ens<M, true>(np, a, n, reserve, st) : run_ens<M, false>(np, a, n, reserve, st); \
+    rc = contig ? run_ens<M, true>(np, a, n, reserve, ctr, nctr, st)                   \
+                : run_ens<M, false>(np, a, n, reserve, ctr, nctr, st);                 \
     break;
   switch (mode) {
     QJ_ENS(M_DENSITY)
@@ -202,8 +201,8 @@ int launch_fused_ens(int mode, int np, const FusedArgs *a, const int *n, int res
     QJ_ENS(M_KICK)
     QJ_ENS(M_DRIFT)
     QJ_ENS(M_DRIFT_DENSITY)
-    case M_FFT_FWD: rc = run_ens<M_FFT_FWD, false>(np, a, n, reserve, st); break;
-    case M_IFFT2: rc = run_ens<M_IFFT2, false>(np, a, n, reserve, st); break;
+    case M_FFT_FWD: rc = run_ens<M_FFT_FWD, false>(np, a, n, reserve, ctr, nctr, st); break;
+    case M_IFFT2: rc = run_ens<M_IFFT2, false>(np, a, n, reserve, ctr, nctr, st); break;
     default:
       set_error("internal: pass mode %d has no ensemble launch", mode);
       rc = QJ_ERR_ARG;

@@ -90,13 +90,14 @@ int launch_fused(int mode, int n, const FusedArgs &a, cudaStream_t st);
 int pass_blocks(int n_axis, int axis, int nx, int ny, int nz, int v = 0);
 // Ensemble launch of pass `mode` for np <= kEnsClasses plans of distinct
 // sizes n[i] in {64, 96, 128} (their axis lengths along a[i].axis, the same
-// axis for all, shape variant 0): one persistent launch whose CTAs run each
-// plan's pass over its boxes; `reserve` CTA slots stay free.  Bit-identical
-// to one launch_fused per plan.
+// axis for all, shape variant 0): one persistent launch whose CTAs claim the
+// tiles of every plan's boxes; `reserve` CTA slots stay free.  ctr holds
+// nctr >= (boxes of all plans) tile counters, zeroed before the launch and
+// used by it alone.  Bit-identical to one launch_fused per plan.
 constexpr int kEnsClasses = 3;
 int ens_slot(int n);  // the size class of length n, -1 if none
 int launch_fused_ens(int mode, int np, const FusedArgs *a, const int *n, int reserve,
-                     cudaStream_t st);
+                     unsigned *ctr, int nctr, cudaStream_t st);
 // Generic in-place FFT pass over a complex field (float2 if dbl == 0, else
 // double2) along a.axis.
 int launch_fft(bool dbl, int n, int dir, const FftArgs &a, cudaStream_t st);

@@ -123,7 +123,7 @@ struct FusedArgs {
   const int *tune;
   // set to nonzero when a pass gave up waiting for a tile copy
   unsigned *err;
-  // batched boxes (CtaPos::box): per-box strides of the fields (cells),
+  // batched boxes (the CTA's box()): per-box strides of the fields (cells),
   // stars, bucket starts, partial sums; a_max is per box
   int nbox;  // launch grid.y (0 or 1 = one box)
   long long box_cells;
@@ -135,18 +135,31 @@ struct FusedArgs {
 // A CTA's place in its pass: box box(), slot bx() of the gx() persistent
 // CTAs that stride over that box's tiles.  k_fused reads them from its grid
 // (GridCta: blockIdx.y, blockIdx.x, gridDim.x, re-read where used, as the
-// special registers they are); an ensemble launch assigns them from the size
-// class's CTA range (CtaPos).
+// special registers they are); an ensemble launch's CTAs claim tiles instead
+// (DynCta).
 struct GridCta {
+  static constexpr bool DYN = false;
   __device__ __forceinline__ int bx() const { return (int)blockIdx.x; }
   __device__ __forceinline__ int box() const { return (int)blockIdx.y; }
   __device__ __forceinline__ int gx() const { return (int)gridDim.x; }
 };
-struct CtaPos {
-  int bx_, box_, gx_;
-  __device__ __forceinline__ int bx() const { return bx_; }
+// A CTA of an ensemble launch that claims the tiles of box box() one at a
+// time from that box's counter (zeroed before the launch): every CTA of the
+// launch that works on the box takes its next tile from the same counter, so
+// the box's tiles are shared out as the CTAs finish their previous ones.
+// Thread 0 claims (one atomicAdd) one tile ahead of the one it starts to
+// copy, so the claim's round trip overlaps a tile's work, and publishes the
+// tile to start in a shared-memory word; a claim of ntiles or more means the
+// box has no tiles left (and every later claim of the CTA is past it too).
+struct DynCta {
+  static constexpr bool DYN = true;
+  int box_;
+  unsigned *ctr;
+  int *slot;
   __device__ __forceinline__ int box() const { return box_; }
-  __device__ __forceinline__ int gx() const { return gx_; }
+  __device__ __forceinline__ int claim() const { return (int)atomicAdd(ctr, 1u); }
+  __device__ __forceinline__ void publish(int tile) const { *(volatile int *)slot = tile; }
+  __device__ __forceinline__ int claimed() const { return *(volatile int *)slot; }
 };
 
 // Offset a pass' pointers to box b of a batched plan.
@@ -743,7 +756,7 @@ template <int N, bool CONTIG, int MODE, int V, int E, class CTA>
 __device__ __forceinline__ bool take_tile(float2 (&v)[E], float2 &c0, const FusedArgs &a,
                                           const TileMaps &maps, float2 *land,
                                           unsigned long long *bar, unsigned &parity, int &f, int tile,
-                                          int p, int t, const CTA &cta) {
+                                          int p, int t, const CTA &cta, int &ahead) {
   using L = Landing<N, CONTIG, V>;
   constexpr int P = N / E, NF = stream_count<MODE>();
   bool ok = mbar_wait_bounded(bar, parity);
@@ -768,12 +781,40 @@ __device__ __forceinline__ bool take_tile(float2 (&v)[E], float2 &c0, const Fuse
   int nf = f + 1, nt = tile;
   if (nf == NF) {
     nf = 0;
-    nt = tile + cta.gx();
+    if constexpr (CTA::DYN) {
+      // the CTA's next tile is the one thread 0 claimed ahead: published for
+      // warp 0's copy and for every thread after the tile (next_tile); the
+      // claim after it goes out now and is waited for at the next tile
+      nt = a.ntiles;
+      if (threadIdx.x < 32) {
+        if (threadIdx.x == 0) {
+          cta.publish(ahead);
+          ahead = cta.claim();
+        }
+        __syncwarp();
+        nt = cta.claimed();
+      }
+    } else {
+      nt = tile + cta.gx();
+    }
   }
   f = nf;
   if (nt < a.ntiles && threadIdx.x < 32)
     issue_tile<N, CONTIG, MODE, V>(a, maps, nf, a.rev ? a.ntiles - 1 - nt : nt, cta.box(), land, bar);
   return true;
+}
+
+// The loop index of a CTA's next tile.  A claiming CTA reads the claim its
+// thread 0 made when it started the next tile's first copy (in the tile's
+// last take_tile); the barrier makes it visible, and no thread can reach the
+// next claim before every thread has read this one (take_tile's barrier).
+template <class CTA> __device__ __forceinline__ int next_tile(int it, const CTA &cta) {
+  if constexpr (CTA::DYN) {
+    __syncthreads();
+    return cta.claimed();
+  } else {
+    return it + cta.gx();
+  }
 }
 
 // The body of a fused pass for one CTA: k_fused runs it with the CTA's own
@@ -827,7 +868,15 @@ __device__ __forceinline__ void fused_body(FusedArgs &a, const TileMaps &maps, c
       tabk[N + i] = (a.axis == 0 ? a.kt[0] : (a.axis == 1 ? a.kt[1] : a.kt[2]))[i];
     }
   }
-  if (tid == 0) mbar_init(&lbar, 1);
+  static_assert(!CTA::DYN || LAY::LANDS, "claimed tiles need the landing pipeline");
+  int ahead = 0;  // claiming CTAs: thread 0's claim after the published tile
+  if (tid == 0) {
+    mbar_init(&lbar, 1);
+    if constexpr (CTA::DYN) {
+      cta.publish(cta.claim());  // the CTA's first tile
+      ahead = cta.claim();
+    }
+  }
   __syncthreads();
   // The tables above are the plan's own; the previous pass's results are read
   // from here on.  Launched as a programmatic dependent of that pass, this
@@ -837,15 +886,21 @@ __device__ __forceinline__ void fused_body(FusedArgs &a, const TileMaps &maps, c
   const float2 *tw = tw_s;
   unsigned parity = 0;
   int fld = 0;
+  int first;
+  if constexpr (CTA::DYN)
+    first = cta.claimed();
+  else
+    first = cta.bx();
   if constexpr (LAY::LANDS)
-    if (cta.bx() < a.ntiles && tid < 32)
-      issue_tile<N, CONTIG, MODE, SV>(a, maps, 0, a.rev ? a.ntiles - 1 - cta.bx() : cta.bx(),
-                                      cta.box(), land, &lbar);
+    if (first < a.ntiles && tid < 32)
+      issue_tile<N, CONTIG, MODE, SV>(a, maps, 0, a.rev ? a.ntiles - 1 - first : first, cta.box(),
+                                      land, &lbar);
 
-  for (int it = cta.bx(); it < a.ntiles; it += cta.gx()) {
+  for (int it = first; it < a.ntiles; it = next_tile(it, cta)) {
     // this CTA's last tile: a next pass launched as a programmatic dependent
     // may start its CTAs in the slots that free up from now on
-    if (it + cta.gx() >= a.ntiles) asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    if constexpr (!CTA::DYN)
+      if (it + cta.gx() >= a.ntiles) asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     const int tile = a.rev ? a.ntiles - 1 - it : it;  // logical tile
     const PencilPos pp = pencil_pos<CONTIG>(a, tile, p, TP);
     const long long base = pp.base, st = a.stride;
@@ -857,7 +912,8 @@ __device__ __forceinline__ void fused_body(FusedArgs &a, const TileMaps &maps, c
       if (a.has_stars) sr = star_ranges(a, pp);
     float2 c0;
 #define QJ_TAKE(v) \
-  if (!take_tile<N, CONTIG, MODE, SV, E, CTA>(v, c0, a, maps, land, &lbar, parity, fld, it, p, t, cta)) \
+  if (!take_tile<N, CONTIG, MODE, SV, E, CTA>(v, c0, a, maps, land, &lbar, parity, fld, it, p, t, cta, \
+                                              ahead))                                                 \
   return
 
     if constexpr (MODE == M_DENSITY) {
@@ -1250,6 +1306,14 @@ __device__ __forceinline__ void fused_body(FusedArgs &a, const TileMaps &maps, c
       }
     }
 #undef QJ_TAKE
+  }
+  if constexpr (CTA::DYN) {
+    // no copy is in flight (the last claim found no tile): retire the
+    // landing barrier, so that this CTA's body for its next box can
+    // initialise one in the same place
+    __syncthreads();
+    if (tid == 0) asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(&lbar)) : "memory");
+    __syncthreads();
   }
 }
 
