@@ -293,7 +293,9 @@ int qj_hydro_cfl_dt(qj_plan *plan, const void *vx, const void *vy, const void *v
  * steps per trial; psi/pos/vel are not modified) and keeps the fastest
  * setting in the plan: with QJ_AUTOTUNE_SHAPES in flags it first picks, per
  * pass and orientation, the radix plan and tile ([10], [11]) among the four
- * combinations, then, as without it, the CTA counts [0..8].  No reference counterpart (XLA
+ * combinations, timing that pass alone (CUDA events around its launches,
+ * unless qj_profile_enable is on, when it times whole steps), then, as
+ * without it, the CTA counts [0..8].  No reference counterpart (XLA
  * picks its own launch shapes and FFT plans). */
 #define QJ_TUNE_N 12
 #define QJ_TUNE_RADIX 10

@@ -250,7 +250,8 @@ int launch_fused(int mode, int n, const FusedArgs &a, cudaStream_t st) {
   const int rc = launch_fused_impl(mode, n, a, st);
   // buckets 0..7 are the passes of the step; the adjoint's passes count as
   // other kernels (8)
-  if (prof && rc == 0) prof_mark_end(mode <= M_DEPOSIT ? mode : 8, st);
+  if (prof && rc == 0)
+    prof_mark_end((mode <= M_DEPOSIT ? mode : 8) + (prof_split() && a.axis == 2 ? kProfZ : 0), st);
   return rc;
 }
 

@@ -58,6 +58,10 @@ constexpr int kProfBuckets = 9;
 bool prof_on();
 void prof_mark_begin(cudaStream_t st);
 void prof_mark_end(int bucket, cudaStream_t st);
+// The autotuner's pass timing: while set, a fused pass along z counts in
+// bucket kProfZ + mode instead of mode.
+constexpr int kProfZ = 16;
+bool prof_split();
 
 bool fft_length_supported(int n);
 // Stage twiddle table of the fused passes for length n and radix plan rv
